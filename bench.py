@@ -1,0 +1,445 @@
+"""Benchmark: batched BFV multiply + relinearise at N=16384 on B200.
+
+Workload (one "step"): 64 independent ciphertext pairs, N=16384, 7 x 60-bit
+ciphertext primes + 1 special prime, t=65537, dnum=1, multiplied and
+relinearised by one fused launch sequence (captured in a CUDA graph).
+Inputs are resident in HBM (235 MB, larger than the 126 MB L2, so no flush
+is needed between steps).
+
+Also reported on the same box: the one-pair-per-call ("per-op") form, the
+end-to-end rate through the C ABI with host buffers, the standalone NTT at
+N=65536 x 2048 rows (32 primes x 64 polynomials), and the CPU baseline.
+
+`--impl reference` times the reference path on the host cores instead: the
+reference (kunpBFV) has no CPU implementation, so this is the CPU oracle's
+restatement of it, run with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFV mult+relin ct/s @N=16384 batched vs per-op on 1 B200; NTT HBM GB/s; p50/p99"
+T = 65537
+LOG_N = 14
+NQ, NP = 7, 1
+BATCH = 64
+SEED = bytes(range(32))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--skip-extras", action="store_true", help="only the headline workload")
+    return ap.parse_args()
+
+
+def c3_primes():
+    import oracle  # prime search only (same rule as the library)
+    ps = oracle.primes_bits(1 << LOG_N, 60, NQ + NP)
+    return ps[NP:NP + NQ], ps[:NP]
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                pass
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = max(mx)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(sm)
+        return out
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU restatement of the reference's path, all host threads
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import numpy as np
+
+    import oracle
+    qs, ps = c3_primes()
+    o = oracle.Oracle(LOG_N, T, qs, ps, dnum=1)
+    sk = o.keygen_secret(SEED)
+    pk = o.keygen_public(SEED, sk)
+    rlk = o.keygen_relin(SEED, sk)
+    rng = np.random.default_rng(0)
+    cores = os.cpu_count() or 1
+    npairs = max(cores, 8)
+    cts = []
+    for i in range(npairs):
+        v1 = rng.integers(0, T, size=o.n, dtype=np.uint64)
+        v2 = rng.integers(0, T, size=o.n, dtype=np.uint64)
+        cts.append((o.encrypt(SEED, 2 * i, pk, o.encode(v1)), o.encrypt(SEED, 2 * i + 1, pk, o.encode(v2))))
+
+    def one_step():
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=cores) as ex:
+            list(ex.map(lambda p: o.mul_relin(p[0], p[1], rlk), cts))
+
+    for _ in range(max(1, min(args.warmup, 1))):
+        one_step()
+    times = []
+    steps = max(1, min(args.steps, 5))
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        one_step()
+        times.append(time.perf_counter() - t0)
+    per_step = statistics.median(times)
+    v = npairs / per_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ct/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"mult+relin N=16384 7x60q+1p t=65537 dnum=1, {npairs} pairs per step on CPU",
+                   "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "ct/s", "cores": cores, "kind": "port",
+                         "sample": f"{npairs} pairs per step, {steps} steps; kunpBFV has no CPU path, "
+                                   "so the CPU oracle restatement stands in"},
+        "e2e": {"value": round(v, 3), "unit": "ct/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def cpu_baseline_sample(seconds=12.0):
+    """Oracle mult+relin on the host cores (bounded sample)."""
+    import numpy as np
+
+    import oracle
+    qs, ps = c3_primes()
+    o = oracle.Oracle(LOG_N, T, qs, ps, dnum=1)
+    sk = o.keygen_secret(SEED)
+    pk = o.keygen_public(SEED, sk)
+    rlk = o.keygen_relin(SEED, sk)
+    rng = np.random.default_rng(1)
+    cores = os.cpu_count() or 1
+    cts = []
+    for i in range(cores):
+        v1 = rng.integers(0, T, size=o.n, dtype=np.uint64)
+        v2 = rng.integers(0, T, size=o.n, dtype=np.uint64)
+        cts.append((o.encrypt(SEED, 2 * i, pk, o.encode(v1)), o.encrypt(SEED, 2 * i + 1, pk, o.encode(v2))))
+    done = [0]
+    lock = threading.Lock()
+    stop = time.perf_counter() + seconds
+
+    def worker(p):
+        while time.perf_counter() < stop:
+            o.mul_relin(p[0], p[1], rlk)
+            with lock:
+                done[0] += 1
+
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=worker, args=(p,)) for p in cts]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    el = time.perf_counter() - t0
+    return {"value": round(done[0] / el, 3), "unit": "ct/s", "cores": cores, "kind": "port",
+            "sample": f"{done[0]} pairs in {el:.1f} s on {cores} threads (CPU oracle restatement; "
+                      "kunpBFV has no CPU path)"}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200.api import to_device
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    qs, ps = c3_primes()
+    ctx = kb.BFVContext(log_n=LOG_N, plain_modulus=T, q_count=NQ, q=qs, p_count=NP, p=ps, dnum=1)
+    sk = kb.SecretKey(ctx, SEED)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    ctx.reserve(BATCH)
+    rng = np.random.default_rng(rank)
+    v1 = rng.integers(0, T, size=(BATCH, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(BATCH, ctx.N), dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v1))), enc_id=rank * 1000000)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v2))), enc_id=rank * 1000000 + BATCH)
+    out = kb.Ciphertext(ctx, count=BATCH)
+    torch.cuda.synchronize()
+
+    def step():
+        sch.mult_relin(c1, c2, out=out, stream=stream)
+
+    # correctness gate on the benchmark data itself
+    with torch.cuda.stream(stream):
+        step()
+    torch.cuda.synchronize()
+    dec = kb.api.to_host(ctx.decode(sch.decryptMsg(sk, out).mx_device)).reshape(BATCH, ctx.N)
+    ok = bool(np.array_equal(dec, (v1 * v2) % T))
+    budget = sch.noise_budget(sk, kb.Ciphertext(ctx, out.cipher_device.view(-1)[: 2 * NQ * ctx.N].clone()))
+
+    graph = None
+    if not args.no_graph:
+        for _ in range(2):
+            with torch.cuda.stream(stream):
+                step()
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            step()
+        torch.cuda.synchronize()
+
+    def run_step():
+        if graph is not None:
+            with torch.cuda.stream(stream):
+                graph.replay()
+        else:
+            with torch.cuda.stream(stream):
+                step()
+
+    for _ in range(args.warmup):
+        run_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            run_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(world, ms)
+    value = world * BATCH / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "ct/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded XSalsa20 encryptions of uniform slots)",
+        "config": {"workload": "mult+relin N=16384 7x60q+1p t=65537 dnum=1 (HPS tensor + hybrid key switch)",
+                   "batch_pairs_per_gpu": BATCH, "cuda_graph": graph is not None,
+                   "l2": "inputs 235 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+        "decrypt_exact": ok, "noise_budget_bits": round(budget, 2),
+        "gpu_launches": 8 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.skip_extras:
+        line.update(extras(args, ctx, sch, c1, c2, out, stream, dev))
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def time_cuda(fn, stream, iters, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(iters):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / iters
+
+
+def extras(args, ctx, sch, c1, c2, out, stream, dev):
+    import torch
+
+    import kunpbfv_b200 as kb
+    res = {}
+    N = ctx.N
+    lq = 2 * NQ * N
+    peak, peak_kind = load_peaks()
+
+    # per-op form: one pair per call, eager launches
+    a1 = [c1.cipher_device.view(-1)[i * lq:(i + 1) * lq] for i in range(BATCH)]
+    b1 = [c2.cipher_device.view(-1)[i * lq:(i + 1) * lq] for i in range(BATCH)]
+    o1 = [out.cipher_device.view(-1)[i * lq:(i + 1) * lq] for i in range(BATCH)]
+
+    def per_op():
+        with torch.cuda.stream(stream):
+            for i in range(BATCH):
+                sch.mult_relin_ptrs([a1[i].data_ptr()], [b1[i].data_ptr()], [o1[i].data_ptr()], stream=stream)
+
+    ms_op = time_cuda(per_op, stream, 3)
+    res["per_op"] = {"value": round(BATCH / (ms_op / 1e3), 2), "unit": "ct/s",
+                     "form": "one pair per call, 8 eager launches each, no graph"}
+
+    # e2e through the C ABI with pinned host buffers
+    h_a = torch.empty(c1.cipher_device.shape, dtype=torch.int64, pin_memory=True)
+    h_b = torch.empty(c2.cipher_device.shape, dtype=torch.int64, pin_memory=True)
+    h_o = torch.empty(out.cipher_device.shape, dtype=torch.int64, pin_memory=True)
+    h_a.copy_(c1.cipher_device)
+    h_b.copy_(c2.cipher_device)
+    d_a = torch.empty_like(c1.cipher_device)
+    d_b = torch.empty_like(c2.cipher_device)
+    d_o = torch.empty_like(out.cipher_device)
+    ca, cb, co = kb.Ciphertext(ctx, d_a), kb.Ciphertext(ctx, d_b), kb.Ciphertext(ctx, d_o)
+
+    def e2e():
+        with torch.cuda.stream(stream):
+            d_a.copy_(h_a, non_blocking=True)
+            d_b.copy_(h_b, non_blocking=True)
+            sch.mult_relin(ca, cb, out=co, stream=stream)
+            h_o.copy_(d_o, non_blocking=True)
+
+    ms_e2e = time_cuda(e2e, stream, 3)
+    res["e2e"] = {"value": round(BATCH / (ms_e2e / 1e3), 2), "unit": "ct/s",
+                  "h2d_bytes_per_step": 2 * d_a.numel() * 8, "d2h_bytes_per_step": d_o.numel() * 8}
+
+    # dominant kernel (forward NTT block kernel, N=16384) timed alone on the
+    # same row count as the pipeline's largest forward-NTT launch
+    rows = BATCH * 4 * (NQ + 1)
+    x = torch.randint(0, 1 << 59, (rows, N), dtype=torch.int64, device=dev)
+    ms_ntt = time_cuda(lambda: ctx.ntt_fwd(x, ctx.idx_r, NQ + 1, stream=stream), stream, 10)
+    alg = 16 * N * rows + 16 * N * (NQ + 1)
+    ach = alg / (ms_ntt / 1e3) / 1e9
+    res["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                       "frac": round(ach / peak, 4), "traffic": None,
+                       "kernel": f"ntt_fwd_block_kernel<14> on {rows} rows ({peak_kind} peak)",
+                       "ms_per_launch": round(ms_ntt, 4)}
+    del x
+
+    # standalone NTT, N=65536, 32 primes x 64 polynomials (1 GiB)
+    qs2 = __import__("oracle").primes_bits(1 << 16, 60, 34)
+    ctx2 = kb.BFVContext(log_n=16, plain_modulus=T, q_count=32, q=qs2[2:34], p_count=1, p=qs2[:1], dnum=1)
+    mods = torch.tensor(ctx2.q, dtype=torch.int64, device=dev)
+    y = torch.randint(0, 1 << 62, (64, 32, 1 << 16), dtype=torch.int64, device=dev)
+    y = torch.remainder(y, mods.view(1, 32, 1))
+    ms_f = time_cuda(lambda: ctx2.ntt_fwd(y, 0, 32, stream=stream), stream, 5)
+    ms_i = time_cuda(lambda: ctx2.ntt_inv(y, 0, 32, stream=stream), stream, 5)
+    alg2 = 16 * 65536 * 2048 + 16 * 65536 * 32
+    res["ntt_n65536"] = {"fwd_gbs": round(alg2 / (ms_f / 1e3) / 1e9, 1),
+                         "inv_gbs": round(alg2 / (ms_i / 1e3) / 1e9, 1),
+                         "fwd_ms": round(ms_f, 4), "inv_ms": round(ms_i, 4),
+                         "frac_of_peak_fwd": round(alg2 / (ms_f / 1e3) / 1e9 / peak, 4),
+                         "rows": 2048, "algorithmic_bytes": alg2}
+    del y
+    ctx2.close()
+    return res
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

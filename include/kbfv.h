@@ -1,0 +1,199 @@
+/*
+ * kbfv.h -- C ABI of the B200-native BFV multiply path (libkbfv.so).
+ *
+ * kunpBFV exposes its multiply path as a header-only C++ class API
+ * (BFVContext / BFVScheme / Plaintext / Ciphertext / SecretKey / Key_decomp)
+ * compiled into the caller. This header is the flat boundary underneath an
+ * equivalent API: opaque context handle, plain device pointers and sizes,
+ * int status codes, caller-supplied CUDA stream (0 = legacy default stream).
+ * kbfv_compat.hpp rebuilds the reference's class names on top of it.
+ *
+ * Data layout (all device memory, uint64 residues, limb-major poly[limb][coeff]):
+ *   ciphertext  [a | b], each q_count limbs, NTT form over Q  (decrypts as b + a*s)
+ *   tensor      [a1*a2 | a1*b2 + b1*a2 | b1*b2], each q_count limbs, NTT form
+ *   secret key  q_count + p_count limbs, NTT form over Q|P
+ *   public key  [a | b], q_count limbs each, NTT form
+ *   relin key   dnum x [a | b], (q_count + p_count) limbs each, NTT form over Q|P
+ *   plaintext   N coefficients mod t (coefficient form)
+ *   slots       N values mod t (batch encoding: slot k <-> NTT index k mod t)
+ * Prime table order inside a context: [ Q | P | R (HPS base) | T (KLSS) | t ].
+ *
+ * Every function returns KBFV_OK or a negative kbfv_status; kbfv_last_error()
+ * describes the most recent failure on the calling thread.
+ */
+#ifndef KBFV_H
+#define KBFV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    KBFV_OK = 0,
+    KBFV_ERR_INVALID = -1,    /* bad argument (std::invalid_argument in the reference) */
+    KBFV_ERR_PARAMS = -2,     /* parameter set cannot be built (logic_error in the reference) */
+    KBFV_ERR_CUDA = -3,       /* a CUDA call failed */
+    KBFV_ERR_NOMEM = -4,      /* device allocation failed */
+    KBFV_ERR_NO_KEY = -5,     /* key missing ("rotKey_23 not exists" in the reference) */
+    KBFV_ERR_LEVEL = -6,      /* ciphertext level unsupported ("Ciphertexts are on level 0") */
+    KBFV_ERR_UNSUPPORTED = -7
+} kbfv_status;
+
+typedef struct kbfv_context kbfv_context;
+typedef void* kbfv_stream; /* cudaStream_t */
+
+/* Parameter set. Explicit primes win over bit sizes; R (the HPS base) is
+ * always derived: q_count + 1 primes below min(q) that are 1 mod 2N.
+ * Replaces the hard-coded BFVContext::getPrimeBFV (include/Params.cuh:7-149). */
+typedef struct {
+    uint32_t log_n;           /* ring degree N = 2^log_n, 10..16 */
+    uint64_t plain_modulus;   /* t, prime, 1 mod 2N for batching */
+    uint32_t q_count;
+    const uint64_t* q;        /* q_count primes, or NULL to generate q_bits-sized primes */
+    uint32_t q_bits;
+    uint32_t p_count;
+    const uint64_t* p;        /* special primes or NULL (generated with p_bits, largest first) */
+    uint32_t p_bits;
+    uint32_t dnum;            /* key-switch digits; digit size alpha = ceil(q_count / dnum) */
+    uint32_t t_count;         /* optional KLSS base (reference key switch), may be 0 */
+    const uint64_t* t_primes;
+    uint32_t gamma;           /* KLSS Ri block size */
+} kbfv_params;
+
+const char* kbfv_last_error(void);
+const char* kbfv_version(void);
+
+/* ---- context ---------------------------------------------------------
+ * BFVContext::BFVContext(size_t N) (include/BFVcontext.cuh:13-101):
+ * precompute on the host, tables to the device. One context per parameter
+ * set; any number of contexts may coexist in a process (no __constant__ state). */
+int kbfv_context_create(const kbfv_params* params, kbfv_context** out);
+/* the reference's own parameter sets, logN = 14 or 15 (include/Params.cuh:31-145) */
+int kbfv_context_create_reference(uint32_t log_n, kbfv_context** out);
+int kbfv_context_destroy(kbfv_context* ctx);
+/* sizes: N, q_count, p_count, r_count, t_count, dnum, alpha */
+int kbfv_context_info(const kbfv_context* ctx, uint64_t* n, uint32_t* q_count, uint32_t* p_count,
+                      uint32_t* r_count, uint32_t* t_count, uint32_t* dnum, uint32_t* alpha);
+/* full prime table [Q|P|R|T|t]; count receives its length (primes may be NULL) */
+int kbfv_context_primes(const kbfv_context* ctx, uint64_t* primes, uint32_t* count);
+uint64_t kbfv_context_plain_modulus(const kbfv_context* ctx);
+/* decrypt rounding variant chosen by bit sizes (0 small, 1 small_lazy, 2 large, 3 large_lazy) */
+int kbfv_context_decrypt_variant(const kbfv_context* ctx);
+/* bytes of device scratch a batched multiply of `count` pairs uses */
+size_t kbfv_mul_relin_scratch_bytes(const kbfv_context* ctx, uint32_t count);
+/* pre-size the context's scratch arena (no allocation happens later for <= count pairs) */
+int kbfv_reserve(kbfv_context* ctx, uint32_t pairs);
+
+/* ---- NTT over the context's prime table --------------------------------
+ * ToNTTInplace / FromNTTInplace (include/BFVcontext.cuh:1513-1552) and the
+ * _for_QR / _for_BFV / _for_externalProduct variants (1554-1757): rows are
+ * consecutive N-coefficient limbs; row r uses prime index
+ * prime0 + (r % period). In place. */
+int kbfv_ntt_fwd(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t prime0, uint32_t period,
+                 kbfv_stream stream);
+int kbfv_ntt_inv(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t prime0, uint32_t period,
+                 kbfv_stream stream);
+
+/* ---- HPS building blocks (per polynomial, coefficient form) ------------
+ * BaseConverter::bConv_HPS (include/BasisConv_QR.cuh:191-207): centred base
+ * extension Q -> R and R -> Q. */
+int kbfv_bconv_q_to_r(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                      kbfv_stream stream);
+int kbfv_bconv_r_to_q(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                      kbfv_stream stream);
+/* tensor_prod_2x2_rns_poly (include/poly_arithmetic.cuh:1180-1219): pairs of
+ * [a|b] over Q|R (NTT form) -> [a1a2 | cross | b1b2] over Q|R */
+int kbfv_tensor_qr(kbfv_context* ctx, const uint64_t* d_ct1, const uint64_t* d_ct2, uint64_t* d_out,
+                   uint32_t pairs, kbfv_stream stream);
+/* scaleAndRound_HPS_QR_R (include/poly_arithmetic.cuh:1263-1316): Q|R -> R */
+int kbfv_scale_round_qr_r(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                          kbfv_stream stream);
+/* hps_decrypt_scale_and_round (include/BFVcontext.cuh:1680-1717): Q -> N values */
+int kbfv_decrypt_round(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                       kbfv_stream stream);
+/* bfv_add_timesQ_overt_kernel (include/poly_arithmetic.cuh:902-927): m -> ceil(Q*m/t) over Q */
+int kbfv_delta_m(kbfv_context* ctx, const uint64_t* d_m, uint64_t* d_out, uint32_t polys,
+                 kbfv_stream stream);
+
+/* ---- key-switch building blocks (coefficient form) ---------------------
+ * digit lift of one polynomial over Q into dnum polynomials over Q|P; the
+ * quotient estimate restates modUpQjtoT_23 (include/BasisConv.cuh:86-151) */
+int kbfv_modup(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+               kbfv_stream stream);
+/* modDownPQltoQl_23 (include/BasisConv.cuh:229-319): Q|P -> Q */
+int kbfv_moddown(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                 kbfv_stream stream);
+
+/* ---- keys --------------------------------------------------------------
+ * SecretKey::SecretKey (include/SecretKey.cuh:20-37), BFVScheme::addEncKey
+ * (include/BFVScheme.cuh:57-85), BFVScheme::addMultKey_23
+ * (include/KeySwitch_23.cuh:21-66). All randomness comes from XSalsa20 keyed
+ * by `seed` (32 bytes); the same seed reproduces the same keys.
+ * secret_kind: 0 = ternary uniform, 1 = Hamming weight h (the reference's HWT). */
+int kbfv_keygen_secret(kbfv_context* ctx, const uint8_t seed[32], int secret_kind, uint32_t h,
+                       uint64_t* d_sk, kbfv_stream stream);
+int kbfv_keygen_public(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint64_t* d_pk,
+                       kbfv_stream stream);
+int kbfv_keygen_relin(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint64_t* d_rlk,
+                      kbfv_stream stream);
+
+/* ---- encoder -----------------------------------------------------------
+ * BFVContext::encode / decode (include/Encoder.cuh:23-112): INTT / NTT mod t.
+ * Unlike the reference, encode does not overwrite its input. */
+int kbfv_encode(kbfv_context* ctx, const uint64_t* d_slots, uint64_t* d_m, uint32_t count,
+                kbfv_stream stream);
+int kbfv_decode(kbfv_context* ctx, const uint64_t* d_m, uint64_t* d_slots, uint32_t count,
+                kbfv_stream stream);
+/* BFVContext::encode_ntt (include/Encoder.cuh:64-79): values as coefficients, NTT over Q */
+int kbfv_encode_ntt(kbfv_context* ctx, const uint64_t* d_vals, uint64_t* d_pt_ntt, uint32_t count,
+                    kbfv_stream stream);
+
+/* ---- scheme ------------------------------------------------------------
+ * BFVScheme::encryptMsg / decryptMsg (include/BFVScheme.cuh:87-166).
+ * Encrypts `count` plaintexts (consecutive, N words each) into `count`
+ * consecutive ciphertexts; ciphertext i uses randomness stream enc_id + i. */
+int kbfv_encrypt(kbfv_context* ctx, const uint8_t seed[32], uint64_t enc_id, const uint64_t* d_pk,
+                 const uint64_t* d_m, uint64_t* d_ct, uint32_t count, kbfv_stream stream);
+int kbfv_decrypt(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, uint64_t* d_m,
+                 uint32_t count, kbfv_stream stream);
+/* BFVScheme::add / addAndEqual (include/BFVScheme.cuh:169-190); polys per item = 2 */
+int kbfv_add(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64_t* d_out,
+             uint32_t count, kbfv_stream stream);
+/* BFVScheme::multConstAndEqual (include/BFVScheme.cuh:226-245) with an encode_ntt plaintext */
+int kbfv_mul_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_pt_ntt, uint64_t* d_out,
+                   uint32_t count, kbfv_stream stream);
+/* compute_t_QInv_c0c1c2 (include/KeySwitch_23.cuh:703-926) without its
+ * secret-key shortcut: HPS tensor of `count` ciphertext pairs -> tensors */
+int kbfv_mul(kbfv_context* ctx, const uint64_t* d_ct1, const uint64_t* d_ct2, uint64_t* d_tensor,
+             uint32_t count, kbfv_stream stream);
+/* key switch of the a1*a2 term (include/KeySwitch_23.cuh:277-305): tensors -> ciphertexts */
+int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_tensor, uint64_t* d_ct,
+                     uint32_t count, kbfv_stream stream);
+/* BFVScheme::multAndEqual_23 / mult_23 (include/KeySwitch_23.cuh:192-310) as
+ * one fused batched launch sequence: out[i] = relin(ct_a[i] * ct_b[i]).
+ * Arrays are HOST arrays of device pointers. */
+int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* const* ct_a,
+                         const uint64_t* const* ct_b, uint64_t* const* out, uint32_t count,
+                         kbfv_stream stream);
+/* same for consecutive ciphertexts (stride 2*q_count*N words) */
+int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                   uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
+/* invariant noise budget in bits of one ciphertext (host-side diagnostic, synchronous) */
+int kbfv_noise_budget(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, double* bits);
+
+/* ---- randomness ---------------------------------------------------------
+ * XSalsa20 keystream (the reference's RNG::generateRandom_device,
+ * include/RNG.cuh:18-51, corrected: "expand 32-byte k" constants, HSalsa20
+ * subkey, 64-bit nonce). compat != 0 reproduces the reference's variant
+ * (zero constants, 32-bit nonce from nonce[0..3], no HSalsa20). */
+int kbfv_salsa20_stream(const uint8_t key[32], const uint8_t nonce[24], uint64_t block0, uint8_t* d_out,
+                        size_t nbytes, int compat, kbfv_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KBFV_H */

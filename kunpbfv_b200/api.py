@@ -1,0 +1,519 @@
+"""ctypes bindings of libkbfv.so and the reference-shaped Python classes.
+
+Class and method names follow kunpBFV (include/BFVScheme.h:12-178,
+include/BFVcontext.h:17-391): ``BFVContext``, ``BFVScheme.encryptMsg``,
+``decryptMsg``, ``addAndEqual``, ``multAndEqual_23``, ``multConstAndEqual``,
+``BFVContext.encode`` / ``decode`` / ``encode_ntt``. Errors surface as
+``KbfvError`` subclasses of the exception types the reference throws
+(``ValueError`` for std::invalid_argument, ``RuntimeError`` otherwise).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libkbfv.so")
+_lib: Optional[C.CDLL] = None
+
+U64P = C.POINTER(C.c_uint64)
+U8P = C.POINTER(C.c_uint8)
+VP = C.c_void_p
+
+KBFV_OK = 0
+_ERR_NAMES = {
+    -1: "invalid argument",
+    -2: "parameter set",
+    -3: "CUDA",
+    -4: "out of device memory",
+    -5: "missing key",
+    -6: "level",
+    -7: "unsupported",
+}
+
+
+class KbfvError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"kbfv error {code} ({_ERR_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class KbfvInvalidArgument(KbfvError, ValueError):
+    pass
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("log_n", C.c_uint32),
+        ("plain_modulus", C.c_uint64),
+        ("q_count", C.c_uint32),
+        ("q", U64P),
+        ("q_bits", C.c_uint32),
+        ("p_count", C.c_uint32),
+        ("p", U64P),
+        ("p_bits", C.c_uint32),
+        ("dnum", C.c_uint32),
+        ("t_count", C.c_uint32),
+        ("t_primes", U64P),
+        ("gamma", C.c_uint32),
+    ]
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib() -> C.CDLL:
+    """Load libkbfv.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError(
+                f"{_LIB_PATH} is missing; build it with `python -m kunpbfv_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(_LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L: C.CDLL) -> None:
+    I = C.c_int
+    u32, u64 = C.c_uint32, C.c_uint64
+    sig = {
+        "kbfv_last_error": (C.c_char_p, []),
+        "kbfv_version": (C.c_char_p, []),
+        "kbfv_context_create": (I, [C.POINTER(_Params), C.POINTER(VP)]),
+        "kbfv_context_create_reference": (I, [u32, C.POINTER(VP)]),
+        "kbfv_context_destroy": (I, [VP]),
+        "kbfv_context_info": (I, [VP, U64P, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32),
+                                  C.POINTER(u32), C.POINTER(u32)]),
+        "kbfv_context_primes": (I, [VP, U64P, C.POINTER(u32)]),
+        "kbfv_context_plain_modulus": (u64, [VP]),
+        "kbfv_context_decrypt_variant": (I, [VP]),
+        "kbfv_mul_relin_scratch_bytes": (C.c_size_t, [VP, u32]),
+        "kbfv_reserve": (I, [VP, u32]),
+        "kbfv_ntt_fwd": (I, [VP, VP, u32, u32, u32, VP]),
+        "kbfv_ntt_inv": (I, [VP, VP, u32, u32, u32, VP]),
+        "kbfv_bconv_q_to_r": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_bconv_r_to_q": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_tensor_qr": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_scale_round_qr_r": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_decrypt_round": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_delta_m": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_modup": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_moddown": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_keygen_secret": (I, [VP, U8P, I, u32, VP, VP]),
+        "kbfv_keygen_public": (I, [VP, U8P, VP, VP, VP]),
+        "kbfv_keygen_relin": (I, [VP, U8P, VP, VP, VP]),
+        "kbfv_encode": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_decode": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_encode_ntt": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_encrypt": (I, [VP, U8P, u64, VP, VP, VP, u32, VP]),
+        "kbfv_decrypt": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_add": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_mul_plain": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_mul": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_relinearize": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_mul_relin_batch": (I, [VP, VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
+        "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
+        "kbfv_noise_budget": (I, [VP, VP, VP, C.POINTER(C.c_double)]),
+        "kbfv_salsa20_stream": (I, [U8P, U8P, u64, VP, C.c_size_t, I, VP]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def _check(rc: int) -> None:
+    if rc != KBFV_OK:
+        msg = lib().kbfv_last_error().decode(errors="replace")
+        if rc == -1:
+            raise KbfvInvalidArgument(rc, msg)
+        raise KbfvError(rc, msg)
+
+
+def _u8(b: bytes):
+    a = (C.c_uint8 * len(b)).from_buffer_copy(bytes(b))
+    return a
+
+
+def _torch():
+    import torch  # deferred: importing the bindings does not need a GPU
+
+    return torch
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        torch = _torch()
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _ptr(t) -> int:
+    return t.data_ptr()
+
+
+def to_device(a: np.ndarray, device="cuda"):
+    """numpy uint64 -> torch int64 device tensor (same bits)."""
+    torch = _torch()
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return torch.from_numpy(a.view(np.int64)).to(device)
+
+
+def to_host(t) -> np.ndarray:
+    return t.detach().cpu().numpy().view(np.uint64)
+
+
+@dataclass
+class Params:
+    log_n: int
+    plain_modulus: int
+    q_count: int
+    q_bits: int = 60
+    p_count: int = 1
+    p_bits: int = 60
+    dnum: int = 1
+    q: Optional[Sequence[int]] = None
+    p: Optional[Sequence[int]] = None
+    t_primes: Sequence[int] = ()
+    gamma: int = 1
+
+
+class BFVContext:
+    """A parameter set (BFVContext, include/BFVcontext.h:17-391).
+
+    Public fields mirror the reference: ``N``, ``L`` (= q_count - 1),
+    ``K`` (= p_count), ``slots`` (= N), ``plain_modulus``.
+    """
+
+    def __init__(self, params: Optional[Params] = None, *, _handle=None, **kw):
+        L = lib()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            if params is None:
+                params = Params(**kw)
+            self.params = params
+            keep = []
+
+            def arr(v):
+                if not v:
+                    return None
+                a = (C.c_uint64 * len(v))(*[int(x) for x in v])
+                keep.append(a)
+                return C.cast(a, U64P)
+
+            pr = _Params(params.log_n, params.plain_modulus, params.q_count, arr(params.q), params.q_bits,
+                         params.p_count, arr(params.p), params.p_bits, params.dnum, len(params.t_primes),
+                         arr(list(params.t_primes)), params.gamma)
+            h = VP()
+            _check(L.kbfv_context_create(C.byref(pr), C.byref(h)))
+            self._h = h
+        n = C.c_uint64()
+        nq, np_, nr, nt, dnum, alpha = (C.c_uint32() for _ in range(6))
+        _check(L.kbfv_context_info(self._h, C.byref(n), C.byref(nq), C.byref(np_), C.byref(nr), C.byref(nt),
+                                   C.byref(dnum), C.byref(alpha)))
+        self.N = int(n.value)
+        self.log_n = self.N.bit_length() - 1
+        self.q_count, self.p_count, self.r_count, self.t_count = nq.value, np_.value, nr.value, nt.value
+        self.dnum, self.alpha = dnum.value, alpha.value
+        self.L = self.q_count - 1
+        self.K = self.p_count
+        self.slots = self.N
+        self.plain_modulus = int(L.kbfv_context_plain_modulus(self._h))
+        cnt = C.c_uint32()
+        _check(L.kbfv_context_primes(self._h, None, C.byref(cnt)))
+        buf = (C.c_uint64 * cnt.value)()
+        _check(L.kbfv_context_primes(self._h, buf, C.byref(cnt)))
+        self.primes = [int(x) for x in buf]
+        self.q = self.primes[: self.q_count]
+        self.p = self.primes[self.q_count: self.q_count + self.p_count]
+        self.r = self.primes[self.q_count + self.p_count: self.q_count + self.p_count + self.r_count]
+        self.tk = self.primes[self.q_count + self.p_count + self.r_count: -1]
+        self.decrypt_variant = int(L.kbfv_context_decrypt_variant(self._h))
+
+    # prime-table offsets
+    @property
+    def idx_p(self):
+        return self.q_count
+
+    @property
+    def idx_r(self):
+        return self.q_count + self.p_count
+
+    @property
+    def idx_t(self):
+        return self.q_count + self.p_count + self.r_count
+
+    @property
+    def idx_plain(self):
+        return len(self.primes) - 1
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.kbfv_context_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def reserve(self, pairs: int):
+        _check(lib().kbfv_reserve(self._h, pairs))
+
+    def scratch_bytes(self, pairs: int) -> int:
+        return int(lib().kbfv_mul_relin_scratch_bytes(self._h, pairs))
+
+    # ---- device buffers
+    def zeros(self, *shape):
+        torch = _torch()
+        return torch.zeros(shape, dtype=torch.int64, device="cuda")
+
+    # ---- NTT (ToNTTInplace / FromNTTInplace)
+    def ntt_fwd(self, rows, prime0: int, period: int, stream=None):
+        nrows = rows.numel() // self.N
+        _check(lib().kbfv_ntt_fwd(self._h, _ptr(rows), nrows, prime0, period, _stream_ptr(stream)))
+
+    def ntt_inv(self, rows, prime0: int, period: int, stream=None):
+        nrows = rows.numel() // self.N
+        _check(lib().kbfv_ntt_inv(self._h, _ptr(rows), nrows, prime0, period, _stream_ptr(stream)))
+
+    # ---- encoder (include/Encoder.cuh)
+    def encode(self, slots, out=None, stream=None):
+        count = slots.numel() // self.N
+        out = out if out is not None else self.zeros(count, self.N)
+        _check(lib().kbfv_encode(self._h, _ptr(slots), _ptr(out), count, _stream_ptr(stream)))
+        return out
+
+    def decode(self, m, out=None, stream=None):
+        count = m.numel() // self.N
+        out = out if out is not None else self.zeros(count, self.N)
+        _check(lib().kbfv_decode(self._h, _ptr(m), _ptr(out), count, _stream_ptr(stream)))
+        return out
+
+    def encode_ntt(self, vals, out=None, stream=None):
+        count = vals.numel() // self.N
+        out = out if out is not None else self.zeros(count, self.q_count, self.N)
+        _check(lib().kbfv_encode_ntt(self._h, _ptr(vals), _ptr(out), count, _stream_ptr(stream)))
+        return out
+
+    # ---- building blocks
+    def _op(self, name, ins, out, polys, stream=None):
+        args = [self._h] + [_ptr(x) for x in ins] + [_ptr(out), polys, _stream_ptr(stream)]
+        _check(getattr(lib(), name)(*args))
+        return out
+
+    def bconv_q_to_r(self, x, stream=None):
+        polys = x.numel() // (self.q_count * self.N)
+        return self._op("kbfv_bconv_q_to_r", [x], self.zeros(polys, self.r_count, self.N), polys, stream)
+
+    def bconv_r_to_q(self, x, stream=None):
+        polys = x.numel() // (self.r_count * self.N)
+        return self._op("kbfv_bconv_r_to_q", [x], self.zeros(polys, self.q_count, self.N), polys, stream)
+
+    def tensor_qr(self, c1, c2, stream=None):
+        nqr = self.q_count + self.r_count
+        pairs = c1.numel() // (2 * nqr * self.N)
+        return self._op("kbfv_tensor_qr", [c1, c2], self.zeros(pairs, 3, nqr, self.N), pairs, stream)
+
+    def scale_round_qr_r(self, x, stream=None):
+        polys = x.numel() // ((self.q_count + self.r_count) * self.N)
+        return self._op("kbfv_scale_round_qr_r", [x], self.zeros(polys, self.r_count, self.N), polys, stream)
+
+    def decrypt_round(self, x, stream=None):
+        polys = x.numel() // (self.q_count * self.N)
+        return self._op("kbfv_decrypt_round", [x], self.zeros(polys, self.N), polys, stream)
+
+    def delta_m(self, m, stream=None):
+        polys = m.numel() // self.N
+        return self._op("kbfv_delta_m", [m], self.zeros(polys, self.q_count, self.N), polys, stream)
+
+    def modup(self, x, stream=None):
+        polys = x.numel() // (self.q_count * self.N)
+        npq = self.q_count + self.p_count
+        return self._op("kbfv_modup", [x], self.zeros(polys, self.dnum, npq, self.N), polys, stream)
+
+    def moddown(self, x, stream=None):
+        npq = self.q_count + self.p_count
+        polys = x.numel() // (npq * self.N)
+        return self._op("kbfv_moddown", [x], self.zeros(polys, self.q_count, self.N), polys, stream)
+
+
+def reference_context(log_n: int) -> BFVContext:
+    """The reference's own parameter set for logN 14 or 15 (include/Params.cuh:31-145)."""
+    h = VP()
+    _check(lib().kbfv_context_create_reference(log_n, C.byref(h)))
+    return BFVContext(_handle=h)
+
+
+class SecretKey:
+    """SecretKey (include/SecretKey.cuh:10-62): NTT form over Q|P."""
+
+    def __init__(self, ctx: BFVContext, seed: bytes = b"\x00" * 32, kind: int = 0, h: int = 64, stream=None):
+        self.ctx = ctx
+        self.sx_device = ctx.zeros(ctx.q_count + ctx.p_count, ctx.N)
+        _check(lib().kbfv_keygen_secret(ctx.handle, _u8(seed), kind, h, _ptr(self.sx_device), _stream_ptr(stream)))
+
+
+class Plaintext:
+    """Plaintext coefficients mod t (N words per plaintext)."""
+
+    def __init__(self, ctx: BFVContext, data=None, count: int = 1):
+        self.ctx = ctx
+        self.mx_device = data if data is not None else ctx.zeros(count, ctx.N)
+
+    @property
+    def count(self):
+        return self.mx_device.numel() // self.ctx.N
+
+
+class Ciphertext:
+    """Ciphertext [a | b] over Q in NTT form (include/Ciphertext.cuh:5-89); may hold a batch."""
+
+    def __init__(self, ctx: BFVContext, data=None, count: int = 1):
+        self.ctx = ctx
+        self.cipher_device = data if data is not None else ctx.zeros(count, 2, ctx.q_count, ctx.N)
+        self.l = ctx.L
+
+    @property
+    def count(self):
+        return self.cipher_device.numel() // (2 * self.ctx.q_count * self.ctx.N)
+
+    @property
+    def ax_device(self):
+        return self.cipher_device.view(self.count, 2, self.ctx.q_count, self.ctx.N)[:, 0]
+
+    @property
+    def bx_device(self):
+        return self.cipher_device.view(self.count, 2, self.ctx.q_count, self.ctx.N)[:, 1]
+
+
+class Tensor3:
+    """Unrelinearised product [a1a2 | cross | b1b2] over Q in NTT form."""
+
+    def __init__(self, ctx: BFVContext, data=None, count: int = 1):
+        self.ctx = ctx
+        self.data = data if data is not None else ctx.zeros(count, 3, ctx.q_count, ctx.N)
+
+
+class BFVScheme:
+    """BFVScheme (include/BFVScheme.h:12-178) over one context."""
+
+    def __init__(self, ctx: BFVContext, seed: bytes = b"\x00" * 32):
+        self.context = ctx
+        self.seed = bytes(seed)
+        self.publicKey = None
+        self.rlk = None
+        self._enc_counter = 0
+
+    def mallocMemory(self, pairs: int = 1):
+        self.context.reserve(pairs)
+
+    def addEncKey(self, sk: SecretKey, stream=None):
+        ctx = self.context
+        self.publicKey = ctx.zeros(2, ctx.q_count, ctx.N)
+        _check(lib().kbfv_keygen_public(ctx.handle, _u8(self.seed), _ptr(sk.sx_device), _ptr(self.publicKey),
+                                        _stream_ptr(stream)))
+
+    def addMultKey_23(self, sk: SecretKey, stream=None):
+        ctx = self.context
+        self.rlk = ctx.zeros(ctx.dnum, 2, ctx.q_count + ctx.p_count, ctx.N)
+        _check(lib().kbfv_keygen_relin(ctx.handle, _u8(self.seed), _ptr(sk.sx_device), _ptr(self.rlk),
+                                       _stream_ptr(stream)))
+
+    def encryptMsg(self, pt: Plaintext, enc_id: Optional[int] = None, stream=None) -> Ciphertext:
+        if self.publicKey is None:
+            raise KbfvError(-5, "public key not generated (call addEncKey)")
+        ctx = self.context
+        cnt = pt.count
+        if enc_id is None:
+            enc_id = self._enc_counter
+            self._enc_counter += cnt
+        ct = Ciphertext(ctx, count=cnt)
+        _check(lib().kbfv_encrypt(ctx.handle, _u8(self.seed), enc_id, _ptr(self.publicKey), _ptr(pt.mx_device),
+                                  _ptr(ct.cipher_device), cnt, _stream_ptr(stream)))
+        return ct
+
+    def decryptMsg(self, sk: SecretKey, ct: Ciphertext, stream=None) -> Plaintext:
+        ctx = self.context
+        pt = Plaintext(ctx, count=ct.count)
+        _check(lib().kbfv_decrypt(ctx.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), _ptr(pt.mx_device),
+                                  ct.count, _stream_ptr(stream)))
+        return pt
+
+    def add(self, c1: Ciphertext, c2: Ciphertext, stream=None) -> Ciphertext:
+        out = Ciphertext(self.context, count=c1.count)
+        _check(lib().kbfv_add(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device),
+                              _ptr(out.cipher_device), c1.count, _stream_ptr(stream)))
+        return out
+
+    def addAndEqual(self, c1: Ciphertext, c2: Ciphertext, stream=None):
+        _check(lib().kbfv_add(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device),
+                              _ptr(c1.cipher_device), c1.count, _stream_ptr(stream)))
+
+    def multConstAndEqual(self, ct: Ciphertext, pt_ntt, stream=None):
+        _check(lib().kbfv_mul_plain(self.context.handle, _ptr(ct.cipher_device), _ptr(pt_ntt),
+                                    _ptr(ct.cipher_device), ct.count, _stream_ptr(stream)))
+
+    def mult(self, c1: Ciphertext, c2: Ciphertext, stream=None) -> Tensor3:
+        out = Tensor3(self.context, count=c1.count)
+        _check(lib().kbfv_mul(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device), _ptr(out.data),
+                              c1.count, _stream_ptr(stream)))
+        return out
+
+    def relinearize(self, t3: Tensor3, stream=None) -> Ciphertext:
+        if self.rlk is None:
+            raise KbfvError(-5, "rotKey_23 not exists")
+        cnt = t3.data.numel() // (3 * self.context.q_count * self.context.N)
+        out = Ciphertext(self.context, count=cnt)
+        _check(lib().kbfv_relinearize(self.context.handle, _ptr(self.rlk), _ptr(t3.data), _ptr(out.cipher_device),
+                                      cnt, _stream_ptr(stream)))
+        return out
+
+    def mult_relin(self, c1: Ciphertext, c2: Ciphertext, out: Optional[Ciphertext] = None, stream=None) -> Ciphertext:
+        """Batched ct1[i] * ct2[i] with relinearisation (multAndEqual_23 without the shortcut)."""
+        if self.rlk is None:
+            raise KbfvError(-5, "rotKey_23 not exists")
+        out = out if out is not None else Ciphertext(self.context, count=c1.count)
+        _check(lib().kbfv_mul_relin(self.context.handle, _ptr(self.rlk), _ptr(c1.cipher_device),
+                                    _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count, _stream_ptr(stream)))
+        return out
+
+    def mult_relin_ptrs(self, a_ptrs, b_ptrs, out_ptrs, stream=None):
+        n = len(a_ptrs)
+        A = (VP * n)(*a_ptrs)
+        B = (VP * n)(*b_ptrs)
+        O = (VP * n)(*out_ptrs)
+        _check(lib().kbfv_mul_relin_batch(self.context.handle, _ptr(self.rlk), A, B, O, n, _stream_ptr(stream)))
+
+    def multAndEqual_23(self, c1: Ciphertext, c2: Ciphertext, stream=None):
+        self.mult_relin(c1, c2, out=c1, stream=stream)
+
+    def noise_budget(self, sk: SecretKey, ct: Ciphertext) -> float:
+        v = C.c_double()
+        _check(lib().kbfv_noise_budget(self.context.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), C.byref(v)))
+        return float(v.value)
+
+
+def salsa20_stream(key: bytes, nonce: bytes, nbytes: int, block0: int = 0, compat: bool = False, stream=None):
+    torch = _torch()
+    out = torch.zeros(nbytes, dtype=torch.uint8, device="cuda")
+    _check(lib().kbfv_salsa20_stream(_u8(key), _u8(nonce), block0, out.data_ptr(), nbytes, int(compat),
+                                     _stream_ptr(stream)))
+    return out

@@ -1,0 +1,80 @@
+// Parameter-set context: host precompute and the device-side constant view.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ntt.cuh"
+
+namespace kbfv {
+
+constexpr int kMaxPrimes = 96;   // whole prime table [Q|P|R|T|t]
+constexpr int kMaxQ = 24;        // ciphertext primes per context
+constexpr int kMaxP = 8;         // special primes
+
+// Everything a kernel needs, passed by value (all pointers into one device pool).
+struct DevConsts {
+    int logn;
+    int nq, np, nr, nt, dnum, alpha, npq, nqr;
+    int idx_p, idx_r, idx_t, idx_pt;   // prime-table offsets of P, R, T, plain modulus
+    uint64_t t;
+    const uint64_t* mods;
+    const uint64_t* mu_hi;
+    const uint64_t* mu_lo;
+    const tw_t* tw_fwd;   // [prime][N]
+    const tw_t* tw_inv;   // [prime][N]; [0] = n^-1, [1] = psi_br^-1[1] * n^-1
+    // HPS base extension Q -> R
+    const uint64_t *q2r_hatinv, *q2r_hatinvs, *q2r_hat, *q2r_alpha;
+    const double* q2r_inv;
+    // HPS base extension R -> Q
+    const uint64_t *r2q_hatinv, *r2q_hatinvs, *r2q_hat, *r2q_alpha;
+    const double* r2q_inv;
+    // t/Q scale-and-round Q|R -> R
+    const double* sr_frac;       // [nq]
+    const uint64_t* sr_c;        // [nr][nq+1]
+    // decrypt rounding
+    const uint64_t *dec_mod_t, *dec_mod_t_s, *dec_modB_t, *dec_modB_t_s;
+    const double *dec_frac, *dec_fracB;
+    int dec_variant, qmsbhf;
+    // delta * m
+    uint64_t negq_mod_t, negq_mod_t_s;
+    const uint64_t *tinv_q, *tinv_qs;
+    // key switching
+    const uint64_t *p_mod_q, *pinv_q, *pinv_qs, *phatinv_p, *phatinv_ps, *phat_mod_q;
+    const uint64_t *dig_hatinv, *dig_hatinvs, *dig_hat_mod, *dig_q_mod;
+    // Gaussian table
+    const uint64_t* gauss_cdt;
+    int gauss_bound;
+};
+
+struct Context {
+    // parameters
+    int logn = 0;
+    uint64_t n = 0;
+    uint64_t t = 0;
+    int nq = 0, np = 0, nr = 0, nt = 0, gamma = 1, dnum = 1, alpha = 1;
+    std::vector<uint64_t> mods;  // Q | P | R | T | t
+    int dec_variant = 0;
+
+    // device
+    void* pool = nullptr;       // constants
+    DevConsts dc{};
+    // host copies used by host-side diagnostics
+    std::vector<uint64_t> h_q2r_hatinv;
+
+    // scratch arena (grows; never shrinks while the context lives)
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // device pointer tables for batched calls
+    uint64_t** d_ptrs = nullptr;
+    size_t d_ptrs_cap = 0;
+    uint64_t** h_ptrs = nullptr;  // pinned staging
+    cudaEvent_t ptrs_event = nullptr;
+    std::mutex mu;
+    int device = 0;
+};
+
+}  // namespace kbfv

@@ -1,0 +1,1457 @@
+// libkbfv: context construction, launch plumbing, the fused batched
+// multiply + relinearize pipeline, and the C ABI declared in include/kbfv.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/kbfv.h"
+#include "context.cuh"
+#include "host_math.hpp"
+#include "kernels.cuh"
+#include "ntt.cuh"
+
+using namespace kbfv;
+namespace H = kbfv::host;
+
+// ===========================================================================
+// errors
+// ===========================================================================
+static thread_local std::string g_last_error;
+
+struct KbfvError : std::runtime_error {
+    int code;
+    KbfvError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define KB_CHECK_CUDA(call)                                                                        \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            throw KbfvError(e_ == cudaErrorMemoryAllocation ? KBFV_ERR_NOMEM : KBFV_ERR_CUDA,      \
+                            std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+    } while (0)
+
+#define KB_REQUIRE(cond, code, msg) \
+    do {                            \
+        if (!(cond)) throw KbfvError((code), (msg)); \
+    } while (0)
+
+template <class F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return KBFV_OK;
+    } catch (const KbfvError& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return KBFV_ERR_INVALID;
+    }
+}
+
+static void check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw KbfvError(KBFV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ===========================================================================
+// context construction (BFVContext::BFVContext / preComputeOnCPU / copyMemoryToGPU,
+// include/BFVcontext.cuh:13-1395, restated without NTL and without __constant__)
+// ===========================================================================
+namespace {
+
+struct Blob {
+    std::vector<uint8_t> bytes;
+    size_t add(const void* p, size_t n) {
+        size_t off = (bytes.size() + 255) & ~(size_t)255;
+        bytes.resize(off + n);
+        std::memcpy(bytes.data() + off, p, n);
+        return off;
+    }
+    template <class T>
+    size_t add(const std::vector<T>& v) { return add(v.data(), v.size() * sizeof(T)); }
+};
+
+std::vector<uint64_t> bitrev_powers(uint64_t root, uint64_t q, int logn) {
+    const uint64_t n = (uint64_t)1 << logn;
+    std::vector<uint64_t> out(n);
+    uint64_t cur = 1;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t r = 0, x = i;
+        for (int b = 0; b < logn; b++) { r = (r << 1) | (x & 1); x >>= 1; }
+        out[r] = cur;  // out[brv(i)] = root^i
+        cur = H::mulmod(cur, root, q);
+    }
+    return out;
+}
+
+struct HostBconv {
+    std::vector<uint64_t> hatinv, hatinvs, hat, alpha;
+    std::vector<double> inv;
+};
+
+// BaseConverter::init (include/BasisConv_QR.cuh:53-189)
+HostBconv make_bconv(const std::vector<uint64_t>& in, const std::vector<uint64_t>& out) {
+    HostBconv b;
+    const size_t nin = in.size(), nout = out.size();
+    b.hatinv.resize(nin); b.hatinvs.resize(nin); b.inv.resize(nin);
+    b.hat.resize(nin * nout); b.alpha.resize((nin + 1) * nout);
+    for (size_t i = 0; i < nin; i++) {
+        uint64_t h = 1;
+        for (size_t k = 0; k < nin; k++) if (k != i) h = H::mulmod(h, in[k] % in[i], in[i]);
+        b.hatinv[i] = nin > 1 ? H::invmod(h, in[i]) : 1;
+        b.hatinvs[i] = H::shoup(b.hatinv[i], in[i]);
+        b.inv[i] = 1.0 / (double)in[i];
+    }
+    for (size_t j = 0; j < nout; j++) {
+        const uint64_t o = out[j];
+        uint64_t bm = 1;
+        for (size_t i = 0; i < nin; i++) {
+            uint64_t h = 1;
+            for (size_t k = 0; k < nin; k++) if (k != i) h = H::mulmod(h, in[k] % o, o);
+            b.hat[j * nin + i] = h;
+            bm = H::mulmod(bm, in[i] % o, o);
+        }
+        for (size_t a = 0; a <= nin; a++) b.alpha[a * nout + j] = H::mulmod(a, bm, o);
+    }
+    return b;
+}
+
+void gaussian_cdt(double sigma, int bound, std::vector<uint64_t>& table) {
+    std::vector<long double> w(2 * bound + 1);
+    long double z = 0;
+    for (int x = -bound; x <= bound; x++) {
+        w[x + bound] = expl(-(long double)x * x / (2.0L * (long double)sigma * sigma));
+        z += w[x + bound];
+    }
+    table.assign(2 * bound + 1, 0);
+    long double acc = 0;
+    for (int k = 0; k < 2 * bound; k++) {
+        acc += w[k];
+        long double v = acc / z * 18446744073709551616.0L;
+        table[k] = v >= 18446744073709551615.0L ? UINT64_MAX : (uint64_t)v;
+    }
+    table[2 * bound] = UINT64_MAX;
+}
+
+}  // namespace
+
+static void build_context(Context& c, const kbfv_params& prm) {
+    KB_REQUIRE(prm.log_n >= 10 && prm.log_n <= 16, KBFV_ERR_INVALID, "log_n must be in [10, 16]");
+    KB_REQUIRE(prm.q_count >= 1 && prm.q_count <= (uint32_t)kMaxQ, KBFV_ERR_INVALID, "q_count out of range");
+    KB_REQUIRE(prm.p_count >= 1 && prm.p_count <= (uint32_t)kMaxP, KBFV_ERR_INVALID, "p_count out of range");
+    c.logn = (int)prm.log_n;
+    c.n = (uint64_t)1 << c.logn;
+    c.t = prm.plain_modulus;
+    c.nq = (int)prm.q_count;
+    c.np = (int)prm.p_count;
+    c.nr = c.nq + 1;
+    c.nt = (int)prm.t_count;
+    c.gamma = prm.gamma ? (int)prm.gamma : 1;
+    c.dnum = prm.dnum ? (int)prm.dnum : 1;
+    KB_REQUIRE(c.dnum <= c.nq, KBFV_ERR_INVALID, "dnum exceeds q_count");
+    c.alpha = (c.nq + c.dnum - 1) / c.dnum;
+    KB_REQUIRE(H::is_prime(c.t) && (c.t - 1) % (2 * c.n) == 0, KBFV_ERR_PARAMS,
+               "plain modulus must be a prime congruent to 1 mod 2N");
+
+    std::vector<uint64_t> P, Q;
+    if (prm.p) P.assign(prm.p, prm.p + c.np);
+    else P = H::primes_bits(c.n, (int)prm.p_bits, c.np, {});
+    KB_REQUIRE((int)P.size() == c.np, KBFV_ERR_PARAMS, "not enough special primes of the requested size");
+    if (prm.q) Q.assign(prm.q, prm.q + c.nq);
+    else Q = H::primes_bits(c.n, (int)prm.q_bits, c.nq, P);
+    KB_REQUIRE((int)Q.size() == c.nq, KBFV_ERR_PARAMS, "not enough ciphertext primes of the requested size");
+    uint64_t qmin = *std::min_element(Q.begin(), Q.end());
+    // R base: r_num = q_num + 1 primes below min q (include/BFVcontext.cuh:56-58)
+    std::vector<uint64_t> R = H::primes_below(c.n, qmin, c.nr);
+    KB_REQUIRE((int)R.size() == c.nr, KBFV_ERR_PARAMS, "not enough R primes below min q");
+
+    c.mods.clear();
+    c.mods.insert(c.mods.end(), Q.begin(), Q.end());
+    c.mods.insert(c.mods.end(), P.begin(), P.end());
+    c.mods.insert(c.mods.end(), R.begin(), R.end());
+    for (int i = 0; i < c.nt; i++) c.mods.push_back(prm.t_primes[i]);
+    c.mods.push_back(c.t);
+    const int nall = (int)c.mods.size();
+    KB_REQUIRE(nall <= kMaxPrimes, KBFV_ERR_INVALID, "too many primes");
+    for (int i = 0; i < nall; i++) {
+        const uint64_t q = c.mods[i];
+        KB_REQUIRE(H::is_prime(q) && q < ((uint64_t)1 << 62) && (q - 1) % (2 * c.n) == 0, KBFV_ERR_PARAMS,
+                   "every modulus must be a prime below 2^62 congruent to 1 mod 2N");
+        for (int j = 0; j < i; j++)
+            KB_REQUIRE(c.mods[j] != q || (i == nall - 1), KBFV_ERR_PARAMS, "moduli must be distinct");
+    }
+
+    DevConsts& dc = c.dc;
+    dc.logn = c.logn; dc.nq = c.nq; dc.np = c.np; dc.nr = c.nr; dc.nt = c.nt;
+    dc.dnum = c.dnum; dc.alpha = c.alpha; dc.npq = c.nq + c.np; dc.nqr = c.nq + c.nr;
+    dc.idx_p = c.nq; dc.idx_r = c.nq + c.np; dc.idx_t = c.nq + c.np + c.nr; dc.idx_pt = nall - 1;
+    dc.t = c.t;
+
+    Blob blob;
+    std::vector<uint64_t> mu_hi(nall), mu_lo(nall);
+    for (int i = 0; i < nall; i++) H::barrett_mu(c.mods[i], mu_hi[i], mu_lo[i]);
+    size_t o_mods = blob.add(c.mods), o_muh = blob.add(mu_hi), o_mul = blob.add(mu_lo);
+
+    // twiddles: fwd[i] = psi^brv(i); inv[i] = psi^-brv(i), inv[0] = n^-1, inv[1] *= n^-1
+    std::vector<tw_t> twf((size_t)nall << c.logn), twi((size_t)nall << c.logn);
+    for (int p = 0; p < nall; p++) {
+        const uint64_t q = c.mods[p];
+        const uint64_t psi = H::root_2n(q, c.n);
+        KB_REQUIRE(H::root_ok(psi, q, c.n), KBFV_ERR_PARAMS, "no primitive 2N-th root for a modulus");
+        const uint64_t ipsi = H::invmod(psi, q);
+        std::vector<uint64_t> f = bitrev_powers(psi, q, c.logn), g = bitrev_powers(ipsi, q, c.logn);
+        const uint64_t ninv = H::invmod(c.n % q, q);
+        g[0] = ninv;
+        g[1] = H::mulmod(g[1], ninv, q);
+        tw_t* tf = twf.data() + ((size_t)p << c.logn);
+        tw_t* ti = twi.data() + ((size_t)p << c.logn);
+        for (uint64_t i = 0; i < c.n; i++) {
+            tf[i].x = f[i]; tf[i].y = H::shoup(f[i], q);
+            ti[i].x = g[i]; ti[i].y = H::shoup(g[i], q);
+        }
+    }
+    size_t o_twf = blob.add(twf), o_twi = blob.add(twi);
+
+    HostBconv q2r = make_bconv(Q, R), r2q = make_bconv(R, Q);
+    c.h_q2r_hatinv = q2r.hatinv;
+    size_t o_q2r[5] = {blob.add(q2r.hatinv), blob.add(q2r.hatinvs), blob.add(q2r.hat), blob.add(q2r.alpha),
+                       blob.add(q2r.inv)};
+    size_t o_r2q[5] = {blob.add(r2q.hatinv), blob.add(r2q.hatinvs), blob.add(r2q.hat), blob.add(r2q.alpha),
+                       blob.add(r2q.inv)};
+
+    // t/Q scale-and-round constants (include/BFVcontext.cuh:1267-1389)
+    std::vector<double> sr_frac(c.nq);
+    std::vector<uint64_t> sr_c((size_t)c.nr * (c.nq + 1));
+    {
+        std::vector<uint64_t> qr(Q);
+        qr.insert(qr.end(), R.begin(), R.end());
+        const int nqr = (int)qr.size();
+        H::Big tR(c.t);
+        for (uint64_t r : R) tR.mul_word(r);
+        std::vector<H::Big> divs(nqr);
+        for (int i = 0; i < nqr; i++) {
+            const uint64_t si = qr[i];
+            uint64_t h = 1;
+            for (int k = 0; k < nqr; k++) if (k != i) h = H::mulmod(h, qr[k] % si, si);
+            H::Big v = tR;
+            v.mul_word(H::invmod(h, si));
+            if (i < c.nq) sr_frac[i] = (double)v.mod_word(si) / (double)si;
+            divs[i] = v.div_word(si);
+        }
+        for (int j = 0; j < c.nr; j++) {
+            for (int i = 0; i < c.nq; i++) sr_c[(size_t)j * (c.nq + 1) + i] = divs[i].mod_word(R[j]);
+            sr_c[(size_t)j * (c.nq + 1) + c.nq] = divs[c.nq + j].mod_word(R[j]);
+        }
+    }
+    size_t o_srf = blob.add(sr_frac), o_src = blob.add(sr_c);
+
+    // decrypt rounding constants (include/BFVcontext.cuh:1030-1156) and variant (1680-1717)
+    const uint64_t qmax = *std::max_element(Q.begin(), Q.end());
+    const int qmsb = H::bit_count(qmax), sizeqmsb = H::bit_count((uint64_t)c.nq), tmsb = H::bit_count(c.t);
+    const int hf = qmsb >> 1;
+    std::vector<uint64_t> dmt(c.nq, 0), dmts(c.nq, 0), dmbt(c.nq, 0), dmbts(c.nq, 0);
+    std::vector<double> dfr(c.nq, 0.0), dfrb(c.nq, 0.0);
+    for (int i = 0; i < c.nq; i++) {
+        const uint64_t qi = Q[i], hinv = q2r.hatinv[i];
+        const H::u128 big_t = (H::u128)c.t * hinv;
+        dmt[i] = (uint64_t)((big_t / qi) % c.t);
+        dmts[i] = H::shoup(dmt[i], c.t);
+        dfr[i] = (double)(uint64_t)(big_t % qi) / (double)qi;
+        if (qmsb + sizeqmsb >= 52) {
+            const uint64_t hb = (uint64_t)(((H::u128)hinv << hf) % qi);
+            const H::u128 bigb = (H::u128)c.t * hb;
+            dmbt[i] = (uint64_t)((bigb / qi) % c.t);
+            dmbts[i] = H::shoup(dmbt[i], c.t);
+            dfrb[i] = (double)(uint64_t)(bigb % qi) / (double)qi;
+        }
+    }
+    if (qmsb + sizeqmsb < 52) c.dec_variant = (qmsb + tmsb + sizeqmsb) < 52 ? 1 : 0;
+    else c.dec_variant = (hf + tmsb + sizeqmsb) < 52 ? 3 : 2;
+    dc.dec_variant = c.dec_variant;
+    dc.qmsbhf = hf;
+    size_t o_dec[6] = {blob.add(dmt), blob.add(dmts), blob.add(dmbt), blob.add(dmbts), blob.add(dfr), blob.add(dfrb)};
+
+    // delta * m (include/BFVcontext.cuh:881-926)
+    {
+        uint64_t qmt = 1;
+        for (uint64_t q : Q) qmt = H::mulmod(qmt, q % c.t, c.t);
+        dc.negq_mod_t = c.t - qmt;
+        dc.negq_mod_t_s = H::shoup(dc.negq_mod_t, c.t);
+    }
+    std::vector<uint64_t> tinv(c.nq), tinvs(c.nq);
+    for (int i = 0; i < c.nq; i++) {
+        tinv[i] = H::invmod(c.t % Q[i], Q[i]);
+        tinvs[i] = H::shoup(tinv[i], Q[i]);
+    }
+    size_t o_tinv = blob.add(tinv), o_tinvs = blob.add(tinvs);
+
+    // key switching: P mod q, P^-1 mod q, (P/p_k)^-1 mod p_k, (P/p_k) mod q
+    std::vector<uint64_t> pmq(c.nq), pinv(c.nq), pinvs(c.nq), phm((size_t)c.nq * c.np), phi(c.np), phis(c.np);
+    for (int i = 0; i < c.nq; i++) {
+        uint64_t pm = 1;
+        for (uint64_t p : P) pm = H::mulmod(pm, p % Q[i], Q[i]);
+        pmq[i] = pm;
+        pinv[i] = H::invmod(pm, Q[i]);
+        pinvs[i] = H::shoup(pinv[i], Q[i]);
+        for (int k = 0; k < c.np; k++) {
+            uint64_t h = 1;
+            for (int m = 0; m < c.np; m++) if (m != k) h = H::mulmod(h, P[m] % Q[i], Q[i]);
+            phm[(size_t)i * c.np + k] = h;
+        }
+    }
+    for (int k = 0; k < c.np; k++) {
+        uint64_t h = 1;
+        for (int m = 0; m < c.np; m++) if (m != k) h = H::mulmod(h, P[m] % P[k], P[k]);
+        phi[k] = H::invmod(h, P[k]);
+        phis[k] = H::shoup(phi[k], P[k]);
+    }
+    // digit lift constants: digit d covers primes [d*alpha, min((d+1)*alpha, nq))
+    const int npq = c.nq + c.np;
+    std::vector<uint64_t> dhi(c.nq), dhis(c.nq), dhm((size_t)c.dnum * npq * c.alpha, 0), dqm((size_t)c.dnum * npq, 0);
+    for (int d = 0; d < c.dnum; d++) {
+        const int lo = d * c.alpha, hi = std::min(lo + c.alpha, c.nq);
+        for (int j = lo; j < hi; j++) {
+            uint64_t h = 1;
+            for (int k = lo; k < hi; k++) if (k != j) h = H::mulmod(h, Q[k] % Q[j], Q[j]);
+            dhi[j] = H::invmod(h, Q[j]);
+            dhis[j] = H::shoup(dhi[j], Q[j]);
+        }
+        for (int m = 0; m < npq; m++) {
+            const uint64_t mod = c.mods[m];
+            uint64_t qm = 1;
+            for (int j = lo; j < hi; j++) {
+                uint64_t h = 1;
+                for (int k = lo; k < hi; k++) if (k != j) h = H::mulmod(h, Q[k] % mod, mod);
+                dhm[((size_t)d * npq + m) * c.alpha + (j - lo)] = h;
+                qm = H::mulmod(qm, Q[j] % mod, mod);
+            }
+            dqm[(size_t)d * npq + m] = qm;
+        }
+    }
+    size_t o_ks[10] = {blob.add(pmq), blob.add(pinv), blob.add(pinvs), blob.add(phi), blob.add(phis),
+                       blob.add(phm), blob.add(dhi), blob.add(dhis), blob.add(dhm), blob.add(dqm)};
+    std::vector<uint64_t> cdt;
+    gaussian_cdt(3.2, 19, cdt);
+    dc.gauss_bound = 19;
+    size_t o_cdt = blob.add(cdt);
+
+    KB_CHECK_CUDA(cudaGetDevice(&c.device));
+    KB_CHECK_CUDA(cudaMalloc(&c.pool, blob.bytes.size()));
+    KB_CHECK_CUDA(cudaMemcpy(c.pool, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice));
+    uint8_t* base = (uint8_t*)c.pool;
+    auto U = [&](size_t o) { return (const uint64_t*)(base + o); };
+    auto D = [&](size_t o) { return (const double*)(base + o); };
+    dc.mods = U(o_mods); dc.mu_hi = U(o_muh); dc.mu_lo = U(o_mul);
+    dc.tw_fwd = (const tw_t*)(base + o_twf); dc.tw_inv = (const tw_t*)(base + o_twi);
+    dc.q2r_hatinv = U(o_q2r[0]); dc.q2r_hatinvs = U(o_q2r[1]); dc.q2r_hat = U(o_q2r[2]);
+    dc.q2r_alpha = U(o_q2r[3]); dc.q2r_inv = D(o_q2r[4]);
+    dc.r2q_hatinv = U(o_r2q[0]); dc.r2q_hatinvs = U(o_r2q[1]); dc.r2q_hat = U(o_r2q[2]);
+    dc.r2q_alpha = U(o_r2q[3]); dc.r2q_inv = D(o_r2q[4]);
+    dc.sr_frac = D(o_srf); dc.sr_c = U(o_src);
+    dc.dec_mod_t = U(o_dec[0]); dc.dec_mod_t_s = U(o_dec[1]); dc.dec_modB_t = U(o_dec[2]);
+    dc.dec_modB_t_s = U(o_dec[3]); dc.dec_frac = D(o_dec[4]); dc.dec_fracB = D(o_dec[5]);
+    dc.tinv_q = U(o_tinv); dc.tinv_qs = U(o_tinvs);
+    dc.p_mod_q = U(o_ks[0]); dc.pinv_q = U(o_ks[1]); dc.pinv_qs = U(o_ks[2]); dc.phatinv_p = U(o_ks[3]);
+    dc.phatinv_ps = U(o_ks[4]); dc.phat_mod_q = U(o_ks[5]); dc.dig_hatinv = U(o_ks[6]);
+    dc.dig_hatinvs = U(o_ks[7]); dc.dig_hat_mod = U(o_ks[8]); dc.dig_q_mod = U(o_ks[9]);
+    dc.gauss_cdt = U(o_cdt);
+    KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.ptrs_event, cudaEventDisableTiming));
+}
+
+// ===========================================================================
+// launch helpers
+// ===========================================================================
+static inline cudaStream_t S(kbfv_stream s) { return (cudaStream_t)s; }
+static inline unsigned blocks_for(size_t total, unsigned threads) { return (unsigned)((total + threads - 1) / threads); }
+
+template <int LOGB, class Src, class Dst>
+static void launch_fwd_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
+    constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;
+    static bool configured = false;
+    if (!configured) {
+        KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_fwd_block_kernel<LOGB, Src, Dst>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        configured = true;
+    }
+    const int nblk = 1 << (logn - LOGB);
+    ntt_fwd_block_kernel<LOGB, Src, Dst><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
+        s, d, dc.tw_fwd, dc.mods, logn);
+}
+
+template <int LOGB, class Src, class Dst>
+static void launch_inv_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
+    constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;
+    static bool configured = false;
+    if (!configured) {
+        KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_inv_block_kernel<LOGB, Src, Dst>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        configured = true;
+    }
+    const int nblk = 1 << (logn - LOGB);
+    ntt_inv_block_kernel<LOGB, Src, Dst><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
+        s, d, dc.tw_inv, dc.mods, logn);
+}
+
+// Forward NTT of `rows` rows read through `s` and written through `d`.
+// For logn <= 14 one block kernel; for 15/16 a column pass (s -> d) then the
+// block kernel in place on d (d must also be readable).
+template <class Src, class Dst>
+static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    switch (dc.logn) {
+        case 10: launch_fwd_block<10>(dc, s, d, rows, 10, st); break;
+        case 11: launch_fwd_block<11>(dc, s, d, rows, 11, st); break;
+        case 12: launch_fwd_block<12>(dc, s, d, rows, 12, st); break;
+        case 13: launch_fwd_block<13>(dc, s, d, rows, 13, st); break;
+        case 14: launch_fwd_block<14>(dc, s, d, rows, 14, st); break;
+        case 15: {
+            const int total = rows << 14;
+            ntt_fwd_col_kernel<1, Src, Dst><<<blocks_for(total, 256), 256, 0, st>>>(s, d, dc.tw_fwd, dc.mods, 15, total);
+            launch_fwd_block<14>(dc, d, d, rows, 15, st);
+            break;
+        }
+        case 16: {
+            const int total = rows << 14;
+            ntt_fwd_col_kernel<2, Src, Dst><<<blocks_for(total, 256), 256, 0, st>>>(s, d, dc.tw_fwd, dc.mods, 16, total);
+            launch_fwd_block<14>(dc, d, d, rows, 16, st);
+            break;
+        }
+        default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
+    }
+    check_launch("ntt_fwd");
+}
+
+template <class Src, class Dst>
+static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    switch (dc.logn) {
+        case 10: launch_inv_block<10>(dc, s, d, rows, 10, st); break;
+        case 11: launch_inv_block<11>(dc, s, d, rows, 11, st); break;
+        case 12: launch_inv_block<12>(dc, s, d, rows, 12, st); break;
+        case 13: launch_inv_block<13>(dc, s, d, rows, 13, st); break;
+        case 14: launch_inv_block<14>(dc, s, d, rows, 14, st); break;
+        case 15: {
+            launch_inv_block<14>(dc, s, d, rows, 15, st);
+            const int total = rows << 14;
+            ntt_inv_col_kernel<1, Dst, Dst><<<blocks_for(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 15, total);
+            break;
+        }
+        case 16: {
+            launch_inv_block<14>(dc, s, d, rows, 16, st);
+            const int total = rows << 14;
+            ntt_inv_col_kernel<2, Dst, Dst><<<blocks_for(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
+            break;
+        }
+        default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
+    }
+    check_launch("ntt_inv");
+}
+
+static inline RowsIO rows_io(const DevConsts& dc, uint64_t* base, int p0, int period) {
+    return RowsIO{base, dc.logn, p0, period};
+}
+
+// bucketed MAX template dispatch for per-coefficient kernels
+#define DISPATCH_MAXQ(nq, MACRO) \
+    do {                         \
+        if ((nq) <= 8) { MACRO(8); }       \
+        else if ((nq) <= 16) { MACRO(16); } \
+        else { MACRO(24); }                 \
+    } while (0)
+
+static void launch_bconv(const DevConsts& dc, const BconvTables& tb, const uint64_t* in, uint64_t* out, int polys,
+                         size_t in_stride, size_t out_stride, cudaStream_t st) {
+    if (polys <= 0) return;
+    const int threads = 256;
+    dim3 grid((unsigned)((1u << dc.logn) / threads), (unsigned)polys);
+    const size_t sh = (size_t)tb.nin * tb.nout * 8;
+#define L_BC(M) bconv_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride)
+    DISPATCH_MAXQ(tb.nin, L_BC);
+#undef L_BC
+    check_launch("bconv");
+}
+
+// ===========================================================================
+// scratch
+// ===========================================================================
+static uint8_t* ensure_scratch(Context& c, size_t bytes) {
+    if (bytes > c.scratch_bytes) {
+        if (c.scratch) {
+            KB_CHECK_CUDA(cudaDeviceSynchronize());
+            KB_CHECK_CUDA(cudaFree(c.scratch));
+            c.scratch = nullptr;
+            c.scratch_bytes = 0;
+        }
+        size_t want = std::max(bytes, (size_t)64 << 20);
+        KB_CHECK_CUDA(cudaMalloc(&c.scratch, want));
+        c.scratch_bytes = want;
+    }
+    return (uint8_t*)c.scratch;
+}
+
+// ===========================================================================
+// multiply pipeline (HPS tensor + hybrid key switch), batched
+// ===========================================================================
+constexpr int kMaxBatch = 128;  // pointer tables ride in kernel parameters
+struct PtrBatch {
+    const uint64_t* a[kMaxBatch];
+    const uint64_t* b[kMaxBatch];
+    uint64_t* o[kMaxBatch];
+};
+
+struct MulScratch {
+    uint64_t *sa, *sb, *sc, *sd, *sd2, *se;
+    size_t bytes;
+};
+
+static MulScratch mul_scratch_layout(const Context& c, int count, uint8_t* base) {
+    const size_t limb = c.n * 8;
+    const int npq = c.nq + c.np, nqr = c.nq + c.nr;
+    size_t off = 0;
+    MulScratch m{};
+    auto take = [&](size_t limbs) {
+        uint64_t* p = (uint64_t*)(base ? base + off : nullptr);
+        off += limbs * limb;
+        return p;
+    };
+    m.sa = take((size_t)count * 4 * c.nq);
+    m.sb = take((size_t)count * 4 * c.nr);
+    m.sc = take((size_t)count * 3 * nqr);
+    m.sd = take((size_t)count * 2 * c.nq);
+    m.sd2 = take((size_t)count * c.dnum * npq);
+    m.se = take((size_t)count * 2 * npq);
+    m.bytes = off;
+    return m;
+}
+
+// Pointer arrays must be device-readable: the batched entry points pass
+// PtrBatch by value as a kernel parameter, so functors point into it through
+// this wrapper kernel-parameter view.
+struct PairQRowsP {
+    PtrBatch pb;
+    int logn, nq;
+    __device__ __forceinline__ int prime(int row) const { return row % nq; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        const int item = row / (4 * nq), w = row % (4 * nq), p = w / nq, l = w % nq;
+        const uint64_t* base = p < 2 ? pb.a[item] : pb.b[item];
+        return PtrRow{const_cast<uint64_t*>(base) + (((size_t)(p & 1) * nq + l) << logn)};
+    }
+};
+
+// K4 source: tensor product of the pair at limb l of Q|R, one of three outputs
+struct TensorRow {
+    const uint64_t *a1, *b1, *a2, *b2;
+    int k;
+    uint64_t q, mh, ml;
+    __device__ __forceinline__ uint64_t load(int j) const {
+        if (k == 0) return mul_mod(a1[j], a2[j], q, mh, ml);
+        if (k == 2) return mul_mod(b1[j], b2[j], q, mh, ml);
+        u128 acc = mul_wide(a1[j], b2[j]);
+        mac(acc, b1[j], a2[j]);
+        return barrett128(acc, q, mh, ml);
+    }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct TensorSrc {
+    PtrBatch pb;
+    const uint64_t* sb;  // NTT-form R limbs: [item][4][nr]
+    DevConsts dc;
+    __device__ __forceinline__ int prime(int row) const {
+        const int l = row % dc.nqr;
+        return l < dc.nq ? l : dc.idx_r + (l - dc.nq);
+    }
+    __device__ __forceinline__ TensorRow bind(int row) const {
+        const int nqr = dc.nqr, nq = dc.nq, nr = dc.nr, logn = dc.logn;
+        const int item = row / (3 * nqr), w = row % (3 * nqr), k = w / nqr, l = w % nqr;
+        TensorRow t;
+        t.k = k;
+        const int pi = l < nq ? l : dc.idx_r + (l - nq);
+        t.q = dc.mods[pi]; t.mh = dc.mu_hi[pi]; t.ml = dc.mu_lo[pi];
+        if (l < nq) {
+            const uint64_t* A = pb.a[item];
+            const uint64_t* B = pb.b[item];
+            t.a1 = A + ((size_t)l << logn); t.b1 = A + ((size_t)(nq + l) << logn);
+            t.a2 = B + ((size_t)l << logn); t.b2 = B + ((size_t)(nq + l) << logn);
+        } else {
+            const int r = l - nq;
+            const uint64_t* base = sb + (((size_t)item * 4 * nr) << logn);
+            t.a1 = base + ((size_t)(0 * nr + r) << logn); t.b1 = base + ((size_t)(1 * nr + r) << logn);
+            t.a2 = base + ((size_t)(2 * nr + r) << logn); t.b2 = base + ((size_t)(3 * nr + r) << logn);
+        }
+        return t;
+    }
+};
+
+// K6b source: inner product with the relinearisation key over Q|P
+struct KeyIPRow {
+    const uint64_t* dig;  // limb m of digit 0 (digit stride ds)
+    const uint64_t* key;  // limb m, half h of digit 0 (digit stride ks)
+    size_t ds, ks;
+    int dnum;
+    uint64_t q, mh, ml;
+    __device__ __forceinline__ uint64_t load(int j) const {
+        u128 acc{0, 0};
+        for (int d = 0; d < dnum; d++) mac(acc, dig[d * ds + j], key[d * ks + j]);
+        return barrett128(acc, q, mh, ml);
+    }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct KeyIPSrc {
+    const uint64_t* sd2;  // [item][dnum][npq]
+    const uint64_t* rlk;  // [dnum][2][npq]
+    DevConsts dc;
+    __device__ __forceinline__ int prime(int row) const { return row % dc.npq; }
+    __device__ __forceinline__ KeyIPRow bind(int row) const {
+        const int npq = dc.npq, logn = dc.logn;
+        const int item = row / (2 * npq), w = row % (2 * npq), h = w / npq, m = w % npq;
+        KeyIPRow r;
+        r.dig = sd2 + (((size_t)item * dc.dnum * npq + m) << logn);
+        r.key = rlk + (((size_t)h * npq + m) << logn);
+        r.ds = (size_t)npq << logn;
+        r.ks = (size_t)2 * npq << logn;
+        r.dnum = dc.dnum;
+        r.q = dc.mods[m]; r.mh = dc.mu_hi[m]; r.ml = dc.mu_lo[m];
+        return r;
+    }
+};
+
+// K7 source: mod down P|Q -> q_l and add the tensor term (coefficient form)
+struct ModDownAddRow {
+    const uint64_t* x;    // limb l of the Q|P polynomial
+    const uint64_t* xp;   // limb 0 of its P part
+    const uint64_t* add;  // limb l of the term to add, or null
+    const uint64_t* pmods;
+    const uint64_t* phatinv;
+    const uint64_t* phatinvs;
+    const uint64_t* phat;  // row l of (P/p_k) mod q_l
+    size_t limb;
+    int np;
+    uint64_t q, mh, ml, pinv, pinvs;
+    __device__ __forceinline__ uint64_t load(int j) const {
+        uint64_t conv;
+        if (np == 1) {
+            conv = barrett64(xp[j], q, mh);
+        } else {
+            u128 acc{0, 0};
+            for (int kk = 0; kk < np; kk++) {
+                uint64_t rb = shoup(xp[kk * limb + j], phatinv[kk], phatinvs[kk], pmods[kk]);
+                mac(acc, rb, phat[kk]);
+            }
+            conv = barrett128(acc, q, mh, ml);
+        }
+        uint64_t v = shoup(q - conv + x[j], pinv, pinvs, q);
+        if (add) v = add_mod(v, add[j], q);
+        return v;
+    }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct ModDownAddSrc {
+    const uint64_t* se;   // [item][2][npq]
+    const uint64_t* sd;   // [item][2][nq] or null
+    DevConsts dc;
+    __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
+    __device__ __forceinline__ ModDownAddRow bind(int row) const {
+        const int nq = dc.nq, npq = dc.npq, logn = dc.logn;
+        const int item = row / (2 * nq), w = row % (2 * nq), h = w / nq, l = w % nq;
+        ModDownAddRow r;
+        const uint64_t* poly = se + (((size_t)item * 2 + h) * npq << logn);
+        r.x = poly + ((size_t)l << logn);
+        r.xp = poly + ((size_t)nq << logn);
+        r.add = sd ? sd + (((size_t)(item * 2 + h) * nq + l) << logn) : nullptr;
+        r.pmods = dc.mods + dc.idx_p;
+        r.phatinv = dc.phatinv_p;
+        r.phatinvs = dc.phatinv_ps;
+        r.phat = dc.phat_mod_q + (size_t)l * dc.np;
+        r.limb = (size_t)1 << logn;
+        r.np = dc.np;
+        r.q = dc.mods[l]; r.mh = dc.mu_hi[l]; r.ml = dc.mu_lo[l];
+        r.pinv = dc.pinv_q[l]; r.pinvs = dc.pinv_qs[l];
+        return r;
+    }
+};
+
+struct OutCtDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
+    PtrBatch pb;
+    int logn, nq;
+    __device__ __forceinline__ int prime(int row) const { return row % nq; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        const int item = row / (2 * nq), w = row % (2 * nq);
+        return PtrRow{pb.o[item] + ((size_t)w << logn)};
+    }
+};
+
+// K5: scale-and-round to R, R -> Q, and (mode 1) the key-switch lift of a1*a2.
+// mode 0: all three outputs over Q to out0 ([item][3][nq]).
+// mode 1: a1*a2 lifted into sd2 ([item][dnum][npq]); cross, b1*b2 to sd ([item][2][nq]).
+template <int MAXQ>
+__global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__ sc, uint64_t* __restrict__ out0,
+                                uint64_t* __restrict__ sd, uint64_t* __restrict__ sd2, int mode) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int poly = blockIdx.y, item = poly / 3, which = poly % 3;
+    const uint64_t* src = sc + ((size_t)poly * c.nqr << c.logn);
+    uint64_t xq[MAXQ], xr[MAXQ + 1], rr[MAXQ + 1];
+#pragma unroll
+    for (int i = 0; i < MAXQ; i++)
+        if (i < c.nq) xq[i] = src[((size_t)i << c.logn) + k];
+#pragma unroll
+    for (int j = 0; j < MAXQ + 1; j++)
+        if (j < c.nr) xr[j] = src[((size_t)(c.nq + j) << c.logn) + k];
+    scale_round_coeff<MAXQ>(c, xq, xr, rr);
+    // R -> Q
+    const BconvTables tb = r2q_tables(c);
+    uint64_t y[MAXQ + 1];
+    const long long v = bconv_prep<MAXQ + 1>(y, rr, tb.nin, tb.in_mods, tb.hatinv, tb.hatinvs, tb.binv);
+#pragma unroll
+    for (int i = 0; i < MAXQ; i++) {
+        if (i < c.nq)
+            xq[i] = bconv_out<MAXQ + 1>(y, tb.nin, tb.hat + (size_t)i * tb.nin, tb.alpha[v * tb.nout + i],
+                                        c.mods[i], c.mu_hi[i], c.mu_lo[i]);
+    }
+    if (mode == 0) {
+        uint64_t* dst = out0 + ((size_t)poly * c.nq << c.logn);
+#pragma unroll
+        for (int i = 0; i < MAXQ; i++)
+            if (i < c.nq) dst[((size_t)i << c.logn) + k] = xq[i];
+    } else if (which == 0) {
+        modup_coeff<MAXQ>(c, xq, sd2 + ((size_t)item * c.dnum * c.npq << c.logn), k);
+    } else {
+        uint64_t* dst = sd + (((size_t)item * 2 + (which - 1)) * c.nq << c.logn);
+#pragma unroll
+        for (int i = 0; i < MAXQ; i++)
+            if (i < c.nq) dst[((size_t)i << c.logn) + k] = xq[i];
+    }
+}
+
+// INTT over Q of the four input polynomials, Q -> R, NTT over R, fused tensor +
+// INTT over Q|R: steps shared by kbfv_mul and the fused multiply-relinearise.
+static void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    // K1: INTT over Q of [a1, b1, a2, b2]
+    ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), count * 4 * dc.nq, st);
+    // K2: Q -> R (centred)
+    launch_bconv(dc, q2r_tables(dc), m.sa, m.sb, count * 4, (size_t)dc.nq << dc.logn, (size_t)dc.nr << dc.logn, st);
+    // K3: NTT over R in place
+    ntt_fwd(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr), count * 4 * dc.nr, st);
+    // K4: tensor (Q part from the NTT-form inputs, R part from K3) fused into INTT over Q|R
+    TensorSrc ts{pb, m.sb, dc};
+    ntt_inv(dc, ts, rows_io(dc, m.sc, 0, 1), count * 3 * dc.nqr, st);
+}
+
+static void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    const int threads = 128;
+    dim3 grid((unsigned)(c.n / threads), (unsigned)(count * 3));
+#define L_K5(M) k5_round_kernel<M><<<grid, threads, 0, st>>>(dc, m.sc, out0, m.sd, m.sd2, mode)
+    DISPATCH_MAXQ(dc.nq + 1, L_K5);
+#undef L_K5
+    check_launch("k5_round");
+}
+
+static void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb, int count, const MulScratch& m,
+                            cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    mul_front(c, pb, count, m, st);
+    k5_launch(c, count, m, nullptr, 1, st);
+    // K6a: NTT over Q|P of the lifted digits, in place
+    ntt_fwd(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq), count * dc.dnum * dc.npq, st);
+    // K6b: inner product with the key fused into INTT over Q|P
+    ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc}, rows_io(dc, m.se, 0, 1), count * 2 * dc.npq, st);
+    // K7: mod down + add (cross | b1b2) fused into NTT over Q, written to the outputs
+    ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
+}
+
+// rows (item, limb) of the first polynomial of consecutive 3-polynomial tensors
+struct TensorA2 {
+    const uint64_t* tz;
+    int logn, nq;
+    __device__ __forceinline__ int prime(int row) const { return row % nq; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        const int item = row / nq, l = row % nq;
+        return PtrRow{const_cast<uint64_t*>(tz) + (((size_t)item * 3 * nq + l) << logn)};
+    }
+};
+
+static void require_batchable(const Context& c) {
+    KB_REQUIRE(c.logn <= 14, KBFV_ERR_UNSUPPORTED, "the fused multiply pipeline supports N <= 16384");
+}
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+struct kbfv_context {
+    Context c;
+};
+
+static Context& CX(kbfv_context* h) {
+    if (!h) throw KbfvError(KBFV_ERR_INVALID, "null context");
+    return h->c;
+}
+
+extern "C" {
+
+const char* kbfv_last_error(void) { return g_last_error.c_str(); }
+const char* kbfv_version(void) { return "kbfv-b200 0.1 (sm_100a)"; }
+
+int kbfv_context_create(const kbfv_params* params, kbfv_context** out) {
+    return guarded([&] {
+        KB_REQUIRE(params && out, KBFV_ERR_INVALID, "null argument");
+        auto* h = new kbfv_context();
+        try {
+            build_context(h->c, *params);
+        } catch (...) {
+            if (h->c.pool) cudaFree(h->c.pool);
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int kbfv_context_create_reference(uint32_t log_n, kbfv_context** out) {
+    return guarded([&] {
+        // include/Params.cuh:31-145
+        static const uint64_t q14[] = {0x7FFE28001ULL, 0x7FFF18001ULL, 0x7FFF80001ULL, 0x7FFFB0001ULL};
+        static const uint64_t p14[] = {0xFFFFCA8001ULL, 0xFFFFE80001ULL};
+        static const uint64_t t4[] = {0xffffffffffc0001ULL, 0xfffffffff840001ULL, 0xfffffffff6a0001ULL,
+                                      0xfffffffff5a0001ULL};
+        static const uint64_t q15[] = {36028797001138177ULL, 36028797003563009ULL, 36028797003694081ULL,
+                                       36028797005135873ULL, 36028797005529089ULL, 36028797005856769ULL,
+                                       36028797009985537ULL, 36028797010444289ULL, 36028797012606977ULL,
+                                       36028797013000193ULL, 36028797013327873ULL, 36028797014376449ULL,
+                                       36028797014573057ULL, 36028797014704129ULL, 36028797017456641ULL};
+        static const uint64_t p15[] = {72057594037338113ULL};
+        kbfv_params p{};
+        p.log_n = log_n;
+        if (log_n == 14) {
+            p.plain_modulus = 23068673; p.q_count = 4; p.q = q14; p.p_count = 2; p.p = p14;
+            p.dnum = 2; p.t_count = 4; p.t_primes = t4; p.gamma = 2;
+        } else if (log_n == 15) {
+            p.plain_modulus = 0xC0001; p.q_count = 15; p.q = q15; p.p_count = 1; p.p = p15;
+            p.dnum = 15; p.t_count = 4; p.t_primes = t4; p.gamma = 4;
+        } else {
+            throw KbfvError(KBFV_ERR_PARAMS, "the reference defines parameter sets for logN 14 and 15 only");
+        }
+        int rc = kbfv_context_create(&p, out);
+        if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+    });
+}
+
+int kbfv_context_destroy(kbfv_context* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        Context& c = ctx->c;
+        cudaDeviceSynchronize();
+        if (c.pool) cudaFree(c.pool);
+        if (c.scratch) cudaFree(c.scratch);
+        if (c.ptrs_event) cudaEventDestroy(c.ptrs_event);
+        delete ctx;
+    });
+}
+
+int kbfv_context_info(const kbfv_context* ctx, uint64_t* n, uint32_t* q_count, uint32_t* p_count, uint32_t* r_count,
+                      uint32_t* t_count, uint32_t* dnum, uint32_t* alpha) {
+    return guarded([&] {
+        KB_REQUIRE(ctx, KBFV_ERR_INVALID, "null context");
+        const Context& c = ctx->c;
+        if (n) *n = c.n;
+        if (q_count) *q_count = c.nq;
+        if (p_count) *p_count = c.np;
+        if (r_count) *r_count = c.nr;
+        if (t_count) *t_count = c.nt;
+        if (dnum) *dnum = c.dnum;
+        if (alpha) *alpha = c.alpha;
+    });
+}
+
+int kbfv_context_primes(const kbfv_context* ctx, uint64_t* primes, uint32_t* count) {
+    return guarded([&] {
+        KB_REQUIRE(ctx && count, KBFV_ERR_INVALID, "null argument");
+        *count = (uint32_t)ctx->c.mods.size();
+        if (primes) std::memcpy(primes, ctx->c.mods.data(), ctx->c.mods.size() * 8);
+    });
+}
+
+uint64_t kbfv_context_plain_modulus(const kbfv_context* ctx) { return ctx ? ctx->c.t : 0; }
+int kbfv_context_decrypt_variant(const kbfv_context* ctx) { return ctx ? ctx->c.dec_variant : -1; }
+
+size_t kbfv_mul_relin_scratch_bytes(const kbfv_context* ctx, uint32_t count) {
+    if (!ctx) return 0;
+    return mul_scratch_layout(ctx->c, (int)std::min<uint32_t>(count, kMaxBatch), nullptr).bytes;
+}
+
+int kbfv_reserve(kbfv_context* ctx, uint32_t pairs) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const int chunk = (int)std::min<uint32_t>(std::max<uint32_t>(pairs, 1), kMaxBatch);
+        size_t need = mul_scratch_layout(c, chunk, nullptr).bytes;
+        // encryption work area: 4 polys x nq per item; secret/relin keygen: 2*(nq+np)
+        need = std::max(need, (size_t)chunk * 4 * c.nq * c.n * 8);
+        ensure_scratch(c, need);
+    });
+}
+
+int kbfv_ntt_fwd(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t prime0, uint32_t period,
+                 kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(d_rows && period >= 1 && prime0 + period <= c.mods.size(), KBFV_ERR_INVALID, "bad NTT rows");
+        RowsIO io = rows_io(c.dc, d_rows, (int)prime0, (int)period);
+        ntt_fwd(c.dc, io, io, (int)rows, S(stream));
+    });
+}
+
+int kbfv_ntt_inv(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t prime0, uint32_t period,
+                 kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(d_rows && period >= 1 && prime0 + period <= c.mods.size(), KBFV_ERR_INVALID, "bad NTT rows");
+        RowsIO io = rows_io(c.dc, d_rows, (int)prime0, (int)period);
+        ntt_inv(c.dc, io, io, (int)rows, S(stream));
+    });
+}
+
+int kbfv_bconv_q_to_r(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        launch_bconv(c.dc, q2r_tables(c.dc), d_in, d_out, (int)polys, (size_t)c.nq << c.logn,
+                     (size_t)c.nr << c.logn, S(stream));
+    });
+}
+
+int kbfv_bconv_r_to_q(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        launch_bconv(c.dc, r2q_tables(c.dc), d_in, d_out, (int)polys, (size_t)c.nr << c.logn,
+                     (size_t)c.nq << c.logn, S(stream));
+    });
+}
+
+int kbfv_tensor_qr(kbfv_context* ctx, const uint64_t* d_ct1, const uint64_t* d_ct2, uint64_t* d_out, uint32_t pairs,
+                   kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        const size_t total = (size_t)pairs * c.dc.nqr * c.n;
+        if (!total) return;
+        tensor_qr_kernel<<<blocks_for(total, 256), 256, 0, S(stream)>>>(c.dc, d_ct1, d_ct2, d_out, total);
+        check_launch("tensor_qr");
+    });
+}
+
+int kbfv_scale_round_qr_r(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                          kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!polys) return;
+        dim3 grid((unsigned)(c.n / 128), polys);
+#define L_SR(M) scale_round_kernel<M><<<grid, 128, 0, S(stream)>>>(c.dc, d_in, d_out)
+        DISPATCH_MAXQ(c.nq, L_SR);
+#undef L_SR
+        check_launch("scale_round");
+    });
+}
+
+int kbfv_decrypt_round(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!polys) return;
+        dim3 grid((unsigned)(c.n / 128), polys);
+#define L_DR(M) decrypt_round_kernel<M><<<grid, 128, 0, S(stream)>>>(c.dc, d_in, d_out)
+        DISPATCH_MAXQ(c.nq, L_DR);
+#undef L_DR
+        check_launch("decrypt_round");
+    });
+}
+
+int kbfv_delta_m(kbfv_context* ctx, const uint64_t* d_m, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        const size_t total = (size_t)polys * c.nq * c.n;
+        if (!total) return;
+        delta_m_kernel<<<blocks_for(total, 256), 256, 0, S(stream)>>>(c.dc, d_m, d_out, total);
+        check_launch("delta_m");
+    });
+}
+
+int kbfv_modup(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!polys) return;
+        dim3 grid((unsigned)(c.n / 128), polys);
+#define L_MU(M) modup_kernel<M><<<grid, 128, 0, S(stream)>>>(c.dc, d_in, d_out)
+        DISPATCH_MAXQ(c.nq, L_MU);
+#undef L_MU
+        check_launch("modup");
+    });
+}
+
+int kbfv_moddown(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!polys) return;
+        dim3 grid((unsigned)(c.n / 128), polys);
+        moddown_kernel<<<grid, 128, 0, S(stream)>>>(c.dc, d_in, d_out);
+        check_launch("moddown");
+    });
+}
+
+// ---- randomness helpers ----
+static void hsalsa_host(const uint8_t key[32], const uint8_t nonce16[16], uint32_t out[8]);
+static SalsaKey subkey_for(const uint8_t seed[32], uint32_t domain, uint32_t sub) {
+    uint8_t n16[16] = {0};
+    for (int i = 0; i < 4; i++) { n16[i] = (uint8_t)(domain >> (8 * i)); n16[4 + i] = (uint8_t)(sub >> (8 * i)); }
+    SalsaKey k;
+    hsalsa_host(seed, n16, k.k);
+    static const char* sig = "expand 32-byte k";
+    for (int i = 0; i < 4; i++) std::memcpy(&k.sigma[i], sig + 4 * i, 4);
+    return k;
+}
+
+static inline uint32_t rl(uint32_t u, int c) { return (u << c) | (u >> (32 - c)); }
+static inline uint32_t ld32(const uint8_t* x) {
+    return (uint32_t)x[0] | ((uint32_t)x[1] << 8) | ((uint32_t)x[2] << 16) | ((uint32_t)x[3] << 24);
+}
+static void hsalsa_host(const uint8_t key[32], const uint8_t nonce16[16], uint32_t out[8]) {
+    static const char* sig = "expand 32-byte k";
+    uint32_t x[16];
+    x[0] = ld32((const uint8_t*)sig); x[5] = ld32((const uint8_t*)sig + 4);
+    x[10] = ld32((const uint8_t*)sig + 8); x[15] = ld32((const uint8_t*)sig + 12);
+    for (int i = 0; i < 4; i++) { x[1 + i] = ld32(key + 4 * i); x[11 + i] = ld32(key + 16 + 4 * i); }
+    for (int i = 0; i < 4; i++) x[6 + i] = ld32(nonce16 + 4 * i);
+    for (int r = 0; r < 10; r++) {
+        x[4] ^= rl(x[0] + x[12], 7);   x[8] ^= rl(x[4] + x[0], 9);
+        x[12] ^= rl(x[8] + x[4], 13);  x[0] ^= rl(x[12] + x[8], 18);
+        x[9] ^= rl(x[5] + x[1], 7);    x[13] ^= rl(x[9] + x[5], 9);
+        x[1] ^= rl(x[13] + x[9], 13);  x[5] ^= rl(x[1] + x[13], 18);
+        x[14] ^= rl(x[10] + x[6], 7);  x[2] ^= rl(x[14] + x[10], 9);
+        x[6] ^= rl(x[2] + x[14], 13);  x[10] ^= rl(x[6] + x[2], 18);
+        x[3] ^= rl(x[15] + x[11], 7);  x[7] ^= rl(x[3] + x[15], 9);
+        x[11] ^= rl(x[7] + x[3], 13);  x[15] ^= rl(x[11] + x[7], 18);
+        x[1] ^= rl(x[0] + x[3], 7);    x[2] ^= rl(x[1] + x[0], 9);
+        x[3] ^= rl(x[2] + x[1], 13);   x[0] ^= rl(x[3] + x[2], 18);
+        x[6] ^= rl(x[5] + x[4], 7);    x[7] ^= rl(x[6] + x[5], 9);
+        x[4] ^= rl(x[7] + x[6], 13);   x[5] ^= rl(x[4] + x[7], 18);
+        x[11] ^= rl(x[10] + x[9], 7);  x[8] ^= rl(x[11] + x[10], 9);
+        x[9] ^= rl(x[8] + x[11], 13);  x[10] ^= rl(x[9] + x[8], 18);
+        x[12] ^= rl(x[15] + x[14], 7); x[13] ^= rl(x[12] + x[15], 9);
+        x[14] ^= rl(x[13] + x[12], 13); x[15] ^= rl(x[14] + x[13], 18);
+    }
+    out[0] = x[0]; out[1] = x[5]; out[2] = x[10]; out[3] = x[15];
+    out[4] = x[6]; out[5] = x[7]; out[6] = x[8]; out[7] = x[9];
+}
+
+enum { DOM_SK = 1, DOM_PK_A = 2, DOM_PK_E = 3, DOM_RLK_A = 4, DOM_RLK_E = 5, DOM_ENC_V = 6, DOM_ENC_E0 = 7,
+       DOM_ENC_E1 = 8 };
+
+static void sample_small(Context& c, const uint8_t seed[32], uint32_t domain, uint64_t id0, int kind, int prime0,
+                         int limbs, uint64_t* out, size_t item_stride, int items, cudaStream_t st) {
+    SalsaKey k = subkey_for(seed, domain, 0);
+    const int per = kind == 0 ? 16 : 8;
+    const size_t total = (size_t)items * (c.n / per);
+    if (kind == 0)
+        sample_small_kernel<0><<<blocks_for(total, 128), 128, 0, st>>>(c.dc, k, id0, prime0, limbs, out, item_stride, items);
+    else
+        sample_small_kernel<1><<<blocks_for(total, 128), 128, 0, st>>>(c.dc, k, id0, prime0, limbs, out, item_stride, items);
+    check_launch("sample_small");
+}
+
+static void sample_uniform(Context& c, const uint8_t seed[32], uint32_t domain, uint32_t sub, uint64_t id0, int prime0,
+                           int limbs, uint64_t* out, size_t item_stride, int items, cudaStream_t st) {
+    SalsaKey k = subkey_for(seed, domain, sub);
+    const size_t total = (size_t)items * limbs * c.n / 4;
+    sample_uniform_kernel<<<blocks_for(total, 128), 128, 0, st>>>(c.dc, k, id0, prime0, limbs, out, item_stride, items);
+    check_launch("sample_uniform");
+}
+
+int kbfv_keygen_secret(kbfv_context* ctx, const uint8_t seed[32], int secret_kind, uint32_t h, uint64_t* d_sk,
+                       kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(seed && d_sk, KBFV_ERR_INVALID, "null argument");
+        const int npq = c.nq + c.np;
+        cudaStream_t st = S(stream);
+        if (secret_kind == 1) {
+            KB_CHECK_CUDA(cudaMemsetAsync(d_sk, 0, (size_t)npq * c.n * 8, st));
+            SalsaKey k = subkey_for(seed, DOM_SK, 0);
+            sample_hwt_kernel<<<1, 32, 0, st>>>(c.dc, k, 0, (int)h, 0, npq, d_sk, 0, 1);
+            check_launch("sample_hwt");
+        } else {
+            sample_small(c, seed, DOM_SK, 0, 0, 0, npq, d_sk, 0, 1, st);
+        }
+        RowsIO io = rows_io(c.dc, d_sk, 0, npq);
+        ntt_fwd(c.dc, io, io, npq, st);
+    });
+}
+
+int kbfv_keygen_public(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint64_t* d_pk,
+                       kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(seed && d_sk && d_pk, KBFV_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        uint64_t* a = d_pk;
+        uint64_t* b = d_pk + lq;
+        sample_uniform(c, seed, DOM_PK_A, 0, 0, 0, c.nq, a, 0, 1, st);
+        sample_small(c, seed, DOM_PK_E, 0, 1, 0, c.nq, b, 0, 1, st);
+        RowsIO io = rows_io(c.dc, b, 0, c.nq);
+        ntt_fwd(c.dc, io, io, c.nq, st);
+        pk_combine_kernel<<<blocks_for(lq, 256), 256, 0, st>>>(c.dc, a, d_sk, b, lq);
+        check_launch("pk_combine");
+    });
+}
+
+int kbfv_keygen_relin(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint64_t* d_rlk,
+                      kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(seed && d_sk && d_rlk, KBFV_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        const int npq = c.nq + c.np;
+        const size_t lpq = (size_t)npq * c.n;
+        for (int d = 0; d < c.dnum; d++) {
+            uint64_t* a = d_rlk + (size_t)d * 2 * lpq;
+            uint64_t* b = a + lpq;
+            sample_uniform(c, seed, DOM_RLK_A, (uint32_t)d, 0, 0, npq, a, 0, 1, st);
+            SalsaKey k = subkey_for(seed, DOM_RLK_E, (uint32_t)d);
+            const size_t total = c.n / 8;
+            sample_small_kernel<1><<<blocks_for(total, 128), 128, 0, st>>>(c.dc, k, 0, 0, npq, b, 0, 1);
+            check_launch("sample_gauss");
+            RowsIO io = rows_io(c.dc, b, 0, npq);
+            ntt_fwd(c.dc, io, io, npq, st);
+            rlk_combine_kernel<<<blocks_for(lpq, 256), 256, 0, st>>>(c.dc, a, d_sk, b, d, lpq);
+            check_launch("rlk_combine");
+        }
+    });
+}
+
+int kbfv_encode(kbfv_context* ctx, const uint64_t* d_slots, uint64_t* d_m, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!count) return;
+        if (d_m != d_slots)
+            KB_CHECK_CUDA(cudaMemcpyAsync(d_m, d_slots, (size_t)count * c.n * 8, cudaMemcpyDeviceToDevice, S(stream)));
+        RowsIO io = rows_io(c.dc, d_m, c.dc.idx_pt, 1);
+        ntt_inv(c.dc, io, io, (int)count, S(stream));
+    });
+}
+
+int kbfv_decode(kbfv_context* ctx, const uint64_t* d_m, uint64_t* d_slots, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!count) return;
+        if (d_m != d_slots)
+            KB_CHECK_CUDA(cudaMemcpyAsync(d_slots, d_m, (size_t)count * c.n * 8, cudaMemcpyDeviceToDevice, S(stream)));
+        RowsIO io = rows_io(c.dc, d_slots, c.dc.idx_pt, 1);
+        ntt_fwd(c.dc, io, io, (int)count, S(stream));
+    });
+}
+
+// values (< t) as polynomial coefficients, replicated over Q and transformed
+struct ReplicateSrc {
+    const uint64_t* vals;
+    int logn, nq;
+    __device__ __forceinline__ int prime(int row) const { return row % nq; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        return PtrRow{const_cast<uint64_t*>(vals) + ((size_t)(row / nq) << logn)};
+    }
+};
+
+int kbfv_encode_ntt(kbfv_context* ctx, const uint64_t* d_vals, uint64_t* d_pt_ntt, uint32_t count,
+                    kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        if (!count) return;
+        require_batchable(c);
+        ntt_fwd(c.dc, ReplicateSrc{d_vals, c.logn, c.nq}, rows_io(c.dc, d_pt_ntt, 0, c.nq), (int)(count * c.nq),
+                S(stream));
+    });
+}
+
+int kbfv_encrypt(kbfv_context* ctx, const uint8_t seed[32], uint64_t enc_id, const uint64_t* d_pk, const uint64_t* d_m,
+                 uint64_t* d_ct, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(seed && d_pk && d_m && d_ct, KBFV_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            uint64_t* work = (uint64_t*)ensure_scratch(c, (size_t)cnt * 4 * lq * 8);
+            const uint64_t id0 = enc_id + off;
+            // [v | e0 | e1 | dm] per item
+            sample_small(c, seed, DOM_ENC_V, id0, 0, 0, c.nq, work, 4 * lq, cnt, st);
+            sample_small(c, seed, DOM_ENC_E0, id0, 1, 0, c.nq, work + lq, 4 * lq, cnt, st);
+            sample_small(c, seed, DOM_ENC_E1, id0, 1, 0, c.nq, work + 2 * lq, 4 * lq, cnt, st);
+            for (int i = 0; i < cnt; i++) {
+                const size_t tot = lq;
+                delta_m_kernel<<<blocks_for(tot, 256), 256, 0, st>>>(c.dc, d_m + (size_t)(off + i) * c.n,
+                                                                      work + (size_t)i * 4 * lq + 3 * lq, tot);
+            }
+            check_launch("delta_m");
+            RowsIO io = rows_io(c.dc, work, 0, c.nq);
+            ntt_fwd(c.dc, io, io, cnt * 4 * c.nq, st);
+            const size_t total = (size_t)cnt * lq;
+            enc_combine_kernel<<<blocks_for(total, 256), 256, 0, st>>>(c.dc, d_pk, work, d_ct + (size_t)off * 2 * lq, total);
+            check_launch("enc_combine");
+        }
+    });
+}
+
+// decrypt: INTT over Q of (a*s + b), then the rounding
+struct DecSrc {
+    const uint64_t* ct;
+    const uint64_t* sk;
+    DevConsts dc;
+    struct Row {
+        const uint64_t *a, *b, *s;
+        uint64_t q, mh, ml;
+        __device__ __forceinline__ uint64_t load(int j) const { return add_mod(mul_mod(a[j], s[j], q, mh, ml), b[j], q); }
+        __device__ __forceinline__ void store(int, uint64_t) const {}
+    };
+    __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
+    __device__ __forceinline__ Row bind(int row) const {
+        const int item = row / dc.nq, l = row % dc.nq;
+        const size_t lq = (size_t)dc.nq << dc.logn;
+        Row r;
+        r.a = ct + item * 2 * lq + ((size_t)l << dc.logn);
+        r.b = r.a + lq;
+        r.s = sk + ((size_t)l << dc.logn);
+        r.q = dc.mods[l]; r.mh = dc.mu_hi[l]; r.ml = dc.mu_lo[l];
+        return r;
+    }
+};
+
+int kbfv_decrypt(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, uint64_t* d_m, uint32_t count,
+                 kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(d_sk && d_ct && d_m, KBFV_ERR_INVALID, "null argument");
+        require_batchable(c);
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            uint64_t* work = (uint64_t*)ensure_scratch(c, (size_t)cnt * lq * 8);
+            ntt_inv(c.dc, DecSrc{d_ct + (size_t)off * 2 * lq, d_sk, c.dc}, rows_io(c.dc, work, 0, c.nq), cnt * c.nq, st);
+            dim3 grid((unsigned)(c.n / 128), (unsigned)cnt);
+#define L_DR(M) decrypt_round_kernel<M><<<grid, 128, 0, st>>>(c.dc, work, d_m + (size_t)off * c.n)
+            DISPATCH_MAXQ(c.nq, L_DR);
+#undef L_DR
+            check_launch("decrypt_round");
+        }
+    });
+}
+
+int kbfv_add(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64_t* d_out, uint32_t count,
+             kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        const size_t total = (size_t)count * 2 * c.nq * c.n;
+        if (!total) return;
+        add_kernel<<<blocks_for(total, 256), 256, 0, S(stream)>>>(c.dc, d_x, d_y, d_out, total, c.nq);
+        check_launch("add");
+    });
+}
+
+int kbfv_mul_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_pt_ntt, uint64_t* d_out, uint32_t count,
+                   kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        const size_t total = (size_t)count * 2 * c.nq * c.n;
+        if (!total) return;
+        mul_plain_kernel<<<blocks_for(total, 256), 256, 0, S(stream)>>>(c.dc, d_ct, d_pt_ntt, d_out, total);
+        check_launch("mul_plain");
+    });
+}
+
+static PtrBatch make_batch(const uint64_t* const* a, const uint64_t* const* b, uint64_t* const* o, int cnt) {
+    PtrBatch pb;
+    std::memset(&pb, 0, sizeof pb);
+    for (int i = 0; i < cnt; i++) {
+        pb.a[i] = a[i];
+        pb.b[i] = b[i];
+        pb.o[i] = o ? o[i] : nullptr;
+    }
+    return pb;
+}
+
+int kbfv_mul(kbfv_context* ctx, const uint64_t* d_ct1, const uint64_t* d_ct2, uint64_t* d_tensor, uint32_t count,
+             kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            std::vector<const uint64_t*> A(cnt), B(cnt);
+            for (int i = 0; i < cnt; i++) {
+                A[i] = d_ct1 + (size_t)(off + i) * 2 * lq;
+                B[i] = d_ct2 + (size_t)(off + i) * 2 * lq;
+            }
+            PtrBatch pb = make_batch(A.data(), B.data(), nullptr, cnt);
+            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            uint64_t* out = d_tensor + (size_t)off * 3 * lq;
+            mul_front(c, pb, cnt, m, st);
+            k5_launch(c, cnt, m, out, 0, st);
+            RowsIO io = rows_io(c.dc, out, 0, c.nq);
+            ntt_fwd(c.dc, io, io, cnt * 3 * c.nq, st);
+        }
+    });
+}
+
+int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_tensor, uint64_t* d_ct, uint32_t count,
+                     kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_rlk, KBFV_ERR_NO_KEY, "relinearisation key missing");
+        cudaStream_t st = S(stream);
+        const DevConsts& dc = c.dc;
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            const uint64_t* tz = d_tensor + (size_t)off * 3 * lq;
+            uint64_t* out = d_ct + (size_t)off * 2 * lq;
+            // INTT of a1*a2 into sa: rows (item, limb) read from the tensor's first poly
+            ntt_inv(dc, TensorA2{tz, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), cnt * dc.nq, st);
+            dim3 grid((unsigned)(c.n / 128), (unsigned)cnt);
+#define L_MU(M) modup_kernel<M><<<grid, 128, 0, st>>>(dc, m.sa, m.sd2)
+            DISPATCH_MAXQ(dc.nq, L_MU);
+#undef L_MU
+            check_launch("modup");
+            ntt_fwd(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq), cnt * dc.dnum * dc.npq, st);
+            ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc}, rows_io(dc, m.se, 0, 1), cnt * 2 * dc.npq, st);
+            std::vector<uint64_t*> O(cnt);
+            std::vector<const uint64_t*> Z(cnt);
+            for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
+            PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
+            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            // add [cross | b1b2] (NTT form)
+            for (int i = 0; i < cnt; i++) {
+                const size_t tot = 2 * lq;
+                add_kernel<<<blocks_for(tot, 256), 256, 0, st>>>(dc, out + (size_t)i * 2 * lq, tz + (size_t)i * 3 * lq + lq,
+                                                                 out + (size_t)i * 2 * lq, tot, dc.nq);
+            }
+            check_launch("relin_add");
+        }
+    });
+}
+
+int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* const* ct_a,
+                         const uint64_t* const* ct_b, uint64_t* const* out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_rlk, KBFV_ERR_NO_KEY, "relinearisation key missing");
+        KB_REQUIRE(ct_a && ct_b && out, KBFV_ERR_INVALID, "null pointer array");
+        cudaStream_t st = S(stream);
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            PtrBatch pb = make_batch(ct_a + off, ct_b + off, out + off, cnt);
+            for (int i = 0; i < cnt; i++)
+                KB_REQUIRE(pb.a[i] && pb.b[i] && pb.o[i], KBFV_ERR_INVALID, "null ciphertext pointer");
+            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            mul_relin_chunk(c, d_rlk, pb, cnt, m, st);
+        }
+    });
+}
+
+int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                   uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        const size_t lq = (size_t)c.nq * c.n;
+        std::vector<const uint64_t*> A(count), B(count);
+        std::vector<uint64_t*> O(count);
+        for (uint32_t i = 0; i < count; i++) {
+            A[i] = d_ct_a + (size_t)i * 2 * lq;
+            B[i] = d_ct_b + (size_t)i * 2 * lq;
+            O[i] = d_out + (size_t)i * 2 * lq;
+        }
+        int rc = kbfv_mul_relin_batch(ctx, d_rlk, A.data(), B.data(), O.data(), count, stream);
+        if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+    });
+}
+
+int kbfv_noise_budget(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, double* bits) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(d_sk && d_ct && bits, KBFV_ERR_INVALID, "null argument");
+        const size_t lq = (size_t)c.nq * c.n;
+        uint64_t* work = (uint64_t*)ensure_scratch(c, lq * 8);
+        ntt_inv(c.dc, DecSrc{d_ct, d_sk, c.dc}, rows_io(c.dc, work, 0, c.nq), c.nq, 0);
+        std::vector<uint64_t> x(lq);
+        KB_CHECK_CUDA(cudaMemcpy(x.data(), work, lq * 8, cudaMemcpyDeviceToHost));
+        // CRT reconstruction of t * x, centred; budget = log2 Q - log2 max - 1
+        H::Big Q(1);
+        for (int i = 0; i < c.nq; i++) Q.mul_word(c.mods[i]);
+        H::Big half = Q.div_word(2);
+        std::vector<H::Big> hats(c.nq);
+        for (int i = 0; i < c.nq; i++) {
+            hats[i] = H::Big(1);
+            for (int k = 0; k < c.nq; k++) if (k != i) hats[i].mul_word(c.mods[k]);
+        }
+        double worst = -INFINITY;
+        for (uint64_t k = 0; k < c.n; k++) {
+            H::Big z(0);
+            for (int i = 0; i < c.nq; i++) {
+                const uint64_t q = c.mods[i];
+                uint64_t y = H::mulmod(H::mulmod(x[(size_t)i * c.n + k], c.t % q, q), c.h_q2r_hatinv[i], q);
+                H::Big term = hats[i];
+                term.mul_word(y);
+                z.add(term);
+            }
+            while (z.cmp(Q) >= 0) z.sub(Q);
+            if (z.cmp(half) > 0) { H::Big w = Q; w.sub(z); z = w; }
+            worst = std::max(worst, z.log2v());
+        }
+        *bits = Q.log2v() - worst - 1.0;
+    });
+}
+
+int kbfv_salsa20_stream(const uint8_t key[32], const uint8_t nonce[24], uint64_t block0, uint8_t* d_out, size_t nbytes,
+                        int compat, kbfv_stream stream) {
+    return guarded([&] {
+        KB_REQUIRE(key && nonce && d_out, KBFV_ERR_INVALID, "null argument");
+        SalsaKey k;
+        uint32_t n0, n1;
+        size_t len = nbytes;
+        if (compat) {
+            // the reference's VecCrypt: zero constants, raw key, nonce word 1 always 0,
+            // partial tail block left zero (include/RNG.cuh:18-51, include/RNG_impl.cuh:70-176)
+            for (int i = 0; i < 8; i++) k.k[i] = ld32(key + 4 * i);
+            for (int i = 0; i < 4; i++) k.sigma[i] = 0;
+            n0 = ld32(nonce);
+            n1 = 0;
+            KB_CHECK_CUDA(cudaMemsetAsync(d_out, 0, nbytes, S(stream)));
+            len = nbytes / 64 * 64;
+        } else {
+            hsalsa_host(key, nonce, k.k);
+            static const char* sig = "expand 32-byte k";
+            for (int i = 0; i < 4; i++) std::memcpy(&k.sigma[i], sig + 4 * i, 4);
+            n0 = ld32(nonce + 16);
+            n1 = ld32(nonce + 20);
+        }
+        if (!len) return;
+        const size_t blocks = (len + 63) / 64;
+        salsa_stream_kernel<<<blocks_for(blocks, 128), 128, 0, S(stream)>>>(k, n0, n1, block0, d_out, len);
+        check_launch("salsa20");
+    });
+}
+
+}  // extern "C"

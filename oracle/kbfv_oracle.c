@@ -1013,12 +1013,15 @@ void orc_gaussian_cdt(double sigma, int bound, uint64_t* table) {
     table[2 * bound] = UINT64_MAX;
 }
 
+/* nonce = [domain | sub | 0 | 0 | id_lo | id_hi] (little-endian words): the
+ * HSalsa20 subkey depends on (key, domain, sub) only; the item id is the
+ * Salsa20 nonce, so every item of a batch draws an independent stream. */
 static void make_nonce(uint32_t domain, uint64_t id, uint32_t sub, uint8_t nonce[24]) {
     memset(nonce, 0, 24);
     st32(nonce, domain);
     st32(nonce + 4, sub);
-    st32(nonce + 8, (uint32_t)id);
-    st32(nonce + 12, (uint32_t)(id >> 32));
+    st32(nonce + 16, (uint32_t)id);
+    st32(nonce + 20, (uint32_t)(id >> 32));
 }
 
 static uint8_t* stream_bytes(const uint8_t key[32], uint32_t domain, uint64_t id, uint32_t sub, size_t nbytes) {

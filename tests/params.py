@@ -1,0 +1,24 @@
+"""Parameter sets shared by the tests (prime lists come from the oracle's generator)."""
+import functools
+
+import oracle
+
+T65537 = 65537
+
+
+@functools.lru_cache(maxsize=None)
+def chain(log_n: int, bits: int, count: int):
+    return tuple(oracle.primes_bits(1 << log_n, bits, count))
+
+
+@functools.lru_cache(maxsize=None)
+def c3_primes():
+    """N=16384, 7 x 60-bit ciphertext primes + 1 special prime (largest first)."""
+    ps = chain(14, 60, 8)
+    return list(ps[1:8]), [ps[0]]
+
+
+@functools.lru_cache(maxsize=None)
+def small_primes(log_n: int = 12, nq: int = 3, np_: int = 1, bits: int = 50):
+    ps = chain(log_n, bits, nq + np_)
+    return list(ps[np_:np_ + nq]), list(ps[:np_])

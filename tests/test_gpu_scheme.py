@@ -1,0 +1,143 @@
+"""Keys, encryption, decryption and the multiply path on the B200 vs the oracle.
+
+Bit-exact ciphertext parity (same seed -> same keys and ciphertexts), exact
+decryption of m1*m2 mod t, and batch-vs-alone determinism."""
+import numpy as np
+import pytest
+
+from tests.gpu_util import c3_pair, dev, host, small_pair
+
+pytestmark = pytest.mark.gpu
+
+T = 65537
+SEED = bytes(range(32))
+
+
+def setup(ctx, orc, kind=0):
+    import kunpbfv_b200 as kb
+    sk = kb.SecretKey(ctx, SEED, kind=kind)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    osk = orc.keygen_secret(SEED, kind)
+    return sk, sch, osk
+
+
+@pytest.mark.parametrize("which", ["c3", "small", "dnum2"])
+def test_keys_bit_exact(which):
+    ctx, orc = {"c3": c3_pair, "small": lambda: small_pair(12, 3, 1, 50),
+                "dnum2": lambda: small_pair(12, 4, 2, 45, 2)}[which]()
+    sk, sch, osk = setup(ctx, orc)
+    assert np.array_equal(host(sk.sx_device).reshape(osk.shape), osk)
+    opk = orc.keygen_public(SEED, osk)
+    assert np.array_equal(host(sch.publicKey).reshape(opk.shape), opk)
+    orlk = orc.keygen_relin(SEED, osk)
+    assert np.array_equal(host(sch.rlk).reshape(orlk.shape), orlk)
+
+
+def test_hwt_secret_bit_exact():
+    import kunpbfv_b200 as kb
+    ctx, orc = small_pair(12, 3, 1, 50)
+    sk = kb.SecretKey(ctx, SEED, kind=1, h=64)
+    assert np.array_equal(host(sk.sx_device).reshape(-1, ctx.N), orc.keygen_secret(SEED, 1, 64))
+
+
+def test_encrypt_decrypt_bit_exact():
+    import kunpbfv_b200 as kb
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    opk = orc.keygen_public(SEED, osk)
+    rng = np.random.default_rng(2)
+    v = rng.integers(0, T, size=(3, ctx.N), dtype=np.uint64)
+    m = host(ctx.encode(dev(v))).reshape(v.shape)
+    ct = sch.encryptMsg(kb.Plaintext(ctx, dev(m)), enc_id=100)
+    got = host(ct.cipher_device).reshape(3, 2, ctx.q_count, ctx.N)
+    for i in range(3):
+        assert np.array_equal(got[i], orc.encrypt(SEED, 100 + i, opk, m[i]))
+    pt = sch.decryptMsg(sk, ct)
+    dm = host(pt.mx_device).reshape(3, ctx.N)
+    for i in range(3):
+        assert np.array_equal(dm[i], orc.decrypt(osk, got[i]))
+    assert np.array_equal(host(ctx.decode(pt.mx_device)).reshape(v.shape), v)
+
+
+@pytest.mark.parametrize("which", ["c3", "small", "dnum2"])
+def test_mul_relin_bit_exact_and_decrypts(which):
+    import kunpbfv_b200 as kb
+    ctx, orc = {"c3": c3_pair, "small": lambda: small_pair(12, 3, 1, 50),
+                "dnum2": lambda: small_pair(12, 4, 2, 45, 2)}[which]()
+    sk, sch, osk = setup(ctx, orc)
+    orlk = orc.keygen_relin(SEED, osk)
+    rng = np.random.default_rng(3)
+    k = 3
+    v1 = rng.integers(0, T, size=(k, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(k, ctx.N), dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=0)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=k)
+    out = sch.mult_relin(c1, c2)
+    h1 = host(c1.cipher_device).reshape(k, 2, ctx.q_count, ctx.N)
+    h2 = host(c2.cipher_device).reshape(k, 2, ctx.q_count, ctx.N)
+    ho = host(out.cipher_device).reshape(k, 2, ctx.q_count, ctx.N)
+    for i in range(k):
+        assert np.array_equal(ho[i], orc.mul_relin(h1[i], h2[i], orlk)), f"pair {i}"
+    dec = host(ctx.decode(sch.decryptMsg(sk, out).mx_device)).reshape(k, ctx.N)
+    assert np.array_equal(dec, (v1 * v2) % T)
+    # split form: tensor then relinearise
+    t3 = sch.mult(c1, c2)
+    ht = host(t3.data).reshape(k, 3, ctx.q_count, ctx.N)
+    for i in range(k):
+        assert np.array_equal(ht[i], orc.mul_tensor(h1[i], h2[i]))
+    assert np.array_equal(host(sch.relinearize(t3).cipher_device).reshape(ho.shape), ho)
+
+
+def test_batch_equals_alone_and_64_pairs_decrypt():
+    """64 pairs in one launch sequence: each result equals the pair run alone,
+    and every decryption equals the slot-wise product mod t."""
+    import kunpbfv_b200 as kb
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    rng = np.random.default_rng(4)
+    B = 64
+    v1 = rng.integers(0, T, size=(B, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(B, ctx.N), dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=1000)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=2000)
+    out = sch.mult_relin(c1, c2)
+    dec = host(ctx.decode(sch.decryptMsg(sk, out).mx_device)).reshape(B, ctx.N)
+    assert np.array_equal(dec, (v1 * v2) % T)
+    ho = host(out.cipher_device).reshape(B, 2, ctx.q_count, ctx.N)
+    lq = 2 * ctx.q_count * ctx.N
+    for i in (0, 31, 63):
+        a = kb.Ciphertext(ctx, c1.cipher_device.view(-1)[i * lq:(i + 1) * lq].clone())
+        b = kb.Ciphertext(ctx, c2.cipher_device.view(-1)[i * lq:(i + 1) * lq].clone())
+        alone = host(sch.mult_relin(a, b).cipher_device).reshape(2, ctx.q_count, ctx.N)
+        assert np.array_equal(alone, ho[i])
+    assert sch.noise_budget(sk, kb.Ciphertext(ctx, out.cipher_device.view(-1)[:lq].clone())) > 10
+
+
+def test_mul_plain_and_add():
+    import kunpbfv_b200 as kb
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    rng = np.random.default_rng(5)
+    v1 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+    v2 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))))
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))))
+    s = sch.add(c1, c2)
+    assert np.array_equal(host(ctx.decode(sch.decryptMsg(sk, s).mx_device)).reshape(-1), (v1 + v2) % T)
+    # encode_ntt takes plaintext coefficients (the reference's encode mutates its input into them)
+    pt = ctx.encode_ntt(ctx.encode(dev(v2)))
+    sch.multConstAndEqual(c1, pt)
+    assert np.array_equal(host(ctx.decode(sch.decryptMsg(sk, c1).mx_device)).reshape(-1), (v1 * v2) % T)
+
+
+def test_errors_are_reported():
+    import kunpbfv_b200 as kb
+    ctx, orc = small_pair(12, 3, 1, 50)
+    sch = kb.BFVScheme(ctx, SEED)
+    c = kb.Ciphertext(ctx)
+    with pytest.raises(kb.KbfvError):
+        sch.mult_relin(c, c)   # no relinearisation key
+    with pytest.raises(ValueError):
+        kb.BFVContext(log_n=12, plain_modulus=65537, q_count=0)
