@@ -45,7 +45,39 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-extras", action="store_true", help="only the headline workload")
+    ap.add_argument("--kernel", default=None, choices=["ntt16k", "ntt16k_inv", "pipeline1"],
+                    help="run one kernel on a profiling-sized case and exit (for ncu)")
     return ap.parse_args()
+
+
+def run_kernel_case(args):
+    """Profiling cases: the forward / inverse NTT block kernel on 1024 rows of
+    N=16384 (128 MiB, above L2), or one batched multiply of 16 pairs."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    qs, ps = c3_primes()
+    ctx = kb.BFVContext(log_n=LOG_N, plain_modulus=T, q_count=NQ, q=qs, p_count=NP, p=ps, dnum=1)
+    if args.kernel.startswith("ntt16k"):
+        rows = 1024
+        x = torch.randint(0, 1 << 59, (rows, ctx.N), dtype=torch.int64, device="cuda")
+        fn = ctx.ntt_inv if args.kernel.endswith("inv") else ctx.ntt_fwd
+        for _ in range(args.steps):
+            fn(x, 0, NQ)
+    else:
+        from kunpbfv_b200.api import to_device
+        import numpy as np
+        sk = kb.SecretKey(ctx, SEED)
+        sch = kb.BFVScheme(ctx, SEED)
+        sch.addEncKey(sk)
+        sch.addMultKey_23(sk)
+        rng = np.random.default_rng(0)
+        v = rng.integers(0, T, size=(16, ctx.N), dtype=np.uint64)
+        c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v))), enc_id=0)
+        for _ in range(args.steps):
+            sch.mult_relin(c1, c1)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": args.kernel, "steps": args.steps}))
 
 
 def c3_primes():
@@ -329,8 +361,14 @@ def run_ours(args, world, rank, local):
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.skip_extras:
-        line.update(extras(args, ctx, sch, c1, c2, out, stream, dev))
-        line["cpu_baseline"] = cpu_baseline_sample()
+        try:
+            line.update(extras(args, ctx, sch, c1, c2, out, stream, dev))
+        except Exception as e:  # report, keep the headline line
+            line["extras_error"] = repr(e)
+        try:
+            line["cpu_baseline"] = cpu_baseline_sample()
+        except Exception as e:
+            line["cpu_baseline_error"] = repr(e)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -409,7 +447,7 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
 
     # standalone NTT, N=65536, 32 primes x 64 polynomials (1 GiB)
     qs2 = __import__("oracle").primes_bits(1 << 16, 60, 34)
-    ctx2 = kb.BFVContext(log_n=16, plain_modulus=T, q_count=32, q=qs2[2:34], p_count=1, p=qs2[:1], dnum=1)
+    ctx2 = kb.BFVContext(log_n=16, plain_modulus=786433, q_count=32, q=qs2[2:34], p_count=1, p=qs2[:1], dnum=1)
     mods = torch.tensor(ctx2.q, dtype=torch.int64, device=dev)
     y = torch.randint(0, 1 << 62, (64, 32, 1 << 16), dtype=torch.int64, device=dev)
     y = torch.remainder(y, mods.view(1, 32, 1))
@@ -428,6 +466,9 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
 
 def main():
     args = parse()
+    if args.kernel:
+        run_kernel_case(args)
+        return
     world, rank, local = dist_init(args)
     try:
         if args.impl == "reference":

@@ -12,7 +12,7 @@
 namespace kbfv {
 
 constexpr int kMaxPrimes = 96;   // whole prime table [Q|P|R|T|t]
-constexpr int kMaxQ = 24;        // ciphertext primes per context
+constexpr int kMaxQ = 32;        // ciphertext primes per context
 constexpr int kMaxP = 8;         // special primes
 
 // Everything a kernel needs, passed by value (all pointers into one device pool).

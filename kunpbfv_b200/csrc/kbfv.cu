@@ -465,7 +465,8 @@ static inline RowsIO rows_io(const DevConsts& dc, uint64_t* base, int p0, int pe
     do {                         \
         if ((nq) <= 8) { MACRO(8); }       \
         else if ((nq) <= 16) { MACRO(16); } \
-        else { MACRO(24); }                 \
+        else if ((nq) <= 24) { MACRO(24); } \
+        else { MACRO(33); }                 \
     } while (0)
 
 static void launch_bconv(const DevConsts& dc, const BconvTables& tb, const uint64_t* in, uint64_t* out, int polys,

@@ -4,7 +4,7 @@ import functools
 import numpy as np
 
 import oracle
-from tests.params import T65537, c3_primes, small_primes
+from tests.params import T65537, c3_primes, plain_modulus_for, small_primes
 
 
 def dev(a):
@@ -17,7 +17,8 @@ def host(t):
     return to_host(t)
 
 
-def make_pair(log_n, qs, ps, dnum=1, t=T65537):
+def make_pair(log_n, qs, ps, dnum=1, t=None):
+    t = t or plain_modulus_for(log_n)
     import kunpbfv_b200 as kb
     ctx = kb.BFVContext(log_n=log_n, plain_modulus=t, q_count=len(qs), q=qs, p_count=len(ps), p=ps, dnum=dnum)
     orc = oracle.Oracle(log_n, t, qs, ps, dnum=dnum)

@@ -22,3 +22,8 @@ def c3_primes():
 def small_primes(log_n: int = 12, nq: int = 3, np_: int = 1, bits: int = 50):
     ps = chain(log_n, bits, nq + np_)
     return list(ps[np_:np_ + nq]), list(ps[:np_])
+
+
+def plain_modulus_for(log_n: int) -> int:
+    """65537 while 2N divides 65536, else 786433 (= 3 * 2^18 + 1)."""
+    return 65537 if (2 << log_n) <= 65536 else 786433
