@@ -55,6 +55,8 @@ def _declare(L: C.CDLL) -> None:
         "orc_create": (C.c_void_p, [C.c_uint32, C.c_uint64, U64P, C.c_int, U64P, C.c_int, C.c_int,
                                     U64P, C.c_int, C.c_int]),
         "orc_destroy": (V, [C.c_void_p]),
+        "orc_set_ref_compat": (V, [C.c_void_p, C.c_int]),
+        "orc_klss_relinearize": (V, [C.c_void_p, U64P, U64P, U64P]),
         "orc_prime_count": (C.c_int, [C.c_void_p]),
         "orc_primes": (V, [C.c_void_p, U64P]),
         "orc_psi": (C.c_uint64, [C.c_void_p, C.c_int]),
@@ -64,6 +66,7 @@ def _declare(L: C.CDLL) -> None:
         "orc_bconv_r_to_q": (V, [C.c_void_p, U64P, U64P]),
         "orc_tensor_qr": (V, [C.c_void_p, U64P, U64P, U64P]),
         "orc_scale_round_qr_r": (V, [C.c_void_p, U64P, U64P]),
+        "orc_scale_round_qr_r_ref": (V, [C.c_void_p, U64P, U64P]),
         "orc_decrypt_round": (V, [C.c_void_p, U64P, U64P, C.c_int]),
         "orc_decrypt_variant": (C.c_int, [C.c_void_p]),
         "orc_delta_m": (V, [C.c_void_p, U64P, U64P]),
@@ -251,6 +254,10 @@ class Oracle:
     def scale_round_qr_r(self, x):
         return self._call("orc_scale_round_qr_r", x, out_shape=(self.nr, self.n))
 
+    def scale_round_qr_r_ref(self, x):
+        """The reference's variant (alpha reduced in place across R primes)."""
+        return self._call("orc_scale_round_qr_r_ref", x, out_shape=(self.nr, self.n))
+
     def decrypt_round(self, x, variant: int = -1):
         return self._call("orc_decrypt_round", x, out_shape=(self.n,), extra=(variant,))
 
@@ -286,6 +293,12 @@ class Oracle:
         nri, _ = self.klss_blocks()
         return self._call("orc_klss_modup_t_to_pq", x_t, out_shape=(npoly, nri * self.nt, self.n),
                           extra=(npoly,))
+
+    def set_ref_compat(self, on: bool):
+        lib().orc_set_ref_compat(self._h, int(on))
+
+    def klss_relinearize(self, d, key_t):
+        return self._call("orc_klss_relinearize", d, key_t, out_shape=(2, self.nq, self.n))
 
     def klss_moddown(self, x, npoly: int = 2):
         return self._call("orc_klss_moddown", x, out_shape=(npoly, self.nq, self.n), extra=(npoly,))

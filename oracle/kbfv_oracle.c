@@ -276,6 +276,7 @@ struct orc_ctx {
     u64 *dig_hat_mod;                           /* [d][target m in 0..nq+np)][j in digit] */
     u64 *dig_Q_mod;                             /* [d][target m] */
     uint64_t gauss_cdt[64]; int gauss_bound;
+    int ref_compat;            /* 1: reproduce the reference's scale-round quirk in mul_tensor */
 };
 
 static u64 brv(u64 x, int bits) {
@@ -517,6 +518,7 @@ void orc_destroy(orc_ctx* c) {
 }
 
 int orc_prime_count(const orc_ctx* c) { return c->nall; }
+void orc_set_ref_compat(orc_ctx* c, int on) { c->ref_compat = on; }
 void orc_primes(const orc_ctx* c, u64* out) { memcpy(out, c->mods, c->nall * 8); }
 u64 orc_psi(const orc_ctx* c, int i) { return c->tab[i].root; }
 
@@ -620,8 +622,13 @@ void orc_tensor_qr(const orc_ctx* c, const u64* ct1, const u64* ct2, u64* out) {
     }
 }
 
-/* scaleAndRound_HPS_QR_R_kernel (poly_arithmetic.cuh:1263-1307) */
-void orc_scale_round_qr_r(const orc_ctx* c, const u64* in, u64* out) {
+/* scaleAndRound_HPS_QR_R_kernel (poly_arithmetic.cuh:1263-1307).
+ * chain_alpha != 0 reproduces the reference exactly: its
+ * barrett_reduce_uint64_uint64 takes alpha by reference (uint128.cuh:156-163,
+ * called at poly_arithmetic.cuh:1299), so alpha is reduced mod r_0, then that
+ * mod r_1, ... and the R residues stop describing one integer once alpha
+ * exceeds an R prime. chain_alpha == 0 reduces alpha mod each r_j (correct). */
+static void scale_round_impl(const orc_ctx* c, const u64* in, u64* out, int chain_alpha) {
     u64 n = c->n;
     const u64* R = c->mods + c->nq + c->np;
     for (u64 k = 0; k < n; k++) {
@@ -634,10 +641,15 @@ void orc_scale_round_qr_r(const orc_ctx* c, const u64* in, u64* out) {
             for (int i = 0; i < c->nq; i++) acc += (u128)in[(size_t)i * n + k] * cj[i];
             acc += (u128)in[(size_t)(c->nq + j) * n + k] * cj[c->nq];
             u64 r = (u64)(acc % R[j]);
-            out[(size_t)j * n + k] = addmod(r, alpha % R[j], R[j]);
+            u64 a;
+            if (chain_alpha) { alpha %= R[j]; a = alpha; }
+            else a = alpha % R[j];
+            out[(size_t)j * n + k] = addmod(r, a, R[j]);
         }
     }
 }
+void orc_scale_round_qr_r(const orc_ctx* c, const u64* in, u64* out) { scale_round_impl(c, in, out, 0); }
+void orc_scale_round_qr_r_ref(const orc_ctx* c, const u64* in, u64* out) { scale_round_impl(c, in, out, 1); }
 
 /* hps_decrypt_scale_and_round_kernel_{small,small_lazy,large,large_lazy}
  * (poly_arithmetic.cuh:930-1075). Returns the rounded value; for inputs that
@@ -1270,7 +1282,7 @@ void orc_mul_tensor(const orc_ctx* c, const u64* ct1, const u64* ct2, u64* d) {
         u64* y = tp + (size_t)k * lqr;
         ntt_inv_limbs(c, 0, y, nq);
         ntt_inv_limbs(c, nq + c->np, y + lq, nr);
-        orc_scale_round_qr_r(c, y, rr);
+        scale_round_impl(c, y, rr, c->ref_compat);
         orc_bconv_r_to_q(c, rr, d + (size_t)k * lq);
         ntt_fwd_limbs(c, 0, d + (size_t)k * lq, nq);
     }
@@ -1356,4 +1368,38 @@ double orc_noise_budget(const orc_ctx* c, const u64* sk, const u64* ct) {
     }
     free(x);
     return big_log2(&Q) - worst - 1.0;
+}
+
+/* The reference's relinearisation (multAndEqual_23, KeySwitch_23.cuh:277-305):
+ * a1a2 to coefficients, Qj blocks lifted into T, NTT over T, external product
+ * with the KLSS key (NTT over T, [ax|bx][digit][Ri][T]), INTT over T, exact
+ * T -> P|Q, mod down, NTT over Q, add [cross | b1b2]. d is [a1a2|cross|b1b2] in
+ * NTT form over Q. */
+void orc_klss_relinearize(const orc_ctx* c, const u64* d, const u64* key_t, u64* ct) {
+    u64 n = c->n;
+    int nq = c->nq, nt = c->nt;
+    int nri = orc_klss_ri_blocks(c), nqj = orc_klss_qj_blocks(c);
+    int t0 = c->nq + c->np + c->nr;
+    size_t lq = (size_t)nq * n;
+    u64* d2 = malloc(lq * 8);
+    u64* dig = malloc((size_t)nqj * nt * n * 8);
+    u64* ext = malloc((size_t)2 * nri * nt * n * 8);
+    u64* pq = calloc((size_t)2 * nri * nt * n, 8);
+    u64* dn = malloc(2 * lq * 8);
+    memcpy(d2, d, lq * 8);
+    ntt_inv_limbs(c, 0, d2, nq);
+    orc_klss_modup_qj_to_t(c, d2, dig);
+    for (int b = 0; b < nqj; b++) ntt_fwd_limbs(c, t0, dig + (size_t)b * nt * n, nt);
+    orc_klss_external_product(c, dig, key_t, ext);
+    for (int b = 0; b < 2 * nri; b++) ntt_inv_limbs(c, t0, ext + (size_t)b * nt * n, nt);
+    orc_klss_modup_t_to_pq(c, ext, pq, 2);
+    orc_klss_moddown(c, pq, dn, 2);
+    ntt_fwd_limbs(c, 0, dn, nq);
+    ntt_fwd_limbs(c, 0, dn + lq, nq);
+    for (size_t i = 0; i < lq; i++) {
+        u64 q = c->mods[i / n];
+        ct[i] = addmod(d[lq + i], dn[i], q);
+        ct[lq + i] = addmod(d[2 * lq + i], dn[lq + i], q);
+    }
+    free(d2); free(dig); free(ext); free(pq); free(dn);
 }

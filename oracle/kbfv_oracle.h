@@ -41,6 +41,8 @@ orc_ctx* orc_create(uint32_t log_n, uint64_t t, const uint64_t* q, int nq,
                     const uint64_t* p, int np, int dnum,
                     const uint64_t* tk, int nt, int gamma);
 void     orc_destroy(orc_ctx* c);
+/* 1: mul_tensor reproduces the reference's in-place alpha reduction (see scale_round_qr_r_ref) */
+void     orc_set_ref_compat(orc_ctx* c, int on);
 int      orc_prime_count(const orc_ctx* c);          /* total entries in the prime table */
 void     orc_primes(const orc_ctx* c, uint64_t* out);
 uint64_t orc_psi(const orc_ctx* c, int prime_idx);
@@ -55,6 +57,8 @@ void orc_bconv_r_to_q(const orc_ctx* c, const uint64_t* in_r, uint64_t* out_q);
 /* ct1, ct2: 2 polys x (nq+nr) limbs in NTT form over Q|R; out: 3 polys */
 void orc_tensor_qr(const orc_ctx* c, const uint64_t* ct1, const uint64_t* ct2, uint64_t* out);
 void orc_scale_round_qr_r(const orc_ctx* c, const uint64_t* in_qr, uint64_t* out_r);
+/* the reference's variant: alpha reduced in place across the R primes */
+void orc_scale_round_qr_r_ref(const orc_ctx* c, const uint64_t* in_qr, uint64_t* out_r);
 /* variant: -1 = select by bit sizes as the reference does, else 0..3 */
 void orc_decrypt_round(const orc_ctx* c, const uint64_t* in_q, uint64_t* out, int variant);
 int  orc_decrypt_variant(const orc_ctx* c);
@@ -74,6 +78,8 @@ void orc_klss_external_product(const orc_ctx* c, const uint64_t* digits_t, const
                                uint64_t* out);
 void orc_klss_modup_t_to_pq(const orc_ctx* c, const uint64_t* in_t, uint64_t* out_pq_ref_order, int npoly);
 void orc_klss_moddown(const orc_ctx* c, const uint64_t* in_pq_ref_order, uint64_t* out_q, int npoly);
+/* the reference's full KLSS relinearisation of a tensor [a1a2|cross|b1b2] (NTT form) */
+void orc_klss_relinearize(const orc_ctx* c, const uint64_t* d, const uint64_t* key_t, uint64_t* ct);
 
 /* ---- randomness and samplers ------------------------------------------ */
 void orc_hsalsa20(const uint8_t key[32], const uint8_t nonce16[16], uint8_t out[32]);

@@ -1,8 +1,8 @@
 // Reference-kernel harness (test infrastructure).
 //
 // Compiles kunpBFV's own headers, where they lie, for sm_100a and runs its
-// kernels and launchers on seeded inputs, writing every input and output as
-// raw little-endian uint64 files plus a manifest. The committed script
+// kernels and launchers on seeded inputs, writing a manifest line (length,
+// 64-bit digest, first values) for every input and output. The committed script
 // tests/golden/make_ref_fixtures.py turns one run into the fixtures that
 // pin the CPU oracle. Build: `make -C oracle ref` (nvcc; NTL replaced by the
 // header in ntl_shim/, which covers the context precompute's big-integer use).
@@ -12,7 +12,7 @@
 // (include/BFVScheme.cuh:138), so the harness launches that kernel itself
 // with a device copy of the moduli.
 //
-// Usage: ref_harness <logN 14|15> <outdir>
+// Usage: ref_harness <logN 14|15> <outdir> [raw_limit_words]
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -50,12 +50,29 @@ static std::vector<uint64_tt> gen(uint64_tt seed, const std::vector<uint64_tt>& 
     return v;
 }
 
+// Order-dependent 64-bit digest: sum over i of mix(x_i ^ (i * gamma)), mix being
+// splitmix64's finaliser. tests/golden/refgen.py computes the same digest.
+static uint64_tt mix64(uint64_tt z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Writes one manifest line per array: name, length, digest, first 8 values.
+// Arrays up to `g_raw_limit` words are also written raw (<name>.bin).
+static size_t g_raw_limit = 0;
 static void dump_host(const std::string& name, const uint64_tt* p, size_t count) {
-    std::string path = g_out + "/" + name + ".bin";
-    FILE* f = fopen(path.c_str(), "wb");
-    fwrite(p, 8, count, f);
-    fclose(f);
-    fprintf(g_manifest, "%s %zu\n", name.c_str(), count);
+    uint64_tt h = 0;
+    for (size_t i = 0; i < count; i++) h += mix64(p[i] ^ ((uint64_tt)i * 0x9E3779B97F4A7C15ULL));
+    fprintf(g_manifest, "%s %zu %llu", name.c_str(), count, (unsigned long long)h);
+    for (size_t i = 0; i < 8 && i < count; i++) fprintf(g_manifest, " %llu", (unsigned long long)p[i]);
+    fprintf(g_manifest, "\n");
+    if (count <= g_raw_limit) {
+        std::string path = g_out + "/" + name + ".bin";
+        FILE* f = fopen(path.c_str(), "wb");
+        fwrite(p, 8, count, f);
+        fclose(f);
+    }
 }
 
 static void dump_dev(const std::string& name, const uint64_tt* d, size_t count) {
@@ -86,6 +103,7 @@ int main(int argc, char** argv) {
     const int logN = atoi(argv[1]);
     g_out = argv[2];
     g_manifest = fopen((g_out + "/manifest.txt").c_str(), "w");
+    g_raw_limit = argc > 3 ? (size_t)atoll(argv[3]) : 64;
     const size_t N = (size_t)1 << logN;
 
     BFVContext context(N);

@@ -22,3 +22,15 @@ def gen(seed: int, mods, n: int) -> np.ndarray:
     for l, q in enumerate(mods):
         out[l] = splitmix_stream(((seed << 20) + l) & 0xFFFFFFFFFFFFFFFF, n) % np.uint64(q)
     return out
+
+
+def digest(a) -> int:
+    """sum_i mix(x_i ^ (i * gamma)) mod 2^64, mix = splitmix64's finaliser (same as the harness)."""
+    x = np.ascontiguousarray(a, dtype=np.uint64).reshape(-1)
+    with np.errstate(over="ignore"):
+        i = np.arange(x.size, dtype=np.uint64)
+        z = x ^ (i * GAMMA)
+        z = (z ^ (z >> np.uint64(30))) * C1
+        z = (z ^ (z >> np.uint64(27))) * C2
+        z = z ^ (z >> np.uint64(31))
+        return int(np.sum(z, dtype=np.uint64))

@@ -3,25 +3,20 @@
 The fixtures in tests/golden/ref_logn*.json were produced by running
 kunpBFV's kernels (compiled from its sources by oracle/ref_harness) on a
 B200 with seeded inputs (tests/golden/refgen.py); tests/golden/make_ref_fixtures.py
-recorded SHA-256 digests of every input and output. Here the oracle recomputes
+recorded 64-bit digests (refgen.digest) of every input and output. Here the oracle recomputes
 each output from the regenerated inputs and must reproduce the digest.
 """
 import glob
-import hashlib
 import json
 import os
 
 import numpy as np
 import pytest
 
-from tests.golden.refgen import gen
+from tests.golden.refgen import digest, gen
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FIXTURES = sorted(glob.glob(os.path.join(HERE, "ref_logn*.json")))
-
-
-def sha(a):
-    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint64).tobytes()).hexdigest()
 
 
 class Ref:
@@ -47,7 +42,7 @@ class Ref:
         w = self.want(name)
         a = np.ascontiguousarray(arr, dtype=np.uint64).reshape(-1)
         assert a.size == w["count"], (name, a.size, w["count"])
-        if sha(a) != w["sha256"]:
+        if digest(a) != w["digest"]:
             head = [int(x) for x in a[:8]]
             raise AssertionError(f"{name}: digest differs; oracle head {head} vs reference {w['head']}")
 
@@ -107,8 +102,16 @@ def test_hps_bconv(ref):
 
 
 def test_scale_round(ref):
+    """The reference reduces alpha in place across the R primes
+    (poly_arithmetic.cuh:1299 passes it by reference); the oracle's _ref variant
+    reproduces that. Where alpha exceeds an R prime the correct per-prime
+    reduction (used by the product) differs: at logN=15 for most coefficients."""
     x = ref.inp("sr_in", 9, list(ref.q) + list(ref.R))
-    ref.check("sr_out", ref.o.scale_round_qr_r(x))
+    ref.check("sr_out", ref.o.scale_round_qr_r_ref(x))
+    fixed = ref.o.scale_round_qr_r(x)
+    same = digest(fixed) == ref.want("sr_out")["digest"]
+    if ref.log_n == 15:
+        assert not same
 
 
 def test_decrypt_round(ref):
@@ -149,3 +152,73 @@ def test_salsa20_compat(ref, oracle_mod):
     nonce = ref.fx["rng_nonce"][0]
     out = np.frombuffer(oracle_mod.salsa20_compat(key, nonce, 64 * 40), dtype=np.uint64)
     ref.check("rng_out", out)
+
+
+def _key_pq_to_mine(ref, k):
+    """reference key layout [digit][P|Q] (NTT form) -> oracle [digit][Q|P]"""
+    k = k.reshape(ref.dnum, len(ref.PQ), ref.n)
+    return np.concatenate([k[:, ref.K:], k[:, :ref.K]], axis=1)
+
+
+def _ntt_rows(o, idxs, x):
+    return np.stack([o.ntt_fwd(i, x[l]) for l, i in enumerate(idxs)])
+
+
+def test_klss_key_conversion(ref):
+    """addMultKey_23's conversion of P|Q key material to T blocks (KeySwitch_23.cuh:55-65)."""
+    o = ref.o
+    ka = ref.inp("mult_key_a", 21, ref.PQ * ref.dnum).reshape(ref.dnum, len(ref.PQ), ref.n)
+    kb = ref.inp("mult_key_b", 22, ref.PQ * ref.dnum).reshape(ref.dnum, len(ref.PQ), ref.n)
+    pq_idx = ref.idx_pqt[: len(ref.PQ)]
+    t_idx = ref.idx_pqt[len(ref.PQ):]
+    parts = []
+    for half in (ka, kb):
+        for dg in range(ref.dnum):
+            coef = np.stack([o.ntt_inv(i, half[dg][l]) for l, i in enumerate(pq_idx)])
+            blocks = o.klss_modup_pq_to_t(coef)  # [Ri][T]
+            parts.append(np.stack([np.stack([o.ntt_fwd(t_idx[tk], blocks[b, tk]) for tk in range(ref.nt)])
+                                   for b in range(ref.Ri)]))
+    ref.check("mult_key_t", np.stack(parts))
+
+
+def test_multiply_path(ref):
+    """compute_t_QInv_c0c1c2 + the KLSS key switch (multAndEqual_23 without its
+    final copy of ct1 * Dec(ct2) over the product).
+
+    The tensor matches the oracle in reference-compat mode. The KLSS
+    relinearisation restated in the oracle matches the reference at both sizes.
+    The hybrid relinearisation (what the product computes) equals the KLSS one
+    at logN=14; at logN=15 the reference's T base (4 x 60 bits) is smaller than
+    the key-switch products it must hold exactly, so the two differ."""
+    o = ref.o
+    c1 = ref.inp("mult_ct1", 23, list(ref.q) * 2)
+    c2 = ref.inp("mult_ct2", 24, list(ref.q) * 2)
+    o.set_ref_compat(True)
+    try:
+        d = o.mul_tensor(c1, c2)
+    finally:
+        o.set_ref_compat(False)
+    ref.check("mult_axax", d[0])
+    ref.check("mult_axbx", d[1])
+    ref.check("mult_bxbx", d[2])
+    ka = ref.inp("mult_key_a", 21, ref.PQ * ref.dnum)
+    kb = ref.inp("mult_key_b", 22, ref.PQ * ref.dnum)
+    # KLSS key as the reference built it (checked in test_klss_key_conversion)
+    o2 = ref.o
+    pq_idx = ref.idx_pqt[: len(ref.PQ)]
+    t_idx = ref.idx_pqt[len(ref.PQ):]
+    parts = []
+    for half in (ka.reshape(ref.dnum, len(ref.PQ), ref.n), kb.reshape(ref.dnum, len(ref.PQ), ref.n)):
+        for dg in range(ref.dnum):
+            coef = np.stack([o2.ntt_inv(i, half[dg][l]) for l, i in enumerate(pq_idx)])
+            blocks = o2.klss_modup_pq_to_t(coef)
+            parts.append(np.stack([np.stack([o2.ntt_fwd(t_idx[tk], blocks[b, tk]) for tk in range(ref.nt)])
+                                   for b in range(ref.Ri)]))
+    key_t = np.stack(parts)
+    ref.check("mult_out", o.klss_relinearize(d, key_t))
+    # hybrid over P|Q with the same key material
+    rlk = np.stack([np.stack([_key_pq_to_mine(ref, ka)[dg], _key_pq_to_mine(ref, kb)[dg]])
+                    for dg in range(ref.dnum)])
+    hyb = o.relinearize(d, rlk)
+    same = digest(hyb) == ref.want("mult_out")["digest"]
+    assert same == (ref.log_n == 14)
