@@ -184,8 +184,8 @@ static void build_context(Context& c, const kbfv_params& prm) {
     KB_REQUIRE(nall <= kMaxPrimes, KBFV_ERR_INVALID, "too many primes");
     for (int i = 0; i < nall; i++) {
         const uint64_t q = c.mods[i];
-        KB_REQUIRE(H::is_prime(q) && q < ((uint64_t)1 << 62) && (q - 1) % (2 * c.n) == 0, KBFV_ERR_PARAMS,
-                   "every modulus must be a prime below 2^62 congruent to 1 mod 2N");
+        KB_REQUIRE(H::is_prime(q) && q < ((uint64_t)1 << 60) && (q - 1) % (2 * c.n) == 0, KBFV_ERR_PARAMS,
+                   "every modulus must be a prime below 2^60 congruent to 1 mod 2N");
         for (int j = 0; j < i; j++)
             KB_REQUIRE(c.mods[j] != q || (i == nall - 1), KBFV_ERR_PARAMS, "moduli must be distinct");
     }
@@ -373,56 +373,57 @@ static void build_context(Context& c, const kbfv_params& prm) {
 static inline cudaStream_t S(kbfv_stream s) { return (cudaStream_t)s; }
 static inline unsigned blocks_for(size_t total, unsigned threads) { return (unsigned)((total + threads - 1) / threads); }
 
-template <int LOGB, class Src, class Dst>
+template <int LOGB, class Src, class Dst, bool FULL = true>
 static void launch_fwd_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
     constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;
     static bool configured = false;
     if (!configured) {
-        KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_fwd_block_kernel<LOGB, Src, Dst>,
+        KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_fwd_block_kernel<LOGB, Src, Dst, FULL>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
         configured = true;
     }
     const int nblk = 1 << (logn - LOGB);
-    ntt_fwd_block_kernel<LOGB, Src, Dst><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
+    ntt_fwd_block_kernel<LOGB, Src, Dst, FULL><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
         s, d, dc.tw_fwd, dc.mods, logn);
 }
 
-template <int LOGB, class Src, class Dst>
+template <int LOGB, class Src, class Dst, bool WHOLE>
 static void launch_inv_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
     constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;
     static bool configured = false;
     if (!configured) {
-        KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_inv_block_kernel<LOGB, Src, Dst>,
+        KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_inv_block_kernel<LOGB, Src, Dst, WHOLE>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
         configured = true;
     }
     const int nblk = 1 << (logn - LOGB);
-    ntt_inv_block_kernel<LOGB, Src, Dst><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
+    ntt_inv_block_kernel<LOGB, Src, Dst, WHOLE><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
         s, d, dc.tw_inv, dc.mods, logn);
 }
 
 // Forward NTT of `rows` rows read through `s` and written through `d`.
 // For logn <= 14 one block kernel; for 15/16 a column pass (s -> d) then the
-// block kernel in place on d (d must also be readable).
-template <class Src, class Dst>
+// block kernel in place on d (d must also be readable). FULL = false leaves
+// outputs in [0, 8q) for consumers that reduce anyway (pipeline stages only).
+template <class Src, class Dst, bool FULL = true>
 static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st) {
     if (rows <= 0) return;
     switch (dc.logn) {
-        case 10: launch_fwd_block<10>(dc, s, d, rows, 10, st); break;
-        case 11: launch_fwd_block<11>(dc, s, d, rows, 11, st); break;
-        case 12: launch_fwd_block<12>(dc, s, d, rows, 12, st); break;
-        case 13: launch_fwd_block<13>(dc, s, d, rows, 13, st); break;
-        case 14: launch_fwd_block<14>(dc, s, d, rows, 14, st); break;
+        case 10: launch_fwd_block<10, Src, Dst, FULL>(dc, s, d, rows, 10, st); break;
+        case 11: launch_fwd_block<11, Src, Dst, FULL>(dc, s, d, rows, 11, st); break;
+        case 12: launch_fwd_block<12, Src, Dst, FULL>(dc, s, d, rows, 12, st); break;
+        case 13: launch_fwd_block<13, Src, Dst, FULL>(dc, s, d, rows, 13, st); break;
+        case 14: launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st); break;
         case 15: {
             const int total = rows << 14;
             ntt_fwd_col_kernel<1, Src, Dst><<<blocks_for(total, 256), 256, 0, st>>>(s, d, dc.tw_fwd, dc.mods, 15, total);
-            launch_fwd_block<14>(dc, d, d, rows, 15, st);
+            launch_fwd_block<14, Dst, Dst, FULL>(dc, d, d, rows, 15, st);
             break;
         }
         case 16: {
             const int total = rows << 14;
             ntt_fwd_col_kernel<2, Src, Dst><<<blocks_for(total, 256), 256, 0, st>>>(s, d, dc.tw_fwd, dc.mods, 16, total);
-            launch_fwd_block<14>(dc, d, d, rows, 16, st);
+            launch_fwd_block<14, Dst, Dst, FULL>(dc, d, d, rows, 16, st);
             break;
         }
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
@@ -434,19 +435,19 @@ template <class Src, class Dst>
 static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st) {
     if (rows <= 0) return;
     switch (dc.logn) {
-        case 10: launch_inv_block<10>(dc, s, d, rows, 10, st); break;
-        case 11: launch_inv_block<11>(dc, s, d, rows, 11, st); break;
-        case 12: launch_inv_block<12>(dc, s, d, rows, 12, st); break;
-        case 13: launch_inv_block<13>(dc, s, d, rows, 13, st); break;
-        case 14: launch_inv_block<14>(dc, s, d, rows, 14, st); break;
+        case 10: launch_inv_block<10, Src, Dst, true>(dc, s, d, rows, 10, st); break;
+        case 11: launch_inv_block<11, Src, Dst, true>(dc, s, d, rows, 11, st); break;
+        case 12: launch_inv_block<12, Src, Dst, true>(dc, s, d, rows, 12, st); break;
+        case 13: launch_inv_block<13, Src, Dst, true>(dc, s, d, rows, 13, st); break;
+        case 14: launch_inv_block<14, Src, Dst, true>(dc, s, d, rows, 14, st); break;
         case 15: {
-            launch_inv_block<14>(dc, s, d, rows, 15, st);
+            launch_inv_block<14, Src, Dst, false>(dc, s, d, rows, 15, st);
             const int total = rows << 14;
             ntt_inv_col_kernel<1, Dst, Dst><<<blocks_for(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 15, total);
             break;
         }
         case 16: {
-            launch_inv_block<14>(dc, s, d, rows, 16, st);
+            launch_inv_block<14, Src, Dst, false>(dc, s, d, rows, 16, st);
             const int total = rows << 14;
             ntt_inv_col_kernel<2, Dst, Dst><<<blocks_for(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
             break;
@@ -740,8 +741,9 @@ static void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratc
     ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), count * 4 * dc.nq, st);
     // K2: Q -> R (centred)
     launch_bconv(dc, q2r_tables(dc), m.sa, m.sb, count * 4, (size_t)dc.nq << dc.logn, (size_t)dc.nr << dc.logn, st);
-    // K3: NTT over R in place
-    ntt_fwd(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr), count * 4 * dc.nr, st);
+    // K3: NTT over R in place (outputs in [0, 8q): the tensor reduces its products)
+    ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr),
+                                   count * 4 * dc.nr, st);
     // K4: tensor (Q part from the NTT-form inputs, R part from K3) fused into INTT over Q|R
     TensorSrc ts{pb, m.sb, dc};
     ntt_inv(dc, ts, rows_io(dc, m.sc, 0, 1), count * 3 * dc.nqr, st);
@@ -762,8 +764,9 @@ static void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb,
     const DevConsts& dc = c.dc;
     mul_front(c, pb, count, m, st);
     k5_launch(c, count, m, nullptr, 1, st);
-    // K6a: NTT over Q|P of the lifted digits, in place
-    ntt_fwd(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq), count * dc.dnum * dc.npq, st);
+    // K6a: NTT over Q|P of the lifted digits, in place ([0, 8q): the key product reduces)
+    ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
+                                   count * dc.dnum * dc.npq, st);
     // K6b: inner product with the key fused into INTT over Q|P
     ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc}, rows_io(dc, m.se, 0, 1), count * 2 * dc.npq, st);
     // K7: mod down + add (cross | b1b2) fused into NTT over Q, written to the outputs
@@ -1334,7 +1337,8 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
             DISPATCH_MAXQ(dc.nq, L_MU);
 #undef L_MU
             check_launch("modup");
-            ntt_fwd(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq), cnt * dc.dnum * dc.npq, st);
+            ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
+                                           cnt * dc.dnum * dc.npq, st);
             ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc}, rows_io(dc, m.se, 0, 1), cnt * 2 * dc.npq, st);
             std::vector<uint64_t*> O(cnt);
             std::vector<const uint64_t*> Z(cnt);

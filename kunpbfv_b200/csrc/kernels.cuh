@@ -96,17 +96,22 @@ __device__ __forceinline__ void scale_round_coeff(const DevConsts& c, const uint
     for (int i = 0; i < MAXQ; i++)
         if (i < c.nq) nu = __fma_rn(__ull2double_rn(xq[i]), c.sr_frac[i], nu);
     const uint64_t alpha = __double2ull_rz(nu);
-    for (int j = 0; j < c.nr; j++) {
-        const uint64_t* cj = c.sr_c + (size_t)j * (c.nq + 1);
-        u128 acc{0, 0};
 #pragma unroll
-        for (int i = 0; i < MAXQ; i++)
-            if (i < c.nq) mac(acc, xq[i], cj[i]);
-        mac(acc, xr[j], cj[c.nq]);
-        const int pj = c.idx_r + j;
-        const uint64_t rj = c.mods[pj];
-        uint64_t v = barrett128(acc, rj, c.mu_hi[pj], c.mu_lo[pj]);
-        out_r[j] = add_mod(v, barrett64(alpha, rj, c.mu_hi[pj]), rj);
+    for (int j = 0; j < MAXQ + 1; j++) {
+        if (j < c.nr) {
+            const uint64_t* cj = c.sr_c + (size_t)j * (c.nq + 1);
+            u128 acc{0, 0};
+#pragma unroll
+            for (int i = 0; i < MAXQ; i++)
+                if (i < c.nq) mac(acc, xq[i], cj[i]);
+            mac(acc, xr[j], cj[c.nq]);
+            const int pj = c.idx_r + j;
+            const uint64_t rj = c.mods[pj];
+            const uint64_t v = barrett128(acc, rj, c.mu_hi[pj], c.mu_lo[pj]);
+            // alpha is reduced mod each r_j on its own (the reference chains the
+            // reduction across r_0, r_1, ..., which breaks the R residues)
+            out_r[j] = add_mod(v, barrett64(alpha, rj, c.mu_hi[pj]), rj);
+        }
     }
 }
 
@@ -135,37 +140,38 @@ __global__ void scale_round_kernel(DevConsts c, const uint64_t* __restrict__ in,
 template <int MAXQ>
 __device__ __forceinline__ void modup_coeff(const DevConsts& c, const uint64_t* xq, uint64_t* __restrict__ out,
                                             size_t k) {
-    // out: [dnum][npq] rows of N
+    // out: [dnum][npq] rows of N. Register arrays are indexed by unrolled
+    // prime positions only; digit membership is a runtime test.
     for (int d = 0; d < c.dnum; d++) {
         const int lo = d * c.alpha;
         const int hi = min(lo + c.alpha, c.nq);
         uint64_t rb[MAXQ];
         float vv = 0.f;
 #pragma unroll
-        for (int j = 0; j < MAXQ; j++) {
-            if (j < hi - lo) {
-                const int g = lo + j;
-                const uint64_t qj = c.mods[g];
-                rb[j] = shoup(xq[g], c.dig_hatinv[g], c.dig_hatinvs[g], qj);
-                vv = __fadd_rn(vv, __fdiv_rn(__ull2float_rn(rb[j]), __ull2float_rn(qj)));
+        for (int i = 0; i < MAXQ; i++) {
+            rb[i] = 0;
+            if (i >= lo && i < hi) {
+                const uint64_t qi = c.mods[i];
+                rb[i] = shoup(xq[i], c.dig_hatinv[i], c.dig_hatinvs[i], qi);
+                vv = __fadd_rn(vv, __fdiv_rn(__ull2float_rn(rb[i]), __ull2float_rn(qi)));
             }
         }
         const uint64_t vf = (uint64_t)__float2int_rz(vv);
         uint64_t* o = out + ((size_t)d * c.npq << c.logn);
-        for (int m = 0; m < c.npq; m++) {
-            uint64_t r;
-            if (m >= lo && m < hi) {
-                r = xq[m];
-            } else {
-                const uint64_t* hm = c.dig_hat_mod + ((size_t)d * c.npq + m) * c.alpha;
-                u128 acc{0, 0};
+        // the digit's own primes: the input residues
 #pragma unroll
-                for (int j = 0; j < MAXQ; j++)
-                    if (j < hi - lo) mac(acc, rb[j], hm[j]);
-                sub128(acc, vf * c.dig_q_mod[(size_t)d * c.npq + m]);
-                r = barrett128(acc, c.mods[m], c.mu_hi[m], c.mu_lo[m]);
-            }
-            o[((size_t)m << c.logn) + k] = r;
+        for (int i = 0; i < MAXQ; i++)
+            if (i >= lo && i < hi) o[((size_t)i << c.logn) + k] = xq[i];
+        // every other prime of Q|P: approximate CRT of the digit
+        for (int m = 0; m < c.npq; m++) {
+            if (m >= lo && m < hi) continue;
+            const uint64_t* hm = c.dig_hat_mod + ((size_t)d * c.npq + m) * c.alpha - lo;
+            u128 acc{0, 0};
+#pragma unroll
+            for (int i = 0; i < MAXQ; i++)
+                if (i >= lo && i < hi) mac(acc, rb[i], hm[i]);
+            sub128(acc, vf * c.dig_q_mod[(size_t)d * c.npq + m]);
+            o[((size_t)m << c.logn) + k] = barrett128(acc, c.mods[m], c.mu_hi[m], c.mu_lo[m]);
         }
     }
 }

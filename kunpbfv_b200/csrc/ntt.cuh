@@ -7,12 +7,13 @@
 //
 // Shape: one CTA transforms one block of 2^LOGB points held in shared memory
 // (N = 2^14 -> 1024 threads x 16 points, 136 KiB of padded smem). Each thread
-// runs radix-16 groups (4 butterfly stages in registers) between shared-memory
-// exchanges. Larger rings (N = 2^15, 2^16) add one elementwise radix-2/4 column
-// pass in front of (forward) or behind (inverse) the block kernels.
+// runs register groups of 8 (N = 2^14) or 16 points (smaller N) through 3 or 4
+// butterfly stages between shared-memory exchanges. Larger rings (2^15, 2^16)
+// add one elementwise radix-2/4 column pass in front of (forward) or behind
+// (inverse) the block kernels. Moduli must be below 2^60 (lazy range 8q < 2^63).
 //
-// Rows are described by Src/Dst functors: src.prime(row), s.load(j),
-// d.store(j, v). This lets pipeline stages fuse their per-element
+// Rows are described by Src/Dst functors: src.prime(row) and
+// src.bind(row) -> {load(j), store(j, v)}. This lets pipeline stages fuse their per-element
 // prologue (e.g. a tensor product) and epilogue (e.g. a key product) into the
 // transform's first load and last store, which are always coalesced
 // (consecutive threads touch consecutive j).
@@ -25,24 +26,48 @@ typedef ulonglong2 tw_t;  // (w, floor(w * 2^64 / q))
 
 __device__ __forceinline__ int spad(int j) { return j + (j >> 4); }
 
-__device__ __forceinline__ void ct_bfly(uint64_t& a, uint64_t& b, tw_t w, uint64_t q, uint64_t q2) {
-    uint64_t v = shoup_lazy(b, w.x, w.y, q);
-    a = a >= q2 ? a - q2 : a;
-    b = a + q2 - v;
-    a = a + v;
+// Shoup product with a quotient estimate from three 32-bit partial products
+// of b * ws (b1*w1, hi(b1*w0), hi(b0*w1)): the dropped terms make the
+// estimate low by at most 3, so the result is b*w mod q plus at most 3q,
+// i.e. in [0, 4q). Any 64-bit b is allowed.
+__device__ __forceinline__ uint64_t shoup4(uint64_t b, uint64_t w, uint64_t ws, uint64_t q) {
+    const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    const uint32_t w0 = (uint32_t)ws, w1 = (uint32_t)(ws >> 32);
+    const uint64_t est = (uint64_t)b1 * w1 + (uint64_t)__umulhi(b1, w0) + (uint64_t)__umulhi(b0, w1);
+    return b * w - est * q;
 }
 
-__device__ __forceinline__ void gs_bfly(uint64_t& a, uint64_t& b, tw_t w, uint64_t q, uint64_t q2) {
-    uint64_t t = a + q2 - b;
-    uint64_t s = a + b;
-    a = s >= q2 ? s - q2 : s;
-    b = shoup_lazy(t, w.x, w.y, q);
+// a - c if that is non-negative, else a; a, c < 2^63
+__device__ __forceinline__ uint64_t csub63(uint64_t a, uint64_t c) {
+    const int64_t t = (int64_t)(a - c);
+    return t < 0 ? a : (uint64_t)t;
+}
+
+// Forward Cooley-Tukey butterfly; values stay in [0, 8q) (q < 2^60 keeps 8q < 2^63).
+__device__ __forceinline__ void ct_bfly(uint64_t& a, uint64_t& b, tw_t w, uint64_t q, uint64_t q4) {
+    const uint64_t v = shoup4(b, w.x, w.y, q);  // [0, 4q)
+    a = csub63(a, q4);                          // [0, 4q)
+    b = a + q4 - v;                             // (0, 8q)
+    a = a + v;                                  // [0, 8q)
+}
+
+// Inverse Gentleman-Sande butterfly; values stay in [0, 4q).
+__device__ __forceinline__ void gs_bfly(uint64_t& a, uint64_t& b, tw_t w, uint64_t q, uint64_t q4) {
+    const uint64_t t = a + q4 - b;   // (0, 8q)
+    a = csub63(a + b, q4);           // [0, 4q)
+    b = shoup4(t, w.x, w.y, q);      // [0, 4q)
+}
+
+__device__ __forceinline__ uint64_t reduce_from(uint64_t v, uint64_t q, int log_mult) {
+    // v < 2^log_mult * q -> [0, q)
+    for (int m = log_mult - 1; m >= 0; m--) v = csub63(v, q << m);
+    return v;
 }
 
 // R forward stages on 2^R registers; stage s0+u uses psi_br[2^(s0+u) + (hi << u) + h].
 template <int R>
 __device__ __forceinline__ void fwd_group(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi,
-                                          uint64_t q, uint64_t q2) {
+                                          uint64_t q, uint64_t q4) {
 #pragma unroll
     for (int u = 0; u < R; u++) {
         const int half = 1 << (R - 1 - u);
@@ -53,32 +78,30 @@ __device__ __forceinline__ void fwd_group(uint64_t* x, const tw_t* __restrict__ 
 #pragma unroll
             for (int k = 0; k < half; k++) {
                 const int i0 = h * 2 * half + k;
-                ct_bfly(x[i0], x[i0 + half], w, q, q2);
+                ct_bfly(x[i0], x[i0 + half], w, q, q4);
             }
         }
     }
 }
 
-// R inverse stages (reverse order); `fold` applies n^-1 at global stage 0
-// using tw[0] = n^-1 and tw[1] = psi^-1 * n^-1, and fully reduces.
+// R inverse stages (reverse order). `fold` (only with s0 == 0, hi == 0) applies
+// n^-1 at global stage 0 using tw[0] = n^-1, tw[1] = psi_br^-1[1] * n^-1 and
+// fully reduces.
 template <int R>
 __device__ __forceinline__ void inv_group(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi,
-                                          uint64_t q, uint64_t q2, bool fold) {
+                                          uint64_t q, uint64_t q4, bool fold) {
 #pragma unroll
     for (int u = R - 1; u >= 0; u--) {
         const int half = 1 << (R - 1 - u);
         const int bidx = (1 << (s0 + u)) + (hi << u);
         if (fold && u == 0) {
-            // s0 == 0 and hi == 0 here: a single butterfly column with psi^-1 at index 1
             const tw_t ni = tw[0];
             const tw_t w1 = tw[1];
 #pragma unroll
             for (int k = 0; k < half; k++) {
-                uint64_t a = x[k], b = x[k + half];
-                uint64_t s = a + b;
-                uint64_t t = a + q2 - b;
-                x[k] = csub(shoup_lazy(s, ni.x, ni.y, q), q);
-                x[k + half] = csub(shoup_lazy(t, w1.x, w1.y, q), q);
+                const uint64_t a = x[k], b = x[k + half];
+                x[k] = reduce_from(shoup4(a + b, ni.x, ni.y, q), q, 2);
+                x[k + half] = reduce_from(shoup4(a + q4 - b, w1.x, w1.y, q), q, 2);
             }
         } else {
 #pragma unroll
@@ -87,105 +110,117 @@ __device__ __forceinline__ void inv_group(uint64_t* x, const tw_t* __restrict__ 
 #pragma unroll
                 for (int k = 0; k < half; k++) {
                     const int i0 = h * 2 * half + k;
-                    gs_bfly(x[i0], x[i0 + half], w, q, q2);
+                    gs_bfly(x[i0], x[i0 + half], w, q, q4);
                 }
             }
         }
     }
 }
 
-__device__ __forceinline__ uint64_t reduce4q(uint64_t v, uint64_t q, uint64_t q2) {
-    v = v >= q2 ? v - q2 : v;
-    return v >= q ? v - q : v;
-}
-
 // ---------------------------------------------------------------------------
 // Block kernels. The CTA handles block `blk` of row `row`; the block holds
 // global indices [blk << LOGB, (blk + 1) << LOGB) of a length-2^logn transform
 // and runs global stages [logn - LOGB, logn). With logn == LOGB this is the
-// whole transform.
+// whole transform. T = 2^LOGB / 16 threads, each owning 16 points; a pass of
+// R <= RAD stages processes 16 / 2^R register groups per thread. Group gi of a
+// pass starting at local stage S0 holds the points
+//   ((gi >> lb) << (lb + R)) | (gi & (2^lb - 1)) + k * 2^lb,  lb = LOGB - S0 - R,
+// and thread t takes gi = g * T + t; with one pad word per 16 points every
+// shared-memory access of every pass is free of bank conflicts.
 // ---------------------------------------------------------------------------
 template <int LOGB>
 struct BlockShape {
     static constexpr int NB = 1 << LOGB;
     static constexpr int THREADS = NB / 16;
     static constexpr int SMEM_BYTES = (NB + NB / 16) * 8;
+    // radix of the register groups: 8 points at 1024 threads (64 registers), else 16
+    static constexpr int RAD = LOGB >= 14 ? 3 : 4;
 };
 
-template <int LOGB, class Src, class Dst>
-__global__ void __launch_bounds__(1 << (LOGB - 4))
-ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
-                     int logn) {
-    constexpr int NB = 1 << LOGB, T = NB / 16;
-    extern __shared__ uint64_t sm[];
-    const int nblk = 1 << (logn - LOGB);
-    const int row = blockIdx.x / nblk;
-    const int blk = blockIdx.x % nblk;
-    const int t = threadIdx.x;
-    const int pidx = src.prime(row);
-    const auto s = src.bind(row);
-    const auto d = dst.bind(row);
-    const uint64_t q = mods[pidx], q2 = q << 1;
-    const tw_t* tw = tw_all + ((size_t)pidx << logn);
-    const int sbase = logn - LOGB;   // first global stage handled here
-    const int goff = blk << LOGB;    // global index of local 0
-    uint64_t x[16];
+struct PassCtx {
+    uint64_t* sm;
+    const tw_t* tw;
+    int t, sbase, goff, logn;
+    uint64_t q, q4;
+};
 
-    // pass 0: local stride NB/16, elements t + k*T (coalesced loads)
+// padded index of lbase + (k << lb); for lb >= 4 the offset is a constant
+template <int LB>
+__device__ __forceinline__ int spad_off(int pbase, int lbase, int k) {
+    if constexpr (LB >= 4) return pbase + k * ((1 << LB) + (1 << (LB - 4)));
+    else return spad(lbase + (k << LB));
+}
+
+template <int LOGB, int S0, int R>
+__device__ __forceinline__ int group_base(int gi) {
+    constexpr int lb = LOGB - S0 - R;
+    return ((gi >> lb) << (lb + R)) | (gi & ((1 << lb) - 1));
+}
+
+// one forward pass over shared memory
+template <int LOGB, int S0, int R>
+__device__ __forceinline__ void fwd_pass_smem(const PassCtx& c) {
+    constexpr int T = (1 << LOGB) / 16, G = 1 << R, NG = 16 / G, lb = LOGB - S0 - R;
 #pragma unroll
-    for (int k = 0; k < 16; k++) x[k] = s.load(goff + t + k * T);
-    fwd_group<4>(x, tw, sbase, goff >> (logn - sbase), q, q2);
+    for (int g = 0; g < NG; g++) {
+        const int lbase = group_base<LOGB, S0, R>(g * T + c.t);
+        const int pbase = spad(lbase);
+        uint64_t x[G];
 #pragma unroll
-    for (int k = 0; k < 16; k++) sm[spad(t + k * T)] = x[k];
+        for (int k = 0; k < G; k++) x[k] = c.sm[spad_off<lb>(pbase, lbase, k)];
+        const int s0 = c.sbase + S0;
+        fwd_group<R>(x, c.tw, s0, (c.goff + lbase) >> (c.logn - s0), c.q, c.q4);
+#pragma unroll
+        for (int k = 0; k < G; k++) c.sm[spad_off<lb>(pbase, lbase, k)] = x[k];
+    }
     __syncthreads();
+}
 
-    // middle passes (full radix-16)
-#pragma unroll
-    for (int ls0 = 4; ls0 + 4 <= LOGB; ls0 += 4) {
-        const int lowbits = LOGB - ls0 - 4;
-        const int stride = 1 << lowbits;
-        const int lbase = ((t >> lowbits) << (lowbits + 4)) | (t & (stride - 1));
-        const int s0 = sbase + ls0;
-#pragma unroll
-        for (int k = 0; k < 16; k++) x[k] = sm[spad(lbase + k * stride)];
-        fwd_group<4>(x, tw, s0, (goff + lbase) >> (logn - s0), q, q2);
-#pragma unroll
-        for (int k = 0; k < 16; k++) sm[spad(lbase + k * stride)] = x[k];
-        __syncthreads();
-    }
-
-    // tail pass: remaining R = LOGB % 4 stages on consecutive groups
-    constexpr int R = LOGB % 4;
-    if (R > 0) {
-        constexpr int RR = R > 0 ? R : 1;
-        constexpr int G = 16 >> RR;
-        const int s0 = sbase + LOGB - RR;
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-            const int gidx = g * T + t;  // group index within block
-            uint64_t y[1 << RR];
-#pragma unroll
-            for (int k = 0; k < (1 << RR); k++) y[k] = sm[spad((gidx << RR) + k)];
-            fwd_group<RR>(y, tw, s0, (goff >> RR) + gidx, q, q2);
-#pragma unroll
-            for (int k = 0; k < (1 << RR); k++) sm[spad((gidx << RR) + k)] = y[k];
-        }
-        __syncthreads();
-    }
-
-    // coalesced write-out with full reduction
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        const int j = t + k * T;
-        d.store(goff + j, reduce4q(sm[spad(j)], q, q2));
+template <int LOGB, int RAD, int S0>
+__device__ __forceinline__ void fwd_passes(const PassCtx& c) {
+    if constexpr (S0 < LOGB) {
+        constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
+        fwd_pass_smem<LOGB, S0, R>(c);
+        fwd_passes<LOGB, RAD, S0 + R>(c);
     }
 }
 
-template <int LOGB, class Src, class Dst>
+template <int LOGB, int S0, int R>
+__device__ __forceinline__ void inv_pass_smem(const PassCtx& c) {
+    constexpr int T = (1 << LOGB) / 16, G = 1 << R, NG = 16 / G, lb = LOGB - S0 - R;
+    // groups one after another: keeps the 1024-thread variant within 64 registers
+#pragma unroll 1
+    for (int g = 0; g < NG; g++) {
+        const int lbase = group_base<LOGB, S0, R>(g * T + c.t);
+        const int pbase = spad(lbase);
+        uint64_t x[G];
+#pragma unroll
+        for (int k = 0; k < G; k++) x[k] = c.sm[spad_off<lb>(pbase, lbase, k)];
+        const int s0 = c.sbase + S0;
+        inv_group<R>(x, c.tw, s0, (c.goff + lbase) >> (c.logn - s0), c.q, c.q4, false);
+#pragma unroll
+        for (int k = 0; k < G; k++) c.sm[spad_off<lb>(pbase, lbase, k)] = x[k];
+    }
+    __syncthreads();
+}
+
+// inverse passes with S0 >= first, run from the last stages back to `first`
+template <int LOGB, int RAD, int S0>
+__device__ __forceinline__ void inv_passes(const PassCtx& c) {
+    if constexpr (S0 < LOGB) {
+        constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
+        inv_passes<LOGB, RAD, S0 + R>(c);
+        inv_pass_smem<LOGB, S0, R>(c);
+    }
+}
+
+// FULL: fully reduce the output to [0, q); otherwise outputs are in [0, 8q).
+template <int LOGB, class Src, class Dst, bool FULL = true>
 __global__ void __launch_bounds__(1 << (LOGB - 4))
-ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
+ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
                      int logn) {
-    constexpr int NB = 1 << LOGB, T = NB / 16;
+    constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
+    constexpr int R0 = RAD < LOGB ? RAD : LOGB, G0 = 1 << R0, lb0 = LOGB - R0;
     extern __shared__ uint64_t sm[];
     const int nblk = 1 << (logn - LOGB);
     const int row = blockIdx.x / nblk;
@@ -194,64 +229,76 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
-    const uint64_t q = mods[pidx], q2 = q << 1;
-    const tw_t* tw = tw_all + ((size_t)pidx << logn);
-    const int sbase = logn - LOGB;
-    const int goff = blk << LOGB;
-    const bool whole = (sbase == 0);
-    uint64_t x[16];
+    const uint64_t q = mods[pidx], q4 = q << 2;
+    PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
+
+    // pass 0 straight from global memory: groups gi + k * 2^lb0 (consecutive lanes, coalesced);
+    // groups one after another so fused loaders keep their temporaries in registers
+#pragma unroll 1
+    for (int g = 0; g < 16 / G0; g++) {
+        const int gi = g * T + t;
+        uint64_t x[G0];
+#pragma unroll
+        for (int k = 0; k < G0; k++) x[k] = s.load(c.goff + gi + (k << lb0));
+        fwd_group<R0>(x, c.tw, c.sbase, c.goff >> LOGB, q, q4);
+        const int pg = spad(gi);
+#pragma unroll
+        for (int k = 0; k < G0; k++) sm[spad_off<lb0>(pg, gi, k)] = x[k];
+    }
+    __syncthreads();
+    fwd_passes<LOGB, RAD, R0>(c);
+    // coalesced write-out
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int j = t + k * T;
+        const uint64_t v = sm[spad(j)];
+        d.store(c.goff + j, FULL ? reduce_from(v, q, 3) : v);
+    }
+}
+
+// WHOLE: the block is the whole ring (logn == LOGB), so n^-1 is applied here.
+template <int LOGB, class Src, class Dst, bool WHOLE = true>
+__global__ void __launch_bounds__(1 << (LOGB - 4))
+ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
+                     int logn) {
+    constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
+    constexpr int R0 = RAD < LOGB ? RAD : LOGB, G0 = 1 << R0, lb0 = LOGB - R0;
+    extern __shared__ uint64_t sm[];
+    const int nblk = 1 << (logn - LOGB);
+    const int row = blockIdx.x / nblk;
+    const int blk = blockIdx.x % nblk;
+    const int t = threadIdx.x;
+    const int pidx = src.prime(row);
+    const auto s = src.bind(row);
+    const auto d = dst.bind(row);
+    const uint64_t q = mods[pidx], q4 = q << 2;
+    PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
 
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         const int j = t + k * T;
-        sm[spad(j)] = s.load(goff + j);
+        sm[spad(j)] = s.load(c.goff + j);
     }
     __syncthreads();
-
-    constexpr int R = LOGB % 4;
-    if (R > 0) {
-        constexpr int RR = R > 0 ? R : 1;
-        constexpr int G = 16 >> RR;
-        const int s0 = sbase + LOGB - RR;
+    inv_passes<LOGB, RAD, R0>(c);
+    // pass 0 (local stages 0..R0-1), coalesced stores
+#pragma unroll 1
+    for (int g = 0; g < 16 / G0; g++) {
+        const int gi = g * T + t;
+        uint64_t x[G0];
+        const int pg = spad(gi);
 #pragma unroll
-        for (int g = 0; g < G; g++) {
-            const int gidx = g * T + t;
-            uint64_t y[1 << RR];
+        for (int k = 0; k < G0; k++) x[k] = sm[spad_off<lb0>(pg, gi, k)];
+        inv_group<R0>(x, c.tw, c.sbase, c.goff >> LOGB, q, q4, WHOLE);
 #pragma unroll
-            for (int k = 0; k < (1 << RR); k++) y[k] = sm[spad((gidx << RR) + k)];
-            inv_group<RR>(y, tw, s0, (goff >> RR) + gidx, q, q2, false);
-#pragma unroll
-            for (int k = 0; k < (1 << RR); k++) sm[spad((gidx << RR) + k)] = y[k];
-        }
-        __syncthreads();
+        for (int k = 0; k < G0; k++) d.store(c.goff + gi + (k << lb0), x[k]);
     }
-
-    // middle passes, last stages first
-#pragma unroll
-    for (int ls0 = ((LOGB - R) - 4); ls0 >= 4; ls0 -= 4) {
-        const int lowbits = LOGB - ls0 - 4;
-        const int stride = 1 << lowbits;
-        const int lbase = ((t >> lowbits) << (lowbits + 4)) | (t & (stride - 1));
-        const int s0 = sbase + ls0;
-#pragma unroll
-        for (int k = 0; k < 16; k++) x[k] = sm[spad(lbase + k * stride)];
-        inv_group<4>(x, tw, s0, (goff + lbase) >> (logn - s0), q, q2, false);
-#pragma unroll
-        for (int k = 0; k < 16; k++) sm[spad(lbase + k * stride)] = x[k];
-        __syncthreads();
-    }
-
-    // pass 0 (local stages 0..3), coalesced stores
-#pragma unroll
-    for (int k = 0; k < 16; k++) x[k] = sm[spad(t + k * T)];
-    inv_group<4>(x, tw, sbase, goff >> (logn - sbase), q, q2, whole);
-#pragma unroll
-    for (int k = 0; k < 16; k++) d.store(goff + t + k * T, x[k]);
 }
 
 // ---------------------------------------------------------------------------
 // Column pass for rings larger than one block: the first (forward) or last
 // (inverse) RC = logn - LOGB stages, elementwise over 2^RC-point columns.
+// Forward outputs are in [0, 8q); inverse inputs may be in [0, 4q).
 // ---------------------------------------------------------------------------
 template <int RC, class Src, class Dst>
 __global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
@@ -263,12 +310,12 @@ __global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
-    const uint64_t q = mods[pidx], q2 = q << 1;
+    const uint64_t q = mods[pidx], q4 = q << 2;
     const tw_t* tw = tw_all + ((size_t)pidx << logn);
     uint64_t x[1 << RC];
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) x[k] = s.load(c + k * cols);
-    fwd_group<RC>(x, tw, 0, 0, q, q2);
+    fwd_group<RC>(x, tw, 0, 0, q, q4);
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) d.store(c + k * cols, x[k]);
 }
@@ -283,12 +330,12 @@ __global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
-    const uint64_t q = mods[pidx], q2 = q << 1;
+    const uint64_t q = mods[pidx], q4 = q << 2;
     const tw_t* tw = tw_all + ((size_t)pidx << logn);
     uint64_t x[1 << RC];
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) x[k] = s.load(c + k * cols);
-    inv_group<RC>(x, tw, 0, 0, q, q2, true);
+    inv_group<RC>(x, tw, 0, 0, q, q4, true);
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) d.store(c + k * cols, x[k]);
 }
