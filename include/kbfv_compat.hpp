@@ -1,0 +1,222 @@
+// kbfv_compat.hpp -- kunpBFV's class API (BFVContext, BFVScheme, Plaintext,
+// Ciphertext, SecretKey) rebuilt on the C ABI in kbfv.h, so drivers written for
+// kunpBFV (correct_mult.cu, perf_mult.cu) run on the B200 path with only their
+// #includes changed. Header-only; link libkbfv.so and cudart.
+//
+// Behaviour kept from the reference: encode() overwrites its input with the
+// plaintext coefficients (include/Encoder.cuh:32), encode_ntt() takes
+// coefficients, errors throw std::invalid_argument / std::runtime_error.
+// Behaviour not kept: multAndEqual_23 computes a genuine relinearised product
+// (the reference overwrites it with ct1 * Dec(ct2), include/KeySwitch_23.cuh:308).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+#include <string>
+
+#include "kbfv.h"
+
+namespace kbfv_compat {
+
+typedef unsigned long long uint64_tt;
+
+inline void check(int rc) {
+    if (rc == KBFV_OK) return;
+    std::string m = kbfv_last_error();
+    if (rc == KBFV_ERR_INVALID || rc == KBFV_ERR_LEVEL || rc == KBFV_ERR_NO_KEY) throw std::invalid_argument(m);
+    throw std::runtime_error(m);
+}
+
+inline void check_cuda(cudaError_t e) {
+    if (e != cudaSuccess) throw std::runtime_error(cudaGetErrorString(e));
+}
+
+class BFVContext;
+
+class Plaintext {
+public:
+    uint64_tt* mx_device = nullptr;  // (L+1) x N words: coefficients in the first N, or NTT form over Q
+    int N = 0, L = 0, l = 0, slots = 0;
+    Plaintext() = default;
+    Plaintext(int N_, int L_, int l_, int slots_) : N(N_), L(L_), l(l_), slots(slots_) {
+        check_cuda(cudaMalloc(&mx_device, sizeof(uint64_tt) * N * (L + 1)));
+        check_cuda(cudaMemset(mx_device, 0, sizeof(uint64_tt) * N * (L + 1)));
+    }
+    Plaintext(const Plaintext&) = delete;
+    Plaintext& operator=(const Plaintext&) = delete;
+    ~Plaintext() { if (mx_device) cudaFree(mx_device); }
+};
+
+class Ciphertext {
+public:
+    uint64_tt* cipher_device = nullptr;  // [ax | bx], (L+1) x N words each, NTT form over Q
+    uint64_tt* ax_device = nullptr;
+    uint64_tt* bx_device = nullptr;
+    int N = 0, L = 0, l = 0, slots = 0;
+    Ciphertext() = default;
+    Ciphertext(int N_, int L_, int l_, int slots_) : N(N_), L(L_), l(l_), slots(slots_) {
+        check_cuda(cudaMalloc(&cipher_device, sizeof(uint64_tt) * N * (L + 1) * 2));
+        ax_device = cipher_device;
+        bx_device = cipher_device + (size_t)N * (L + 1);
+    }
+    Ciphertext(const Ciphertext&) = delete;
+    Ciphertext& operator=(const Ciphertext&) = delete;
+    ~Ciphertext() { if (cipher_device) cudaFree(cipher_device); }
+};
+
+class BFVContext {
+public:
+    kbfv_context* handle = nullptr;
+    long N = 0;
+    int logN = 0, L = 0, K = 0, slots = 0, q_num = 0, p_num = 0, dnum = 0;
+    uint64_tt plain_modulus = 0;
+
+    // the reference's parameter set for this ring degree (include/Params.cuh)
+    explicit BFVContext(size_t poly_modulus_degree) {
+        const int lg = (int)std::lround(std::log2((double)poly_modulus_degree));
+        check(kbfv_context_create_reference((uint32_t)lg, &handle));
+        fill();
+    }
+    explicit BFVContext(const kbfv_params& p) {
+        check(kbfv_context_create(&p, &handle));
+        fill();
+    }
+    BFVContext(const BFVContext&) = delete;
+    BFVContext& operator=(const BFVContext&) = delete;
+    ~BFVContext() { if (handle) kbfv_context_destroy(handle); }
+
+    // INTT mod t into msg; like the reference, `vals` is overwritten with the coefficients
+    void encode(uint64_tt* vals, Plaintext& msg) {
+        check(kbfv_encode(handle, reinterpret_cast<const uint64_t*>(vals), reinterpret_cast<uint64_t*>(msg.mx_device),
+                          1, 0));
+        check_cuda(cudaMemcpy(vals, msg.mx_device, sizeof(uint64_tt) * N, cudaMemcpyDeviceToDevice));
+    }
+    // coefficients -> NTT form over Q (for multConstAndEqual)
+    void encode_ntt(uint64_tt* vals, Plaintext& msg) {
+        check(kbfv_encode_ntt(handle, reinterpret_cast<const uint64_t*>(vals),
+                              reinterpret_cast<uint64_t*>(msg.mx_device), 1, 0));
+    }
+    void decode(Plaintext& msg, uint64_tt* vals) {
+        check(kbfv_decode(handle, reinterpret_cast<const uint64_t*>(msg.mx_device), reinterpret_cast<uint64_t*>(vals),
+                          1, 0));
+    }
+
+private:
+    void fill() {
+        uint64_t n;
+        uint32_t nq, np, nr, nt, dn, al;
+        check(kbfv_context_info(handle, &n, &nq, &np, &nr, &nt, &dn, &al));
+        N = (long)n;
+        logN = (int)std::lround(std::log2((double)n));
+        q_num = (int)nq;
+        p_num = (int)np;
+        L = q_num - 1;
+        K = p_num;
+        dnum = (int)dn;
+        slots = (int)N;
+        plain_modulus = kbfv_context_plain_modulus(handle);
+    }
+};
+
+class SecretKey {
+public:
+    uint64_tt* sx_device = nullptr;  // (K+L+1) x N words, NTT form over Q|P
+    int N = 0, L = 0, K = 0;
+    uint8_t seed[32];
+    // Hamming-weight-64 ternary secret as in the reference (include/SecretKey.cuh:31);
+    // the seed is drawn from std::random_device unless given
+    explicit SecretKey(BFVContext& ctx, cudaStream_t stream = 0, const uint8_t* seed_in = nullptr)
+        : N((int)ctx.N), L(ctx.L), K(ctx.K) {
+        if (seed_in) std::memcpy(seed, seed_in, 32);
+        else {
+            std::random_device rd;
+            for (int i = 0; i < 32; i++) seed[i] = (uint8_t)rd();
+        }
+        check_cuda(cudaMalloc(&sx_device, sizeof(uint64_tt) * N * (K + L + 1)));
+        check(kbfv_keygen_secret(ctx.handle, seed, 1, 64, reinterpret_cast<uint64_t*>(sx_device), stream));
+    }
+    SecretKey(const SecretKey&) = delete;
+    SecretKey& operator=(const SecretKey&) = delete;
+    ~SecretKey() { if (sx_device) cudaFree(sx_device); }
+};
+
+class BFVScheme {
+public:
+    BFVContext& context;
+    uint64_tt* publicKey = nullptr;
+    uint64_tt* rlk_23 = nullptr;
+    uint64_t enc_counter = 0;
+    uint8_t seed[32];
+
+    explicit BFVScheme(BFVContext& ctx) : context(ctx) {
+        std::random_device rd;
+        for (int i = 0; i < 32; i++) seed[i] = (uint8_t)rd();
+    }
+    BFVScheme(const BFVScheme&) = delete;
+    BFVScheme& operator=(const BFVScheme&) = delete;
+    ~BFVScheme() {
+        if (publicKey) cudaFree(publicKey);
+        if (rlk_23) cudaFree(rlk_23);
+    }
+
+    void mallocMemory() { check(kbfv_reserve(context.handle, 1)); }
+
+    void addEncKey(SecretKey& sk, cudaStream_t stream = 0) {
+        if (!publicKey) check_cuda(cudaMalloc(&publicKey, sizeof(uint64_tt) * context.N * context.q_num * 2));
+        check(kbfv_keygen_public(context.handle, seed, reinterpret_cast<const uint64_t*>(sk.sx_device),
+                                 reinterpret_cast<uint64_t*>(publicKey), stream));
+    }
+    void addMultKey_23(SecretKey& sk, cudaStream_t stream = 0) {
+        if (rlk_23) return;
+        const size_t words = (size_t)context.dnum * 2 * (context.q_num + context.p_num) * context.N;
+        check_cuda(cudaMalloc(&rlk_23, sizeof(uint64_tt) * words));
+        check(kbfv_keygen_relin(context.handle, seed, reinterpret_cast<const uint64_t*>(sk.sx_device),
+                                reinterpret_cast<uint64_t*>(rlk_23), stream));
+    }
+    // rotation keys are outside this path; accepted and ignored
+    void addLeftRotKey_23(SecretKey&, long, cudaStream_t = 0) {}
+
+    void encryptMsg(Ciphertext& cipher, Plaintext& message, cudaStream_t stream = 0) {
+        if (!publicKey) throw std::invalid_argument("public key not generated");
+        cipher.l = message.l;
+        check(kbfv_encrypt(context.handle, seed, enc_counter++, reinterpret_cast<const uint64_t*>(publicKey),
+                           reinterpret_cast<const uint64_t*>(message.mx_device),
+                           reinterpret_cast<uint64_t*>(cipher.cipher_device), 1, stream));
+    }
+    void decryptMsg(Plaintext& plain, SecretKey& sk, Ciphertext& cipher, cudaStream_t stream = 0) {
+        plain.l = cipher.l;
+        check(kbfv_decrypt(context.handle, reinterpret_cast<const uint64_t*>(sk.sx_device),
+                           reinterpret_cast<const uint64_t*>(cipher.cipher_device),
+                           reinterpret_cast<uint64_t*>(plain.mx_device), 1, stream));
+    }
+    void add(Ciphertext& res, Ciphertext& c1, Ciphertext& c2) {
+        res.l = std::min(c1.l, c2.l);
+        check(kbfv_add(context.handle, reinterpret_cast<const uint64_t*>(c1.cipher_device),
+                       reinterpret_cast<const uint64_t*>(c2.cipher_device),
+                       reinterpret_cast<uint64_t*>(res.cipher_device), 1, 0));
+    }
+    void addAndEqual(Ciphertext& c1, Ciphertext& c2) { add(c1, c1, c2); }
+    void multConstAndEqual(Ciphertext& cipher, Plaintext& cnst) {
+        if (cipher.l == 0) throw std::invalid_argument("Ciphertexts are on level 0");
+        check(kbfv_mul_plain(context.handle, reinterpret_cast<const uint64_t*>(cipher.cipher_device),
+                             reinterpret_cast<const uint64_t*>(cnst.mx_device),
+                             reinterpret_cast<uint64_t*>(cipher.cipher_device), 1, 0));
+    }
+    void mult_23(Ciphertext& res, Ciphertext& c1, Ciphertext& c2) {
+        if (c1.l == 0 || c2.l == 0) throw std::invalid_argument("Ciphertexts are on level 0");
+        if (!rlk_23) throw std::invalid_argument("rotKey_23 not exists");
+        res.l = std::min(c1.l, c2.l);
+        check(kbfv_mul_relin(context.handle, reinterpret_cast<const uint64_t*>(rlk_23),
+                             reinterpret_cast<const uint64_t*>(c1.cipher_device),
+                             reinterpret_cast<const uint64_t*>(c2.cipher_device),
+                             reinterpret_cast<uint64_t*>(res.cipher_device), 1, 0));
+    }
+    void multAndEqual_23(Ciphertext& c1, Ciphertext& c2) { mult_23(c1, c1, c2); }
+};
+
+}  // namespace kbfv_compat
