@@ -549,6 +549,17 @@ struct PairQRowsP {
     }
 };
 
+// rows of consecutive Q|R polynomials; limb l of Q|R uses prime l (Q) or idx_r + l - nq (R)
+struct QRRowsIO {
+    uint64_t* base;
+    int logn, nq, nqr, idx_r;
+    __device__ __forceinline__ int prime(int row) const {
+        const int l = row % nqr;
+        return l < nq ? l : idx_r + (l - nq);
+    }
+    __device__ __forceinline__ PtrRow bind(int row) const { return PtrRow{base + ((size_t)row << logn)}; }
+};
+
 // K4 source: tensor product of the pair at limb l of Q|R, one of three outputs
 struct TensorRow {
     const uint64_t *a1, *b1, *a2, *b2;
@@ -746,7 +757,7 @@ static void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratc
                                    count * 4 * dc.nr, st);
     // K4: tensor (Q part from the NTT-form inputs, R part from K3) fused into INTT over Q|R
     TensorSrc ts{pb, m.sb, dc};
-    ntt_inv(dc, ts, rows_io(dc, m.sc, 0, 1), count * 3 * dc.nqr, st);
+    ntt_inv(dc, ts, QRRowsIO{m.sc, dc.logn, dc.nq, dc.nqr, dc.idx_r}, count * 3 * dc.nqr, st);
 }
 
 static void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st) {
@@ -768,7 +779,7 @@ static void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb,
     ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                    count * dc.dnum * dc.npq, st);
     // K6b: inner product with the key fused into INTT over Q|P
-    ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc}, rows_io(dc, m.se, 0, 1), count * 2 * dc.npq, st);
+    ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
     // K7: mod down + add (cross | b1b2) fused into NTT over Q, written to the outputs
     ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
 }
@@ -784,8 +795,11 @@ struct TensorA2 {
     }
 };
 
+// Fused stages run as one block kernel for N <= 2^14; for N = 2^15, 2^16 the
+// fused loader feeds the column pass and the fused store target is read back
+// by the block kernel, which every functor here supports.
 static void require_batchable(const Context& c) {
-    KB_REQUIRE(c.logn <= 14, KBFV_ERR_UNSUPPORTED, "the fused multiply pipeline supports N <= 16384");
+    KB_REQUIRE(c.logn >= 10 && c.logn <= 16, KBFV_ERR_UNSUPPORTED, "ring degree outside 2^10..2^16");
 }
 
 // ===========================================================================
@@ -1339,7 +1353,7 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
             check_launch("modup");
             ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                            cnt * dc.dnum * dc.npq, st);
-            ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc}, rows_io(dc, m.se, 0, 1), cnt * 2 * dc.npq, st);
+            ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
             std::vector<uint64_t*> O(cnt);
             std::vector<const uint64_t*> Z(cnt);
             for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
