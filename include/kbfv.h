@@ -182,6 +182,26 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);
 
+/* ---- multiply without allocating -------------------------------------
+ * No counterpart in the reference. Same result as kbfv_mul_relin, for callers
+ * that must not allocate device memory during a call: services that fix their
+ * device-memory budget at start-up, code running where cudaMalloc is not
+ * allowed (inside a stream being captured into a CUDA graph, a host callback,
+ * an allocator hook), or pools that must not fragment. Its scratch is a
+ * statically sized device array inside libkbfv.so of KBFV_NOALLOC_SCRATCH_BYTES
+ * (40 MiB, held by every GPU that loads the library until exit): enough for 2
+ * pairs at N=16384 with 7 ciphertext primes and 1 special prime
+ * (kbfv_mul_relin_scratch_bytes gives the need). Larger requests return
+ * KBFV_ERR_INVALID and launch nothing; nothing on this path calls cudaMalloc,
+ * cudaFree or any allocating routine. All calls share the one array: calls
+ * that overlap on the GPU (several streams or contexts) race and must be
+ * serialised by the caller. The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress); make that first call outside any
+ * stream capture. The context's device must be current. */
+#define KBFV_NOALLOC_SCRATCH_BYTES ((size_t)40 << 20)
+int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                           uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
 /* invariant noise budget in bits of one ciphertext (host-side diagnostic, synchronous) */
 int kbfv_noise_budget(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, double* bits);
 

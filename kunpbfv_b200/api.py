@@ -121,6 +121,7 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_relinearize": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_batch": (I, [VP, VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
+        "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_noise_budget": (I, [VP, VP, VP, C.POINTER(C.c_double)]),
         "kbfv_salsa20_stream": (I, [U8P, U8P, u64, VP, C.c_size_t, I, VP]),
     }

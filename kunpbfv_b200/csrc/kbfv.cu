@@ -1407,6 +1407,64 @@ int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_c
     });
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// allocation-free multiply: scratch in a static device array
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) uint8_t g_noalloc_scratch[KBFV_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+constexpr int kMaxDevices = 64;
+static void* g_noalloc_addr[kMaxDevices];
+
+// Device address of the static scratch on the current device, resolved once per
+// device (the host-side symbol is only a handle, never a device address).
+static uint8_t* noalloc_scratch(int device) {
+    KB_REQUIRE(device >= 0 && device < kMaxDevices, KBFV_ERR_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            throw KbfvError(KBFV_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[device] = p;
+    }
+    return (uint8_t*)g_noalloc_addr[device];
+}
+
+extern "C" {
+
+int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                           uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_rlk, KBFV_ERR_NO_KEY, "relinearisation key missing");
+        KB_REQUIRE(d_ct_a && d_ct_b && d_out, KBFV_ERR_INVALID, "null ciphertext pointer");
+        if (count == 0) return;
+        KB_REQUIRE(count <= (uint32_t)kMaxBatch, KBFV_ERR_INVALID, "too many pairs for one allocation-free call");
+        const size_t need = mul_scratch_layout(c, (int)count, nullptr).bytes;
+        if (need > KBFV_NOALLOC_SCRATCH_BYTES)
+            throw KbfvError(KBFV_ERR_INVALID, "kbfv_mul_relin_noalloc: " + std::to_string(count) + " pair(s) need " +
+                                                  std::to_string(need) + " bytes of scratch; the static array holds " +
+                                                  std::to_string((size_t)KBFV_NOALLOC_SCRATCH_BYTES));
+        int dev = -1;
+        KB_CHECK_CUDA(cudaGetDevice(&dev));
+        KB_REQUIRE(dev == c.device, KBFV_ERR_INVALID, "the context's device is not current");
+        MulScratch m = mul_scratch_layout(c, (int)count, noalloc_scratch(dev));
+        // every scratch word is written before it is read: nothing to clear
+        PtrBatch pb;
+        std::memset(&pb, 0, sizeof pb);
+        const size_t stride = (size_t)2 * c.nq * c.n;
+        for (uint32_t i = 0; i < count; i++) {
+            pb.a[i] = d_ct_a + i * stride;
+            pb.b[i] = d_ct_b + i * stride;
+            pb.o[i] = d_out + i * stride;
+        }
+        mul_relin_chunk(c, d_rlk, pb, (int)count, m, S(stream));
+    });
+}
+
 int kbfv_noise_budget(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, double* bits) {
     return guarded([&] {
         Context& c = CX(ctx);
