@@ -47,19 +47,21 @@ def parse():
     ap.add_argument("--skip-extras", action="store_true", help="only the headline workload")
     ap.add_argument("--kernel", default=None, choices=["ntt16k", "ntt16k_inv", "pipeline1"],
                     help="run one kernel on a profiling-sized case and exit (for ncu)")
+    ap.add_argument("--rows", type=int, default=1024, help="rows for the ntt16k profiling cases")
+    ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
     return ap.parse_args()
 
 
 def run_kernel_case(args):
-    """Profiling cases: the forward / inverse NTT block kernel on 1024 rows of
-    N=16384 (128 MiB, above L2), or one batched multiply of 16 pairs."""
+    """Profiling cases: the forward / inverse NTT block kernel on --rows rows of
+    N=16384 (1024 rows = 128 MiB, above L2), or batched multiplies of --pairs pairs."""
     import torch
 
     import kunpbfv_b200 as kb
     qs, ps = c3_primes()
     ctx = kb.BFVContext(log_n=LOG_N, plain_modulus=T, q_count=NQ, q=qs, p_count=NP, p=ps, dnum=1)
     if args.kernel.startswith("ntt16k"):
-        rows = 1024
+        rows = args.rows
         x = torch.randint(0, 1 << 59, (rows, ctx.N), dtype=torch.int64, device="cuda")
         fn = ctx.ntt_inv if args.kernel.endswith("inv") else ctx.ntt_fwd
         for _ in range(args.steps):
@@ -72,7 +74,7 @@ def run_kernel_case(args):
         sch.addEncKey(sk)
         sch.addMultKey_23(sk)
         rng = np.random.default_rng(0)
-        v = rng.integers(0, T, size=(16, ctx.N), dtype=np.uint64)
+        v = rng.integers(0, T, size=(args.pairs, ctx.N), dtype=np.uint64)
         c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v))), enc_id=0)
         for _ in range(args.steps):
             sch.mult_relin(c1, c1)
@@ -439,10 +441,18 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     ms_ntt = time_cuda(lambda: ctx.ntt_fwd(x, ctx.idx_r, NQ + 1, stream=stream), stream, 10)
     alg = 16 * N * rows + 16 * N * (NQ + 1)
     ach = alg / (ms_ntt / 1e3) / 1e9
+    bfly = rows * (N // 2) * LOG_N
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of this launch at
+    # 2048 rows, from one ncu capture of `bench.py --kernel ntt16k --rows 2048`
+    traffic = 270467840 + 220812032 if rows == 2048 else None
     res["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                       "frac": round(ach / peak, 4), "traffic": None,
+                       "frac": round(ach / peak, 4), "traffic": traffic,
                        "kernel": f"ntt_fwd_block_kernel<14> on {rows} rows ({peak_kind} peak)",
-                       "ms_per_launch": round(ms_ntt, 4)}
+                       "ms_per_launch": round(ms_ntt, 4),
+                       "algorithmic_bytes": alg,
+                       "note": "60-bit Shoup butterflies are bound by the IMAD pipe, not HBM: ncu shows "
+                               "fmaheavy busy ~65% of elapsed with math-pipe throttling the top stall",
+                       "butterflies_per_s": round(bfly / (ms_ntt / 1e3), 0)}
     del x
 
     # standalone NTT, N=65536, 32 primes x 64 polynomials (1 GiB)
