@@ -182,6 +182,44 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);
 
+/* ---- key switch over the auxiliary T base (the reference's own method) ---
+ * Available when the context has T primes (kbfv_params.t_count), q_count is a
+ * multiple of p_count and dnum == q_count / p_count (the reference's parameter
+ * sets: kbfv_context_create_reference). Layouts (N words per limb):
+ *   T-form key    [a|b][digit][Ri block][T prime], NTT form over T
+ *   Qj digits     [poly][Qj block][T prime]
+ *   Ri blocks     [poly][Ri block][T prime]
+ * Qj block i = Q primes [i*p_count, (i+1)*p_count); Ri block b = P|Q primes in
+ * the reference's order (P first) [b*gamma, (b+1)*gamma).
+ * kbfv_context_klss: block counts and the T-form key size in words. */
+int kbfv_context_klss(const kbfv_context* ctx, uint32_t* ri_blocks, uint32_t* qj_blocks, uint64_t* key_words);
+/* addMultKey_23's key conversion (include/KeySwitch_23.cuh:55-65):
+ * relinearisation key [digit][a|b][Q|P] (NTT) -> T-form key */
+int kbfv_rlk_to_klss(kbfv_context* ctx, const uint64_t* d_rlk, uint64_t* d_rlk_t, kbfv_stream stream);
+/* modUpQjtoT_23 (include/BasisConv.cuh:86-151): [poly][Q] coefficient form -> Qj digits over T */
+int kbfv_klss_modup_qj_to_t(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                            kbfv_stream stream);
+/* modUpPQtoT_23 (include/BasisConv.cuh:11-79): [poly][Q|P] coefficient form -> Ri blocks over T */
+int kbfv_klss_modup_pq_to_t(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                            kbfv_stream stream);
+/* external_product_T (include/ExternalProduct.cuh:11-112) of NTT-form digits
+ * [count][Qj][T] with the T-form key, returned in COEFFICIENT form
+ * ([count][a|b][Ri][T]; the inverse NTT over T is fused) */
+int kbfv_klss_external_product(kbfv_context* ctx, const uint64_t* d_digits, const uint64_t* d_rlk_t,
+                               uint64_t* d_out, uint32_t count, kbfv_stream stream);
+/* modUpTtoPQl_23 (include/BasisConv.cuh:159-226): centred exact Ri blocks over T
+ * (coefficient form) -> [poly][Q|P] */
+int kbfv_klss_t_to_pq(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                      kbfv_stream stream);
+/* key switch of a1*a2 as multAndEqual_23 does it (include/KeySwitch_23.cuh:277-305):
+ * tensors -> ciphertexts, with the T-form key */
+int kbfv_relinearize_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64_t* d_tensor, uint64_t* d_ct,
+                          uint32_t count, kbfv_stream stream);
+/* multAndEqual_23 (include/KeySwitch_23.cuh:244-310) with the reference's key
+ * switch, as one batched launch sequence (consecutive ciphertexts) */
+int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                        uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
 /* ---- multiply without allocating -------------------------------------
  * No counterpart in the reference. Same result as kbfv_mul_relin, for callers
  * that must not allocate device memory during a call: services that fix their

@@ -122,6 +122,14 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_mul_relin_batch": (I, [VP, VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
+        "kbfv_context_klss": (I, [VP, C.POINTER(u32), C.POINTER(u32), U64P]),
+        "kbfv_rlk_to_klss": (I, [VP, VP, VP, VP]),
+        "kbfv_klss_modup_qj_to_t": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_klss_modup_pq_to_t": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_klss_external_product": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_klss_t_to_pq": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_relinearize_klss": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_mul_relin_klss": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_noise_budget": (I, [VP, VP, VP, C.POINTER(C.c_double)]),
         "kbfv_salsa20_stream": (I, [U8P, U8P, u64, VP, C.c_size_t, I, VP]),
     }
@@ -355,6 +363,37 @@ class BFVContext:
         polys = x.numel() // (npq * self.N)
         return self._op("kbfv_moddown", [x], self.zeros(polys, self.q_count, self.N), polys, stream)
 
+    # ---- key switch over the T base (the reference's KLSS)
+    def klss_info(self):
+        """(Ri blocks, Qj blocks, T-form key words); raises if the context has no T base."""
+        nri, nqj, kw = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        _check(lib().kbfv_context_klss(self._h, C.byref(nri), C.byref(nqj), C.byref(kw)))
+        return nri.value, nqj.value, kw.value
+
+    def klss_modup_qj_to_t(self, x, stream=None):
+        _, nqj, _ = self.klss_info()
+        polys = x.numel() // (self.q_count * self.N)
+        return self._op("kbfv_klss_modup_qj_to_t", [x], self.zeros(polys, nqj, self.t_count, self.N), polys, stream)
+
+    def klss_modup_pq_to_t(self, x, stream=None):
+        nri, _, _ = self.klss_info()
+        polys = x.numel() // ((self.q_count + self.p_count) * self.N)
+        return self._op("kbfv_klss_modup_pq_to_t", [x], self.zeros(polys, nri, self.t_count, self.N), polys, stream)
+
+    def klss_external_product(self, digits, key_t, stream=None):
+        nri, nqj, _ = self.klss_info()
+        count = digits.numel() // (nqj * self.t_count * self.N)
+        out = self.zeros(count, 2, nri, self.t_count, self.N)
+        _check(lib().kbfv_klss_external_product(self._h, _ptr(digits), _ptr(key_t), _ptr(out), count,
+                                                _stream_ptr(stream)))
+        return out
+
+    def klss_t_to_pq(self, x, stream=None):
+        nri, _, _ = self.klss_info()
+        polys = x.numel() // (nri * self.t_count * self.N)
+        npq = self.q_count + self.p_count
+        return self._op("kbfv_klss_t_to_pq", [x], self.zeros(polys, npq, self.N), polys, stream)
+
 
 def reference_context(log_n: int) -> BFVContext:
     """The reference's own parameter set for logN 14 or 15 (include/Params.cuh:31-145)."""
@@ -416,12 +455,20 @@ class Tensor3:
 class BFVScheme:
     """BFVScheme (include/BFVScheme.h:12-178) over one context."""
 
-    def __init__(self, ctx: BFVContext, seed: bytes = b"\x00" * 32):
+    def __init__(self, ctx: BFVContext, seed: bytes = b"\x00" * 32, relin: str = "hybrid"):
+        """relin: "hybrid" (digit lift over Q|P, the default) or "klss" (the
+        reference's key switch over the T base; needs a context with T primes)."""
+        if relin not in ("hybrid", "klss"):
+            raise ValueError("relin must be 'hybrid' or 'klss'")
         self.context = ctx
         self.seed = bytes(seed)
+        self.relin = relin
         self.publicKey = None
         self.rlk = None
+        self.rlk_t = None
         self._enc_counter = 0
+        if relin == "klss":
+            ctx.klss_info()
 
     def mallocMemory(self, pairs: int = 1):
         self.context.reserve(pairs)
@@ -437,6 +484,15 @@ class BFVScheme:
         self.rlk = ctx.zeros(ctx.dnum, 2, ctx.q_count + ctx.p_count, ctx.N)
         _check(lib().kbfv_keygen_relin(ctx.handle, _u8(self.seed), _ptr(sk.sx_device), _ptr(self.rlk),
                                        _stream_ptr(stream)))
+        if self.relin == "klss":
+            self.convert_rlk_klss(stream)
+
+    def convert_rlk_klss(self, stream=None):
+        """The T-form copy of self.rlk (addMultKey_23's conversion, KeySwitch_23.cuh:55-65)."""
+        ctx = self.context
+        nri, nqj, _ = ctx.klss_info()
+        self.rlk_t = ctx.zeros(2, nqj, nri, ctx.t_count, ctx.N)
+        _check(lib().kbfv_rlk_to_klss(ctx.handle, _ptr(self.rlk), _ptr(self.rlk_t), _stream_ptr(stream)))
 
     def encryptMsg(self, pt: Plaintext, enc_id: Optional[int] = None, stream=None) -> Ciphertext:
         if self.publicKey is None:
@@ -483,8 +539,12 @@ class BFVScheme:
             raise KbfvError(-5, "rotKey_23 not exists")
         cnt = t3.data.numel() // (3 * self.context.q_count * self.context.N)
         out = Ciphertext(self.context, count=cnt)
-        _check(lib().kbfv_relinearize(self.context.handle, _ptr(self.rlk), _ptr(t3.data), _ptr(out.cipher_device),
-                                      cnt, _stream_ptr(stream)))
+        if self.relin == "klss":
+            _check(lib().kbfv_relinearize_klss(self.context.handle, _ptr(self.rlk_t), _ptr(t3.data),
+                                               _ptr(out.cipher_device), cnt, _stream_ptr(stream)))
+        else:
+            _check(lib().kbfv_relinearize(self.context.handle, _ptr(self.rlk), _ptr(t3.data),
+                                          _ptr(out.cipher_device), cnt, _stream_ptr(stream)))
         return out
 
     def mult_relin(self, c1: Ciphertext, c2: Ciphertext, out: Optional[Ciphertext] = None, stream=None) -> Ciphertext:
@@ -492,8 +552,14 @@ class BFVScheme:
         if self.rlk is None:
             raise KbfvError(-5, "rotKey_23 not exists")
         out = out if out is not None else Ciphertext(self.context, count=c1.count)
-        _check(lib().kbfv_mul_relin(self.context.handle, _ptr(self.rlk), _ptr(c1.cipher_device),
-                                    _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count, _stream_ptr(stream)))
+        if self.relin == "klss":
+            _check(lib().kbfv_mul_relin_klss(self.context.handle, _ptr(self.rlk_t), _ptr(c1.cipher_device),
+                                             _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count,
+                                             _stream_ptr(stream)))
+        else:
+            _check(lib().kbfv_mul_relin(self.context.handle, _ptr(self.rlk), _ptr(c1.cipher_device),
+                                        _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count,
+                                        _stream_ptr(stream)))
         return out
 
     def mult_relin_ptrs(self, a_ptrs, b_ptrs, out_ptrs, stream=None):

@@ -50,6 +50,27 @@ struct DevConsts {
     int gauss_bound;
 };
 
+constexpr int kMaxBlk = 16;  // primes per block of the T-base key switch (p_count or gamma)
+constexpr int kMaxT = 12;    // T primes
+
+// Constants of the reference's key switch over the auxiliary T base (KLSS).
+// Qj blocks: block i = Q primes [i*np, (i+1)*np). Ri blocks: the P|Q primes in
+// the reference's order (P first, then Q), gamma per block.
+struct KlssConsts {
+    int nt, gamma, nri, nqj;
+    const uint64_t *qj_hatinv, *qj_hatinvs;  // [nqj][np]
+    const uint64_t* qj_hat_t;                // [nqj][nt][np]
+    const uint64_t* qj_mod_t;                // [nqj][nt]
+    const uint64_t *ri_hatinv, *ri_hatinvs;  // [nri][gamma]
+    const uint64_t* ri_hat_t;                // [nri][nt][gamma]
+    const uint64_t* ri_mod_t;                // [nri][nt]
+    const uint64_t *thatinv, *thatinvs;      // [nt]: (T/t_k)^-1 mod t_k
+    const uint64_t* that_pq;                 // [npq][nt]: T/t_k mod r_m, m in reference order
+    const uint64_t* t_pq;                    // [npq]: T mod r_m
+    const uint64_t* halft_t;                 // [nt]: floor(T/2) mod t_k
+    const uint64_t* halft_pq;                // [npq]: floor(T/2) mod r_m
+};
+
 struct Context {
     // parameters
     int logn = 0;
@@ -75,6 +96,10 @@ struct Context {
     cudaEvent_t ptrs_event = nullptr;
     std::mutex mu;
     int device = 0;
+    // T-base key switch: available when T primes are given and its blocks
+    // line up with the hybrid digits (alpha == p_count, dnum == q_count / p_count)
+    bool klss_ok = false;
+    KlssConsts kc{};
 };
 
 }  // namespace kbfv

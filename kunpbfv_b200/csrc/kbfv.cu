@@ -16,6 +16,7 @@
 #include "host_math.hpp"
 #include "kernels.cuh"
 #include "ntt.cuh"
+#include "klss.cuh"
 
 using namespace kbfv;
 namespace H = kbfv::host;
@@ -339,6 +340,71 @@ static void build_context(Context& c, const kbfv_params& prm) {
     }
     size_t o_ks[10] = {blob.add(pmq), blob.add(pinv), blob.add(pinvs), blob.add(phi), blob.add(phis),
                        blob.add(phm), blob.add(dhi), blob.add(dhis), blob.add(dhm), blob.add(dqm)};
+    // T-base key switch constants (include/BasisConv.cuh:11-226; the reference's
+    // precompute is in include/BFVcontext.cuh). Blocks lift by approximate CRT:
+    // (B/b_j)^-1 mod b_j, B/b_j mod t_k and B mod t_k per block B.
+    c.klss_ok = c.nt > 0 && c.nt <= kMaxT && c.np <= kMaxBlk && c.gamma >= 1 && c.gamma <= kMaxBlk &&
+                c.nq % c.np == 0 && c.alpha == c.np && c.dnum == c.nq / c.np;
+    size_t o_kl[14] = {};
+    if (c.klss_ok) {
+        const int nt = c.nt, g = c.gamma, nqj = c.nq / c.np, nri = (npq + g - 1) / g;
+        const std::vector<uint64_t> Tm(c.mods.begin() + c.nq + c.np + c.nr, c.mods.begin() + c.nq + c.np + c.nr + nt);
+        std::vector<uint64_t> PQr;  // reference order: P then Q
+        PQr.insert(PQr.end(), P.begin(), P.end());
+        PQr.insert(PQr.end(), Q.begin(), Q.end());
+        auto lift = [&](const uint64_t* blk, int w, int stride, uint64_t* hinv, uint64_t* hinvs, uint64_t* hat_t,
+                        uint64_t* mod_t) {
+            for (int j = 0; j < w; j++) {
+                uint64_t h = 1;
+                for (int k = 0; k < w; k++) if (k != j) h = H::mulmod(h, blk[k] % blk[j], blk[j]);
+                hinv[j] = H::invmod(h, blk[j]);
+                hinvs[j] = H::shoup(hinv[j], blk[j]);
+            }
+            for (int t = 0; t < nt; t++) {
+                uint64_t bm = 1;
+                for (int j = 0; j < w; j++) {
+                    uint64_t h = 1;
+                    for (int k = 0; k < w; k++) if (k != j) h = H::mulmod(h, blk[k] % Tm[t], Tm[t]);
+                    hat_t[(size_t)t * stride + j] = h;
+                    bm = H::mulmod(bm, blk[j] % Tm[t], Tm[t]);
+                }
+                mod_t[t] = bm;
+            }
+        };
+        std::vector<uint64_t> qhi((size_t)nqj * c.np), qhis(qhi.size()), qht((size_t)nqj * nt * c.np), qmt((size_t)nqj * nt);
+        for (int b = 0; b < nqj; b++)
+            lift(Q.data() + (size_t)b * c.np, c.np, c.np, &qhi[(size_t)b * c.np], &qhis[(size_t)b * c.np],
+                 &qht[(size_t)b * nt * c.np], &qmt[(size_t)b * nt]);
+        std::vector<uint64_t> rhi((size_t)nri * g, 0), rhis(rhi.size(), 0), rht((size_t)nri * nt * g, 0), rmt((size_t)nri * nt);
+        for (int b = 0; b < nri; b++)
+            lift(PQr.data() + (size_t)b * g, std::min(g, npq - b * g), g, &rhi[(size_t)b * g], &rhis[(size_t)b * g],
+                 &rht[(size_t)b * nt * g], &rmt[(size_t)b * nt]);
+        std::vector<uint64_t> thi(nt), this_(nt), thpq((size_t)npq * nt), tpq(npq), htt(nt), htpq(npq);
+        H::Big Tb(1);
+        for (uint64_t tk : Tm) Tb.mul_word(tk);
+        const H::Big half = Tb.div_word(2);
+        for (int i = 0; i < nt; i++) {
+            uint64_t h = 1;
+            for (int k = 0; k < nt; k++) if (k != i) h = H::mulmod(h, Tm[k] % Tm[i], Tm[i]);
+            thi[i] = H::invmod(h, Tm[i]);
+            this_[i] = H::shoup(thi[i], Tm[i]);
+            htt[i] = half.mod_word(Tm[i]);
+        }
+        for (int m = 0; m < npq; m++) {
+            const uint64_t r = PQr[m];
+            for (int i = 0; i < nt; i++) {
+                uint64_t h = 1;
+                for (int k = 0; k < nt; k++) if (k != i) h = H::mulmod(h, Tm[k] % r, r);
+                thpq[(size_t)m * nt + i] = h;
+            }
+            tpq[m] = Tb.mod_word(r);
+            htpq[m] = half.mod_word(r);
+        }
+        const std::vector<uint64_t>* tabs[14] = {&qhi, &qhis, &qht, &qmt, &rhi, &rhis, &rht, &rmt,
+                                                 &thi, &this_, &thpq, &tpq, &htt, &htpq};
+        for (int i = 0; i < 14; i++) o_kl[i] = blob.add(*tabs[i]);
+        c.kc.nt = nt; c.kc.gamma = g; c.kc.nri = nri; c.kc.nqj = nqj;
+    }
     std::vector<uint64_t> cdt;
     gaussian_cdt(3.2, 19, cdt);
     dc.gauss_bound = 19;
@@ -364,6 +430,13 @@ static void build_context(Context& c, const kbfv_params& prm) {
     dc.phatinv_ps = U(o_ks[4]); dc.phat_mod_q = U(o_ks[5]); dc.dig_hatinv = U(o_ks[6]);
     dc.dig_hatinvs = U(o_ks[7]); dc.dig_hat_mod = U(o_ks[8]); dc.dig_q_mod = U(o_ks[9]);
     dc.gauss_cdt = U(o_cdt);
+    if (c.klss_ok) {
+        KlssConsts& k = c.kc;
+        k.qj_hatinv = U(o_kl[0]); k.qj_hatinvs = U(o_kl[1]); k.qj_hat_t = U(o_kl[2]); k.qj_mod_t = U(o_kl[3]);
+        k.ri_hatinv = U(o_kl[4]); k.ri_hatinvs = U(o_kl[5]); k.ri_hat_t = U(o_kl[6]); k.ri_mod_t = U(o_kl[7]);
+        k.thatinv = U(o_kl[8]); k.thatinvs = U(o_kl[9]); k.that_pq = U(o_kl[10]); k.t_pq = U(o_kl[11]);
+        k.halft_t = U(o_kl[12]); k.halft_pq = U(o_kl[13]);
+    }
     KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.ptrs_event, cudaEventDisableTiming));
 }
 
@@ -512,6 +585,7 @@ struct PtrBatch {
 
 struct MulScratch {
     uint64_t *sa, *sb, *sc, *sd, *sd2, *se;
+    uint64_t *st1, *st2;  // T-base key switch: digits [item][nqj][nt], products [item][2][nri][nt]
     size_t bytes;
 };
 
@@ -531,6 +605,10 @@ static MulScratch mul_scratch_layout(const Context& c, int count, uint8_t* base)
     m.sd = take((size_t)count * 2 * c.nq);
     m.sd2 = take((size_t)count * c.dnum * npq);
     m.se = take((size_t)count * 2 * npq);
+    if (c.klss_ok) {
+        m.st1 = take((size_t)count * c.kc.nqj * c.nt);
+        m.st2 = take((size_t)count * 2 * c.kc.nri * c.nt);
+    }
     m.bytes = off;
     return m;
 }
@@ -705,6 +783,7 @@ struct OutCtDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
 // K5: scale-and-round to R, R -> Q, and (mode 1) the key-switch lift of a1*a2.
 // mode 0: all three outputs over Q to out0 ([item][3][nq]).
 // mode 1: a1*a2 lifted into sd2 ([item][dnum][npq]); cross, b1*b2 to sd ([item][2][nq]).
+// mode 2: a1*a2 over Q into sd2 ([item][nq]); cross, b1*b2 to sd (T-base key switch).
 template <int MAXQ>
 __global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__ sc, uint64_t* __restrict__ out0,
                                 uint64_t* __restrict__ sd, uint64_t* __restrict__ sd2, int mode) {
@@ -731,6 +810,11 @@ __global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__ sc, ui
     }
     if (mode == 0) {
         uint64_t* dst = out0 + ((size_t)poly * c.nq << c.logn);
+#pragma unroll
+        for (int i = 0; i < MAXQ; i++)
+            if (i < c.nq) dst[((size_t)i << c.logn) + k] = xq[i];
+    } else if (which == 0 && mode == 2) {  // a1*a2 over Q, coefficient form, to sd2 ([item][nq])
+        uint64_t* dst = sd2 + ((size_t)item * c.nq << c.logn);
 #pragma unroll
         for (int i = 0; i < MAXQ; i++)
             if (i < c.nq) dst[((size_t)i << c.logn) + k] = xq[i];
@@ -800,6 +884,42 @@ struct TensorA2 {
 // by the block kernel, which every functor here supports.
 static void require_batchable(const Context& c) {
     KB_REQUIRE(c.logn >= 10 && c.logn <= 16, KBFV_ERR_UNSUPPORTED, "ring degree outside 2^10..2^16");
+}
+
+// T-base key switch (the reference's KLSS, include/KeySwitch_23.cuh:244-330) of
+// a1*a2 given in coefficient form over Q (sd2, [item][nq]); writes the P|Q
+// results into se ([item][2][npq]).
+static void klss_keyswitch(Context& c, const uint64_t* rlk_t, int count, const MulScratch& m, cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    const KlssConsts& kc = c.kc;
+    // Qj blocks -> T (modUpQjtoT_23)
+    klss_block_to_t_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)kc.nqj, (unsigned)count), 128, 0, st>>>(
+        dc, kc, m.sd2, m.st1, 0, (size_t)c.nq << c.logn, (size_t)kc.nqj * c.nt << c.logn);
+    check_launch("klss_qj_to_t");
+    // NTT over T ([0, 8q): the external product reduces its sums)
+    ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.st1, dc.idx_t, c.nt), rows_io(dc, m.st1, dc.idx_t, c.nt),
+                                   count * kc.nqj * c.nt, st);
+    // external product over T fused into INTT over T (external_product_T)
+    ntt_inv(dc, ExtProdSrc{m.st1, rlk_t, dc, c.nt, kc.nri, kc.nqj, kc.nqj}, rows_io(dc, m.st2, dc.idx_t, c.nt),
+            count * 2 * kc.nri * c.nt, st);
+    // centred T -> P|Q (modUpTtoPQl_23)
+    klss_t_to_pq_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)kc.nri, (unsigned)(count * 2)), 128, 0, st>>>(
+        dc, kc, m.st2, m.se);
+    check_launch("klss_t_to_pq");
+}
+
+static void mul_relin_klss_chunk(Context& c, const uint64_t* rlk_t, const PtrBatch& pb, int count,
+                                 const MulScratch& m, cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    mul_front(c, pb, count, m, st);
+    k5_launch(c, count, m, nullptr, 2, st);
+    klss_keyswitch(c, rlk_t, count, m, st);
+    ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
+}
+
+static void require_klss(const Context& c) {
+    KB_REQUIRE(c.klss_ok, KBFV_ERR_INVALID,
+               "context has no T-base key switch (needs T primes, q_count divisible by p_count, dnum = q_count / p_count)");
 }
 
 // ===========================================================================
@@ -1404,6 +1524,157 @@ int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_c
         }
         int rc = kbfv_mul_relin_batch(ctx, d_rlk, A.data(), B.data(), O.data(), count, stream);
         if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+    });
+}
+
+
+// ---- T-base key switch (the reference's KLSS) ------------------------------
+int kbfv_context_klss(const kbfv_context* ctx, uint32_t* ri_blocks, uint32_t* qj_blocks, uint64_t* key_words) {
+    return guarded([&] {
+        const Context& c = CX(const_cast<kbfv_context*>(ctx));
+        require_klss(c);
+        if (ri_blocks) *ri_blocks = (uint32_t)c.kc.nri;
+        if (qj_blocks) *qj_blocks = (uint32_t)c.kc.nqj;
+        if (key_words) *key_words = (uint64_t)2 * c.kc.nqj * c.kc.nri * c.nt * c.n;
+    });
+}
+
+int kbfv_rlk_to_klss(kbfv_context* ctx, const uint64_t* d_rlk, uint64_t* d_rlk_t, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(d_rlk && d_rlk_t, KBFV_ERR_INVALID, "null key pointer");
+        cudaStream_t st = S(stream);
+        const DevConsts& dc = c.dc;
+        const KlssConsts& kc = c.kc;
+        const int npq = dc.npq;
+        uint64_t* coef = (uint64_t*)ensure_scratch(c, (size_t)c.dnum * 2 * npq * c.n * 8);
+        // key [digit][a|b][Q|P] in NTT form -> coefficient form
+        ntt_inv(dc, rows_io(dc, const_cast<uint64_t*>(d_rlk), 0, npq), rows_io(dc, coef, 0, npq),
+                c.dnum * 2 * npq, st);
+        // Ri blocks -> T (modUpPQtoT_23), written as [a|b][digit][Ri][T]
+        for (int h = 0; h < 2; h++) {
+            klss_block_to_t_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)kc.nri, (unsigned)c.dnum), 128, 0, st>>>(
+                dc, kc, coef + ((size_t)h * npq << c.logn), d_rlk_t + ((size_t)h * c.dnum * kc.nri * c.nt << c.logn), 1,
+                (size_t)2 * npq << c.logn, (size_t)kc.nri * c.nt << c.logn);
+            check_launch("klss_pq_to_t");
+        }
+        RowsIO io = rows_io(dc, d_rlk_t, dc.idx_t, c.nt);
+        ntt_fwd(dc, io, io, 2 * c.dnum * kc.nri * c.nt, st);
+    });
+}
+
+int kbfv_klss_modup_qj_to_t(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                            kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(polys <= 65535, KBFV_ERR_INVALID, "at most 65535 polynomials per call");
+        if (!polys) return;
+        klss_block_to_t_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)c.kc.nqj, polys), 128, 0, S(stream)>>>(
+            c.dc, c.kc, d_in, d_out, 0, (size_t)c.nq << c.logn, (size_t)c.kc.nqj * c.nt << c.logn);
+        check_launch("klss_qj_to_t");
+    });
+}
+
+int kbfv_klss_modup_pq_to_t(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys,
+                            kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(polys <= 65535, KBFV_ERR_INVALID, "at most 65535 polynomials per call");
+        if (!polys) return;
+        klss_block_to_t_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)c.kc.nri, polys), 128, 0, S(stream)>>>(
+            c.dc, c.kc, d_in, d_out, 1, (size_t)c.dc.npq << c.logn, (size_t)c.kc.nri * c.nt << c.logn);
+        check_launch("klss_pq_to_t");
+    });
+}
+
+int kbfv_klss_external_product(kbfv_context* ctx, const uint64_t* d_digits, const uint64_t* d_rlk_t,
+                               uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(d_rlk_t, KBFV_ERR_NO_KEY, "T-base relinearisation key missing");
+        const KlssConsts& kc = c.kc;
+        ntt_inv(c.dc, ExtProdSrc{d_digits, d_rlk_t, c.dc, c.nt, kc.nri, kc.nqj, kc.nqj},
+                rows_io(c.dc, d_out, c.dc.idx_t, c.nt), (int)count * 2 * kc.nri * c.nt, S(stream));
+    });
+}
+
+int kbfv_klss_t_to_pq(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint32_t polys, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(polys <= 65535, KBFV_ERR_INVALID, "at most 65535 polynomials per call");
+        if (!polys) return;
+        klss_t_to_pq_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)c.kc.nri, polys), 128, 0, S(stream)>>>(
+            c.dc, c.kc, d_in, d_out);
+        check_launch("klss_t_to_pq");
+    });
+}
+
+int kbfv_relinearize_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64_t* d_tensor, uint64_t* d_ct,
+                          uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(d_rlk_t, KBFV_ERR_NO_KEY, "T-base relinearisation key missing");
+        cudaStream_t st = S(stream);
+        const DevConsts& dc = c.dc;
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            const uint64_t* tz = d_tensor + (size_t)off * 3 * lq;
+            uint64_t* out = d_ct + (size_t)off * 2 * lq;
+            ntt_inv(dc, TensorA2{tz, dc.logn, dc.nq}, rows_io(dc, m.sd2, 0, dc.nq), cnt * dc.nq, st);
+            klss_keyswitch(c, d_rlk_t, cnt, m, st);
+            std::vector<uint64_t*> O(cnt);
+            std::vector<const uint64_t*> Z(cnt);
+            for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
+            PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
+            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            for (int i = 0; i < cnt; i++) {
+                const size_t tot = 2 * lq;
+                add_kernel<<<blocks_for(tot, 256), 256, 0, st>>>(dc, out + (size_t)i * 2 * lq, tz + (size_t)i * 3 * lq + lq,
+                                                                 out + (size_t)i * 2 * lq, tot, dc.nq);
+            }
+            check_launch("relin_add");
+        }
+    });
+}
+
+int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                        uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        require_klss(c);
+        KB_REQUIRE(d_rlk_t, KBFV_ERR_NO_KEY, "T-base relinearisation key missing");
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            std::vector<const uint64_t*> A(cnt), B(cnt);
+            std::vector<uint64_t*> O(cnt);
+            for (int i = 0; i < cnt; i++) {
+                A[i] = d_ct_a + (size_t)(off + i) * 2 * lq;
+                B[i] = d_ct_b + (size_t)(off + i) * 2 * lq;
+                O[i] = d_out + (size_t)(off + i) * 2 * lq;
+            }
+            PtrBatch pb = make_batch(A.data(), B.data(), O.data(), cnt);
+            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            mul_relin_klss_chunk(c, d_rlk_t, pb, cnt, m, st);
+        }
     });
 }
 
