@@ -63,6 +63,15 @@ typedef struct {
     uint32_t gamma;           /* KLSS Ri block size */
 } kbfv_params;
 
+/* Parameter set from per-prime bit sizes (SEAL-style coeff_modulus sizes):
+ * p_count special primes of p_bits[i] bits, then q_count ciphertext primes of
+ * q_bits[i] bits, all distinct, 1 mod 2N, largest first within each size.
+ * Replaces the hard-coded prime lists of include/Params.cuh:7-149. Free with
+ * kbfv_params_destroy. */
+int kbfv_params_create(uint32_t log_n, const uint32_t* q_bits, uint32_t q_count, const uint32_t* p_bits,
+                       uint32_t p_count, uint64_t plain_modulus, uint32_t dnum, kbfv_params** out);
+int kbfv_params_destroy(kbfv_params* params);
+
 const char* kbfv_last_error(void);
 const char* kbfv_version(void);
 
@@ -87,6 +96,10 @@ size_t kbfv_mul_relin_scratch_bytes(const kbfv_context* ctx, uint32_t count);
 /* pre-size the context's scratch arena (no allocation happens later for <= count pairs) */
 int kbfv_reserve(kbfv_context* ctx, uint32_t pairs);
 
+/* seed for keygen / encryption calls that pass seed = NULL (the reference
+ * seeds its RNG once per scheme, include/RNG.cuh:18-51) */
+int kbfv_set_seed(kbfv_context* ctx, const uint8_t seed[32]);
+
 /* ---- NTT over the context's prime table --------------------------------
  * ToNTTInplace / FromNTTInplace (include/BFVcontext.cuh:1513-1552) and the
  * _for_QR / _for_BFV / _for_externalProduct variants (1554-1757): rows are
@@ -96,6 +109,12 @@ int kbfv_ntt_fwd(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t pr
                  kbfv_stream stream);
 int kbfv_ntt_inv(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t prime0, uint32_t period,
                  kbfv_stream stream);
+/* the same over `count` polynomials at arbitrary addresses (HOST array of
+ * device pointers), each `limbs` rows using primes prime0 .. prime0+limbs-1 */
+int kbfv_ntt_fwd_batch(kbfv_context* ctx, uint64_t* const* d_polys, uint32_t count, uint32_t limbs,
+                       uint32_t prime0, kbfv_stream stream);
+int kbfv_ntt_inv_batch(kbfv_context* ctx, uint64_t* const* d_polys, uint32_t count, uint32_t limbs,
+                       uint32_t prime0, kbfv_stream stream);
 
 /* ---- HPS building blocks (per polynomial, coefficient form) ------------
  * BaseConverter::bConv_HPS (include/BasisConv_QR.cuh:191-207): centred base
@@ -131,7 +150,8 @@ int kbfv_moddown(kbfv_context* ctx, const uint64_t* d_in, uint64_t* d_out, uint3
  * SecretKey::SecretKey (include/SecretKey.cuh:20-37), BFVScheme::addEncKey
  * (include/BFVScheme.cuh:57-85), BFVScheme::addMultKey_23
  * (include/KeySwitch_23.cuh:21-66). All randomness comes from XSalsa20 keyed
- * by `seed` (32 bytes); the same seed reproduces the same keys.
+ * by `seed` (32 bytes; NULL = the context seed, kbfv_set_seed); the same seed
+ * reproduces the same keys. kbfv_encrypt takes seeds the same way.
  * secret_kind: 0 = ternary uniform, 1 = Hamming weight h (the reference's HWT). */
 int kbfv_keygen_secret(kbfv_context* ctx, const uint8_t seed[32], int secret_kind, uint32_t h,
                        uint64_t* d_sk, kbfv_stream stream);
@@ -162,6 +182,10 @@ int kbfv_decrypt(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, 
 /* BFVScheme::add / addAndEqual (include/BFVScheme.cuh:169-190); polys per item = 2 */
 int kbfv_add(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64_t* d_out,
              uint32_t count, kbfv_stream stream);
+/* BFVScheme::addConstAndEqual(Ciphertext&, Plaintext&) (include/BFVScheme.cuh:192-217):
+ * b += NTT(Delta * m) for plaintexts m of N coefficients mod t */
+int kbfv_add_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_m, uint64_t* d_out,
+                   uint32_t count, kbfv_stream stream);
 /* BFVScheme::multConstAndEqual (include/BFVScheme.cuh:226-245) with an encode_ntt plaintext */
 int kbfv_mul_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_pt_ntt, uint64_t* d_out,
                    uint32_t count, kbfv_stream stream);

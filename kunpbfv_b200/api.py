@@ -123,6 +123,13 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_context_klss": (I, [VP, C.POINTER(u32), C.POINTER(u32), U64P]),
+        "kbfv_params_create": (I, [u32, C.POINTER(u32), u32, C.POINTER(u32), u32, u64, u32,
+                                   C.POINTER(C.POINTER(_Params))]),
+        "kbfv_params_destroy": (I, [C.POINTER(_Params)]),
+        "kbfv_set_seed": (I, [VP, U8P]),
+        "kbfv_ntt_fwd_batch": (I, [VP, C.POINTER(VP), u32, u32, u32, VP]),
+        "kbfv_ntt_inv_batch": (I, [VP, C.POINTER(VP), u32, u32, u32, VP]),
+        "kbfv_add_plain": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_rlk_to_klss": (I, [VP, VP, VP, VP]),
         "kbfv_klss_modup_qj_to_t": (I, [VP, VP, VP, u32, VP]),
         "kbfv_klss_modup_pq_to_t": (I, [VP, VP, VP, u32, VP]),
@@ -293,6 +300,33 @@ class BFVContext:
     def zeros(self, *shape):
         torch = _torch()
         return torch.zeros(shape, dtype=torch.int64, device="cuda")
+
+    @classmethod
+    def from_bits(cls, log_n: int, q_bits, p_bits, plain_modulus: int, dnum: int = 1) -> "BFVContext":
+        """Parameter set from per-prime bit sizes (kbfv_params_create), e.g.
+        from_bits(12, [36, 36], [37], 65537, dnum=2)."""
+        qb = (C.c_uint32 * len(q_bits))(*q_bits)
+        pb = (C.c_uint32 * len(p_bits))(*p_bits)
+        out = C.POINTER(_Params)()
+        _check(lib().kbfv_params_create(log_n, qb, len(q_bits), pb, len(p_bits), plain_modulus, dnum, C.byref(out)))
+        try:
+            h = VP()
+            _check(lib().kbfv_context_create(out, C.byref(h)))
+        finally:
+            lib().kbfv_params_destroy(out)
+        return cls(_handle=h)
+
+    def set_seed(self, seed: bytes):
+        _check(lib().kbfv_set_seed(self._h, _u8(seed)))
+
+    def ntt_fwd_batch(self, polys, limbs: int, prime0: int = 0, stream=None):
+        """forward NTT of polynomials at arbitrary addresses (a list of device tensors)"""
+        arr = (VP * len(polys))(*[_ptr(p) for p in polys])
+        _check(lib().kbfv_ntt_fwd_batch(self._h, arr, len(polys), limbs, prime0, _stream_ptr(stream)))
+
+    def ntt_inv_batch(self, polys, limbs: int, prime0: int = 0, stream=None):
+        arr = (VP * len(polys))(*[_ptr(p) for p in polys])
+        _check(lib().kbfv_ntt_inv_batch(self._h, arr, len(polys), limbs, prime0, _stream_ptr(stream)))
 
     # ---- NTT (ToNTTInplace / FromNTTInplace)
     def ntt_fwd(self, rows, prime0: int, period: int, stream=None):
@@ -523,6 +557,11 @@ class BFVScheme:
     def addAndEqual(self, c1: Ciphertext, c2: Ciphertext, stream=None):
         _check(lib().kbfv_add(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device),
                               _ptr(c1.cipher_device), c1.count, _stream_ptr(stream)))
+
+    def addConstAndEqual(self, ct: Ciphertext, pt: Plaintext, stream=None):
+        """ct.b += NTT(Delta * m) (BFVScheme.cuh:192-217)"""
+        _check(lib().kbfv_add_plain(self.context.handle, _ptr(ct.cipher_device), _ptr(pt.mx_device),
+                                    _ptr(ct.cipher_device), ct.count, _stream_ptr(stream)))
 
     def multConstAndEqual(self, ct: Ciphertext, pt_ntt, stream=None):
         _check(lib().kbfv_mul_plain(self.context.handle, _ptr(ct.cipher_device), _ptr(pt_ntt),

@@ -100,6 +100,8 @@ struct Context {
     // line up with the hybrid digits (alpha == p_count, dnum == q_count / p_count)
     bool klss_ok = false;
     KlssConsts kc{};
+    // seed used by keygen / encryption calls that pass no seed (kbfv_set_seed)
+    uint8_t seed[32] = {0};
 };
 
 }  // namespace kbfv

@@ -917,6 +917,16 @@ static void mul_relin_klss_chunk(Context& c, const uint64_t* rlk_t, const PtrBat
     ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
 }
 
+// rows of polynomials at arbitrary addresses: row (item, limb) -> pb.o[item] + limb*N
+struct PtrPolysIO {
+    PtrBatch pb;
+    int logn, limbs, p0;
+    __device__ __forceinline__ int prime(int row) const { return p0 + row % limbs; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        return PtrRow{pb.o[row / limbs] + ((size_t)(row % limbs) << logn)};
+    }
+};
+
 static void require_klss(const Context& c) {
     KB_REQUIRE(c.klss_ok, KBFV_ERR_INVALID,
                "context has no T-base key switch (needs T primes, q_count divisible by p_count, dnum = q_count / p_count)");
@@ -1214,7 +1224,8 @@ int kbfv_keygen_secret(kbfv_context* ctx, const uint8_t seed[32], int secret_kin
                        kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
-        KB_REQUIRE(seed && d_sk, KBFV_ERR_INVALID, "null argument");
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(d_sk, KBFV_ERR_INVALID, "null argument");
         const int npq = c.nq + c.np;
         cudaStream_t st = S(stream);
         if (secret_kind == 1) {
@@ -1234,7 +1245,8 @@ int kbfv_keygen_public(kbfv_context* ctx, const uint8_t seed[32], const uint64_t
                        kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
-        KB_REQUIRE(seed && d_sk && d_pk, KBFV_ERR_INVALID, "null argument");
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(d_sk && d_pk, KBFV_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
         const size_t lq = (size_t)c.nq * c.n;
         uint64_t* a = d_pk;
@@ -1252,7 +1264,8 @@ int kbfv_keygen_relin(kbfv_context* ctx, const uint8_t seed[32], const uint64_t*
                       kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
-        KB_REQUIRE(seed && d_sk && d_rlk, KBFV_ERR_INVALID, "null argument");
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(d_sk && d_rlk, KBFV_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
         const int npq = c.nq + c.np;
         const size_t lpq = (size_t)npq * c.n;
@@ -1319,7 +1332,8 @@ int kbfv_encrypt(kbfv_context* ctx, const uint8_t seed[32], uint64_t enc_id, con
                  uint64_t* d_ct, uint32_t count, kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
-        KB_REQUIRE(seed && d_pk && d_m && d_ct, KBFV_ERR_INVALID, "null argument");
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(d_pk && d_m && d_ct, KBFV_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
         const size_t lq = (size_t)c.nq * c.n;
         for (uint32_t off = 0; off < count; off += kMaxBatch) {
@@ -1674,6 +1688,122 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
             uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
             MulScratch m = mul_scratch_layout(c, cnt, base);
             mul_relin_klss_chunk(c, d_rlk_t, pb, cnt, m, st);
+        }
+    });
+}
+
+
+// ---- parameter sets, seeds, batched NTT over pointer arrays, plaintext add -----
+struct kbfv_params_owned {
+    kbfv_params p;
+    std::vector<uint64_t> q, pp;
+};
+
+int kbfv_params_create(uint32_t log_n, const uint32_t* q_bits, uint32_t q_count, const uint32_t* p_bits,
+                       uint32_t p_count, uint64_t plain_modulus, uint32_t dnum, kbfv_params** out) {
+    return guarded([&] {
+        KB_REQUIRE(out && q_bits && p_bits, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE(log_n >= 10 && log_n <= 16, KBFV_ERR_INVALID, "log_n out of range");
+        KB_REQUIRE(q_count >= 1 && q_count <= (uint32_t)kMaxQ && p_count >= 1 && p_count <= (uint32_t)kMaxP,
+                   KBFV_ERR_INVALID, "prime counts out of range");
+        auto* o = new kbfv_params_owned();
+        const uint64_t n = (uint64_t)1 << log_n;
+        std::vector<uint64_t> used;
+        auto pick = [&](uint32_t bits, std::vector<uint64_t>& dst) {
+            if (bits < 20 || bits > 60) {
+                delete o;
+                throw KbfvError(KBFV_ERR_INVALID, "prime sizes must be 20..60 bits");
+            }
+            auto v = H::primes_bits(n, (int)bits, 1, used);
+            if (v.empty()) {
+                delete o;
+                throw KbfvError(KBFV_ERR_PARAMS, "not enough NTT-friendly primes of the requested size");
+            }
+            dst.push_back(v[0]);
+            used.push_back(v[0]);
+        };
+        for (uint32_t i = 0; i < p_count; i++) pick(p_bits[i], o->pp);
+        for (uint32_t i = 0; i < q_count; i++) pick(q_bits[i], o->q);
+        std::memset(&o->p, 0, sizeof o->p);
+        o->p.log_n = log_n;
+        o->p.plain_modulus = plain_modulus;
+        o->p.q_count = q_count;
+        o->p.q = o->q.data();
+        o->p.p_count = p_count;
+        o->p.p = o->pp.data();
+        o->p.dnum = dnum ? dnum : 1;
+        *out = &o->p;
+    });
+}
+
+int kbfv_params_destroy(kbfv_params* params) {
+    if (params) delete reinterpret_cast<kbfv_params_owned*>(params);  // p is the first member
+    return KBFV_OK;
+}
+
+int kbfv_set_seed(kbfv_context* ctx, const uint8_t seed[32]) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(seed, KBFV_ERR_INVALID, "null seed");
+        std::memcpy(c.seed, seed, 32);
+    });
+}
+
+static int ntt_batch(kbfv_context* ctx, uint64_t* const* d_polys, uint32_t count, uint32_t limbs, uint32_t prime0,
+                     kbfv_stream stream, bool fwd) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_polys || !count, KBFV_ERR_INVALID, "null pointer array");
+        KB_REQUIRE(limbs >= 1 && prime0 + limbs <= c.mods.size(), KBFV_ERR_INVALID, "prime range out of table");
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            PtrBatch pb{};
+            for (int i = 0; i < cnt; i++) {
+                KB_REQUIRE(d_polys[off + i], KBFV_ERR_INVALID, "null polynomial pointer");
+                pb.o[i] = d_polys[off + i];
+            }
+            PtrPolysIO io{pb, c.logn, (int)limbs, (int)prime0};
+            if (fwd) ntt_fwd(c.dc, io, io, cnt * (int)limbs, S(stream));
+            else ntt_inv(c.dc, io, io, cnt * (int)limbs, S(stream));
+        }
+    });
+}
+
+int kbfv_ntt_fwd_batch(kbfv_context* ctx, uint64_t* const* d_polys, uint32_t count, uint32_t limbs, uint32_t prime0,
+                       kbfv_stream stream) {
+    return ntt_batch(ctx, d_polys, count, limbs, prime0, stream, true);
+}
+
+int kbfv_ntt_inv_batch(kbfv_context* ctx, uint64_t* const* d_polys, uint32_t count, uint32_t limbs, uint32_t prime0,
+                       kbfv_stream stream) {
+    return ntt_batch(ctx, d_polys, count, limbs, prime0, stream, false);
+}
+
+int kbfv_add_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_m, uint64_t* d_out, uint32_t count,
+                   kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_ct && d_m && d_out, KBFV_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            uint64_t* dm = (uint64_t*)ensure_scratch(c, (size_t)cnt * lq * 8);
+            delta_m_kernel<<<blocks_for((size_t)cnt * lq, 256), 256, 0, st>>>(c.dc, d_m + (size_t)off * c.n, dm,
+                                                                             (size_t)cnt * lq);
+            check_launch("delta_m");
+            RowsIO io = rows_io(c.dc, dm, 0, c.nq);
+            ntt_fwd(c.dc, io, io, cnt * c.nq, st);
+            for (int i = 0; i < cnt; i++) {
+                const uint64_t* src = d_ct + (size_t)(off + i) * 2 * lq;
+                uint64_t* dst = d_out + (size_t)(off + i) * 2 * lq;
+                if (dst != src) KB_CHECK_CUDA(cudaMemcpyAsync(dst, src, lq * 8, cudaMemcpyDeviceToDevice, st));
+                add_kernel<<<blocks_for(lq, 256), 256, 0, st>>>(c.dc, src + lq, dm + (size_t)i * lq, dst + lq, lq,
+                                                                c.nq);
+            }
+            check_launch("add_plain");
         }
     });
 }

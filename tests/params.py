@@ -27,3 +27,12 @@ def small_primes(log_n: int = 12, nq: int = 3, np_: int = 1, bits: int = 50):
 def plain_modulus_for(log_n: int) -> int:
     """65537 while 2N divides 65536, else 786433 (= 3 * 2^18 + 1)."""
     return 65537 if (2 << log_n) <= 65536 else 786433
+
+
+@functools.lru_cache(maxsize=None)
+def c1_primes():
+    """N=4096: ciphertext primes of 36 and 36 bits, special prime of 37 bits
+    (SEAL's default coeff_modulus sizes for N=4096), all 1 mod 8192."""
+    p = oracle.primes_bits(4096, 37, 1)
+    q = oracle.primes_bits(4096, 36, 2, skip=p)
+    return q, p

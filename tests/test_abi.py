@@ -24,9 +24,13 @@ def declared_symbols():
 
 def test_header_declares_entry_points():
     names = declared_symbols()
-    for must in ("kbfv_context_create", "kbfv_ntt_fwd", "kbfv_mul_relin_batch", "kbfv_encrypt", "kbfv_decrypt",
-                 "kbfv_relinearize", "kbfv_keygen_relin", "kbfv_noise_budget"):
-        assert must in names
+    # the entry points a kunpBFV caller binds (context, keys, encoder, scheme ops, NTT, seed)
+    for must in ("kbfv_params_create", "kbfv_context_create", "kbfv_context_destroy", "kbfv_keygen_secret",
+                 "kbfv_keygen_public", "kbfv_keygen_relin", "kbfv_encode", "kbfv_decode", "kbfv_encrypt",
+                 "kbfv_decrypt", "kbfv_add", "kbfv_add_plain", "kbfv_mul_plain", "kbfv_mul", "kbfv_relinearize",
+                 "kbfv_mul_relin_batch", "kbfv_ntt_fwd", "kbfv_ntt_inv", "kbfv_ntt_fwd_batch", "kbfv_ntt_inv_batch",
+                 "kbfv_noise_budget", "kbfv_set_seed"):
+        assert must in names, must
 
 
 def test_library_exports_all_declared_symbols():
@@ -40,3 +44,29 @@ def test_library_exports_all_declared_symbols():
 def test_library_reports_version_without_gpu():
     import kunpbfv_b200 as kb
     assert b"sm_100a" in kb.lib().kbfv_version()
+
+
+def test_params_create_without_gpu(oracle_mod):
+    """Per-prime bit sizes (36, 36 | 37 at N=4096) give distinct NTT-friendly
+    primes equal to the oracle's generator; no device is touched."""
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200.api import _Params
+    L = kb.lib()
+    qb = (ctypes.c_uint32 * 2)(36, 36)
+    pb = (ctypes.c_uint32 * 1)(37)
+    out = ctypes.POINTER(_Params)()
+    assert L.kbfv_params_create(12, qb, 2, pb, 1, 65537, 2, ctypes.byref(out)) == 0
+    prm = out.contents
+    q = [prm.q[i] for i in range(prm.q_count)]
+    p = [prm.p[i] for i in range(prm.p_count)]
+    assert prm.log_n == 12 and prm.plain_modulus == 65537 and prm.dnum == 2
+    assert [x.bit_length() for x in q] == [36, 36] and [x.bit_length() for x in p] == [37]
+    assert len(set(q + p)) == 3 and all(x % 8192 == 1 for x in q + p)
+    want_p = oracle_mod.primes_bits(4096, 37, 1)
+    want_q = oracle_mod.primes_bits(4096, 36, 2, skip=want_p)
+    assert p == want_p and q == want_q
+    assert L.kbfv_params_destroy(out) == 0
+    # out-of-range sizes are rejected with a status, not a crash
+    bad = (ctypes.c_uint32 * 1)(61)
+    out2 = ctypes.POINTER(_Params)()
+    assert L.kbfv_params_create(12, bad, 1, pb, 1, 65537, 1, ctypes.byref(out2)) == -1

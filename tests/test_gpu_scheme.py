@@ -141,3 +141,71 @@ def test_errors_are_reported():
         sch.mult_relin(c, c)   # no relinearisation key
     with pytest.raises(ValueError):
         kb.BFVContext(log_n=12, plain_modulus=65537, q_count=0)
+
+
+def test_c1_end_to_end():
+    """N=4096 with 36+36-bit ciphertext primes and a 37-bit special prime,
+    t=65537, ternary secret, Gaussian error, dnum=2; batch size 1. The context
+    is built from bit sizes (kbfv_params_create) and must pick the oracle's
+    primes; keys, encryptions and the product are bit-exact, decryption exact."""
+    import kunpbfv_b200 as kb
+    import oracle
+    from tests.params import c1_primes
+    qs, ps = c1_primes()
+    ctx = kb.BFVContext.from_bits(12, [36, 36], [37], T, dnum=2)
+    assert ctx.q == qs and ctx.p == ps
+    orc = oracle.Oracle(12, T, qs, ps, dnum=2)
+    sk, sch, osk = setup(ctx, orc)
+    opk, orlk = orc.keygen_public(SEED, osk), orc.keygen_relin(SEED, osk)
+    assert np.array_equal(host(sch.rlk).reshape(orlk.shape), orlk)
+    rng = np.random.default_rng(41)
+    v1 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+    v2 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=0)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=1)
+    h1 = host(c1.cipher_device).reshape(2, 2, ctx.N)
+    assert np.array_equal(h1, orc.encrypt(SEED, 0, opk, orc.encode(v1)))
+    h2 = host(c2.cipher_device).reshape(2, 2, ctx.N)
+    out = sch.mult_relin(c1, c2)
+    assert np.array_equal(host(out.cipher_device).reshape(2, 2, ctx.N), orc.mul_relin(h1, h2, orlk))
+    dec = host(ctx.decode(sch.decryptMsg(sk, out).mx_device)).reshape(-1)
+    assert np.array_equal(dec, (v1 * v2) % T)
+    assert sch.noise_budget(sk, out) > 10
+
+
+def test_add_plain_bit_exact():
+    """addConstAndEqual: b += NTT(Delta * m)."""
+    import kunpbfv_b200 as kb
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    rng = np.random.default_rng(6)
+    v1 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+    c = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=500)
+    before = host(c.cipher_device).reshape(2, 2, ctx.q_count, ctx.N)
+    m2 = ctx.encode(dev(v2))
+    sch.addConstAndEqual(c, kb.Plaintext(ctx, m2))
+    after = host(c.cipher_device).reshape(2, 2, ctx.q_count, ctx.N)
+    hm = host(m2).reshape(2, ctx.N)
+    for i in range(2):
+        dm = orc.delta_m(hm[i])
+        add = np.stack([orc.ntt_fwd(l, dm[l]) for l in range(ctx.q_count)])
+        want = orc.add(before[i], np.stack([np.zeros_like(add), add]))
+        assert np.array_equal(after[i], want)
+    dec = host(ctx.decode(sch.decryptMsg(sk, c).mx_device)).reshape(2, ctx.N)
+    assert np.array_equal(dec, (v1 + v2) % T)
+
+
+def test_ntt_batch_pointer_arrays():
+    """kbfv_ntt_fwd_batch / inv_batch over polynomials at separate addresses."""
+    from tests.gpu_util import rand_rows
+    ctx, orc = c3_pair()
+    polys = [rand_rows(orc, range(ctx.q_count), ctx.N, 60 + i) for i in range(3)]
+    d = [dev(p) for p in polys]
+    ctx.ntt_fwd_batch(d, ctx.q_count, 0)
+    for p, x in zip(polys, d):
+        want = np.stack([orc.ntt_fwd(l, p[l]) for l in range(ctx.q_count)])
+        assert np.array_equal(host(x).reshape(want.shape), want)
+    ctx.ntt_inv_batch(d, ctx.q_count, 0)
+    for p, x in zip(polys, d):
+        assert np.array_equal(host(x).reshape(p.shape), p)

@@ -234,6 +234,28 @@ def test_scheme_c3_params(oracle_mod):
     assert o.noise_budget(sk, c3) > 10
 
 
+def test_scheme_c1_params(oracle_mod):
+    """N=4096, q = 36+36 bits, special prime 37 bits, t=65537, ternary secret,
+    Gaussian error sigma 3.2, one digit per ciphertext prime (dnum=2): batch-encode
+    two vectors of 4096 values mod t, encrypt, multiply, relinearise, decrypt."""
+    from tests.params import c1_primes
+    O = oracle_mod
+    qs, ps = c1_primes()
+    o = O.Oracle(12, T65537, qs, ps, dnum=2)
+    key = b"\x01" * 32
+    sk = o.keygen_secret(key)
+    pk = o.keygen_public(key, sk)
+    rlk = o.keygen_relin(key, sk)
+    rng = np.random.default_rng(41)
+    v1 = rng.integers(0, T65537, size=o.n, dtype=np.uint64)
+    v2 = rng.integers(0, T65537, size=o.n, dtype=np.uint64)
+    c1 = o.encrypt(key, 0, pk, o.encode(v1))
+    c2 = o.encrypt(key, 1, pk, o.encode(v2))
+    c3 = o.mul_relin(c1, c2, rlk)
+    assert np.array_equal(o.decode(o.decrypt(sk, c3)), (v1 * v2) % T65537)
+    assert o.noise_budget(sk, c3) > 0
+
+
 def test_hybrid_dnum(oracle_mod):
     O = oracle_mod
     qs, ps = small_primes(12, 4, 2, 45)
