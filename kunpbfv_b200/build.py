@@ -1,6 +1,9 @@
-"""Build libkbfv.so (sm_100a) in-tree with nvcc."""
+"""Build libkbfv.so (sm_100a) in-tree with nvcc: each translation unit is
+compiled to an object under _build/ (in parallel, only when it or a header
+changed), then linked into the shared library."""
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -8,14 +11,17 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libkbfv.so")
-SOURCES = [os.path.join(HERE, "csrc", "kbfv.cu")]
-DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
-    os.path.join(ROOT, "include", "kbfv.h")]
+OBJDIR = os.path.join(HERE, "_build")
+SOURCES = [os.path.join(HERE, "csrc", "kbfv.cu"), os.path.join(HERE, "csrc", "serve.cpp")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))
+           if f.endswith((".cuh", ".hpp", ".h"))] + [
+    os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
+DEPS = SOURCES + HEADERS
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
     "-Xptxas", "-warn-spills",
 ]
@@ -35,14 +41,38 @@ def stale() -> bool:
     return any(os.path.getmtime(d) > t for d in DEPS if os.path.exists(d))
 
 
+def _obj(src: str) -> str:
+    return os.path.join(OBJDIR, os.path.basename(src) + ".o")
+
+
+def _stale_obj(src: str) -> bool:
+    o = _obj(src)
+    if not os.path.exists(o):
+        return True
+    t = os.path.getmtime(o)
+    return any(os.path.getmtime(d) > t for d in [src] + HEADERS if os.path.exists(d))
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp", *SOURCES]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    todo = [s for s in SOURCES if force or _stale_obj(s)]
+
+    def compile_one(src):
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", _obj(src) + ".tmp", src]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(_obj(src) + ".tmp", _obj(src))
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        for f in [ex.submit(compile_one, s) for s in todo]:
+            f.result()
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp",
+            *[_obj(s) for s in SOURCES], "-lpthread"]
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 
