@@ -49,6 +49,10 @@ def parse():
                     help="run one kernel on a profiling-sized case and exit (for ncu)")
     ap.add_argument("--rows", type=int, default=1024, help="rows for the ntt16k profiling cases")
     ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
+    ap.add_argument("--serve-rates", default="250,500,1000,2000",
+                    help="Poisson arrival rates (requests/s) of the serving sweep")
+    ap.add_argument("--serve-seconds", type=float, default=2.5, help="arrival window per rate")
+    ap.add_argument("--serving-only", action="store_true", help="run only the serving sweep and print it")
     return ap.parse_args()
 
 
@@ -368,6 +372,12 @@ def run_ours(args, world, rank, local):
         except Exception as e:  # report, keep the headline line
             line["extras_error"] = repr(e)
         try:
+            sv = serving(args)
+            line["serving"] = sv
+            line["p50_ms"], line["p99_ms"] = sv["p50_ms"], sv["p99_ms"]
+        except Exception as e:
+            line["serving_error"] = repr(e)
+        try:
             line["cpu_baseline"] = cpu_baseline_sample()
         except Exception as e:
             line["cpu_baseline_error"] = repr(e)
@@ -474,10 +484,56 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     return res
 
 
+# Serving rings: one per ring degree, one key-switch digit per ciphertext
+# prime where the special prime is a single prime (noise stays small over
+# chains), and the most multiplies per chain each ring's noise budget allows.
+SERVE_RINGS = [  # (log_n, q bits, p bits, dnum, max multiplies per chain)
+    (12, [36, 36], [37], 2, 1),
+    (13, [50, 50, 50], [52], 3, 3),
+    (14, [60] * 7, [60], 7, 4),
+    (15, [60] * 14, [60, 60], 3, 4),
+]
+
+
+def serving(args):
+    """Open-loop Poisson streams of 1-4 op chains (mult+relin / add) over
+    N = 4096, 8192, 16384, 32768 through the request server; every result is
+    decrypted and checked exactly. Latency is submit-to-decrypted-result."""
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200.serve import Ring, Server, make_workload, run_open_loop
+    rings = [Ring.make(kb.BFVContext.from_bits(ln, qb, pb, T, dnum=d), bytes([40 + i]) * 32)
+             for i, (ln, qb, pb, d, _) in enumerate(SERVE_RINGS)]
+    w = make_workload(rings, 64, [m for *_, m in SERVE_RINGS], seed=11)
+    points = []
+    with Server(rings, hbm_budget_bytes=8 << 30, max_batch=32, pinned_bytes=1 << 30) as srv:
+        run_open_loop(srv, w, rate=200.0, duration_s=0.5, seed=99)  # warm-up
+        for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
+            pt = run_open_loop(srv, w, rate=rate, duration_s=args.serve_seconds, seed=100 + i,
+                               enc_base=(i + 1) << 36)
+            points.append(pt)
+        st = srv.stats()
+    ok = [p for p in points if p["throughput"] >= 0.9 * p["offered"] / p["submit_span_s"]]
+    head = ok[-1] if ok else points[0]
+    return {
+        "rings": [{"N": 1 << ln, "q_bits": qb, "p_bits": pb, "dnum": d, "max_mul": m}
+                  for ln, qb, pb, d, m in SERVE_RINGS],
+        "chains": "1-4 ops, 60% multiply (capped per ring), fresh seeded encryptions",
+        "points": points,
+        "all_decryptions_exact": all(p["wrong"] == 0 and p["errors"] == 0 for p in points),
+        "headline_rate": head["rate"], "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
+        "throughput": head["throughput"],
+        "server": {"iterations": st["iterations"], "mul_launches": st["mul_launches"], "mul_ops": st["mul_ops"],
+                   "add_ops": st["add_ops"], "device_bytes_peak": st["bytes_peak"]},
+    }
+
+
 def main():
     args = parse()
     if args.kernel:
         run_kernel_case(args)
+        return
+    if args.serving_only:
+        print(json.dumps(serving(args)), flush=True)
         return
     world, rank, local = dist_init(args)
     try:

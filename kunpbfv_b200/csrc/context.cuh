@@ -45,6 +45,7 @@ struct DevConsts {
     // key switching
     const uint64_t *p_mod_q, *pinv_q, *pinv_qs, *phatinv_p, *phatinv_ps, *phat_mod_q;
     const uint64_t *dig_hatinv, *dig_hatinvs, *dig_hat_mod, *dig_q_mod;
+    const uint64_t* dig_vq_mod;  // [d][v = 0..alpha][npq]: v * Q_d mod p_m
     // Gaussian table
     const uint64_t* gauss_cdt;
     int gauss_bound;

@@ -338,8 +338,15 @@ static void build_context(Context& c, const kbfv_params& prm) {
             dqm[(size_t)d * npq + m] = qm;
         }
     }
-    size_t o_ks[10] = {blob.add(pmq), blob.add(pinv), blob.add(pinvs), blob.add(phi), blob.add(phis),
-                       blob.add(phm), blob.add(dhi), blob.add(dhis), blob.add(dhm), blob.add(dqm)};
+    // v * Q_d mod p_m for the lift's quotient estimate v = 0..alpha
+    std::vector<uint64_t> dvq((size_t)c.dnum * (c.alpha + 1) * npq);
+    for (int d = 0; d < c.dnum; d++)
+        for (int v = 0; v <= c.alpha; v++)
+            for (int m = 0; m < npq; m++)
+                dvq[((size_t)d * (c.alpha + 1) + v) * npq + m] =
+                    H::mulmod((uint64_t)v, dqm[(size_t)d * npq + m], c.mods[m]);
+    size_t o_ks[11] = {blob.add(pmq), blob.add(pinv), blob.add(pinvs), blob.add(phi), blob.add(phis),
+                       blob.add(phm), blob.add(dhi), blob.add(dhis), blob.add(dhm), blob.add(dqm), blob.add(dvq)};
     // T-base key switch constants (include/BasisConv.cuh:11-226; the reference's
     // precompute is in include/BFVcontext.cuh). Blocks lift by approximate CRT:
     // (B/b_j)^-1 mod b_j, B/b_j mod t_k and B mod t_k per block B.
@@ -429,6 +436,7 @@ static void build_context(Context& c, const kbfv_params& prm) {
     dc.p_mod_q = U(o_ks[0]); dc.pinv_q = U(o_ks[1]); dc.pinv_qs = U(o_ks[2]); dc.phatinv_p = U(o_ks[3]);
     dc.phatinv_ps = U(o_ks[4]); dc.phat_mod_q = U(o_ks[5]); dc.dig_hatinv = U(o_ks[6]);
     dc.dig_hatinvs = U(o_ks[7]); dc.dig_hat_mod = U(o_ks[8]); dc.dig_q_mod = U(o_ks[9]);
+    dc.dig_vq_mod = U(o_ks[10]);
     dc.gauss_cdt = U(o_cdt);
     if (c.klss_ok) {
         KlssConsts& k = c.kc;

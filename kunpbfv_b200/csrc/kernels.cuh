@@ -156,7 +156,8 @@ __device__ __forceinline__ void modup_coeff(const DevConsts& c, const uint64_t* 
                 vv = __fadd_rn(vv, __fdiv_rn(__ull2float_rn(rb[i]), __ull2float_rn(qi)));
             }
         }
-        const uint64_t vf = (uint64_t)__float2int_rz(vv);
+        const int vf = min(__float2int_rz(vv), c.alpha);
+        const uint64_t* vq = c.dig_vq_mod + ((size_t)d * (c.alpha + 1) + vf) * c.npq;
         uint64_t* o = out + ((size_t)d * c.npq << c.logn);
         // the digit's own primes: the input residues
 #pragma unroll
@@ -170,8 +171,8 @@ __device__ __forceinline__ void modup_coeff(const DevConsts& c, const uint64_t* 
 #pragma unroll
             for (int i = 0; i < MAXQ; i++)
                 if (i >= lo && i < hi) mac(acc, rb[i], hm[i]);
-            sub128(acc, vf * c.dig_q_mod[(size_t)d * c.npq + m]);
-            o[((size_t)m << c.logn) + k] = barrett128(acc, c.mods[m], c.mu_hi[m], c.mu_lo[m]);
+            // subtract v * Q_d after reducing: the sum can be below v * Q_d (one-prime digits)
+            o[((size_t)m << c.logn) + k] = sub_mod(barrett128(acc, c.mods[m], c.mu_hi[m], c.mu_lo[m]), vq[m], c.mods[m]);
         }
     }
 }

@@ -202,7 +202,7 @@ def run_open_loop(server: Server, w: Workload, rate: float, duration_s: float, s
     arrivals = arrivals[arrivals < duration_s]
     ids = []
     lock = threading.Lock()
-    lat, wrong, errors = [], [0], []
+    lat, wrong, errors, bad = [], [0], [], []
     done = threading.Event()
 
     def collector():
@@ -224,6 +224,9 @@ def run_open_loop(server: Server, w: Workload, rate: float, duration_s: float, s
                 lat.append(ms)
                 if not np.array_equal(res, w.want[tmpl]):
                     wrong[0] += 1
+                    if len(bad) < 8:
+                        bad.append({"request": rid, "ring": w.ring[tmpl], "ops": w.ops[tmpl],
+                                    "slots_wrong": int(np.count_nonzero(res != w.want[tmpl]))})
             except KbfvError as e:
                 errors.append(str(e))
             i += 1
@@ -250,4 +253,5 @@ def run_open_loop(server: Server, w: Workload, rate: float, duration_s: float, s
         "throughput": round(len(lat) / t_all, 1),
         "p50_ms": round(float(np.percentile(lat_a, 50)), 3), "p99_ms": round(float(np.percentile(lat_a, 99)), 3),
         "mean_ms": round(float(lat_a.mean()), 3),
+        **({"wrong_detail": bad} if bad else {}),
     }

@@ -708,7 +708,11 @@ void orc_delta_m(const orc_ctx* c, const u64* m, u64* out) {
 /* ======================================================================= */
 /* Digit lift: restates modUpQjtoT_23_kernel's approximate CRT with the
  * single-precision quotient estimate (BasisConv.cuh:86-135), targeting the
- * primes of P and of Q outside the digit instead of the T base. */
+ * primes of P and of Q outside the digit instead of the T base. One change:
+ * v * (Q_d mod p) is subtracted after reducing the sum, not from the 128-bit
+ * sum. The reference subtracts first; when a digit has one prime the sum is
+ * x < q_j, the float estimate can round x / q_j up to 1, and the 128-bit
+ * subtraction wraps, giving a residue inconsistent with the other primes. */
 void orc_modup(const orc_ctx* c, const u64* d2, u64* out) {
     u64 n = c->n;
     int nq = c->nq, np = c->np, npq = nq + np;
@@ -731,8 +735,9 @@ void orc_modup(const orc_ctx* c, const u64* d2, u64* out) {
                 u128 acc = 0;
                 const u64* hm = c->dig_hat_mod + ((size_t)d * npq + m) * c->alpha;
                 for (int j = lo; j < hi; j++) acc += (u128)rb[j - lo] * hm[j - lo];
-                acc -= (u128)((u64)vf * c->dig_Q_mod[(size_t)d * npq + m]);
-                o[(size_t)m * n + k] = (u64)(acc % mod);
+                u64 sub = (u64)(((u128)(u64)vf * c->dig_Q_mod[(size_t)d * npq + m]) % mod);
+                u64 r = (u64)(acc % mod);
+                o[(size_t)m * n + k] = r >= sub ? r - sub : r + mod - sub;
             }
         }
     }
@@ -1128,7 +1133,7 @@ void orc_keygen_secret(const orc_ctx* c, const uint8_t key[32], int kind, int h,
 void orc_keygen_public(const orc_ctx* c, const uint8_t key[32], const u64* sk, u64* pk) {
     u64 n = c->n;
     int nq = c->nq;
-    int idx[64];
+    int idx[64] = {0};
     for (int i = 0; i < nq; i++) idx[i] = i;
     u64* a = pk;
     u64* b = pk + (size_t)nq * n;

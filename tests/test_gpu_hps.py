@@ -7,7 +7,7 @@ from tests.gpu_util import c3_pair, dev, host, rand_rows, small_pair
 pytestmark = pytest.mark.gpu
 
 PAIRS = [("c3", lambda: c3_pair()), ("small", lambda: small_pair(12, 3, 1, 50)),
-         ("dnum2", lambda: small_pair(12, 4, 2, 45, 2))]
+         ("dnum2", lambda: small_pair(12, 4, 2, 45, 2)), ("onedigit", lambda: small_pair(12, 3, 1, 50, 3))]
 
 
 @pytest.fixture(params=PAIRS, ids=[p[0] for p in PAIRS])

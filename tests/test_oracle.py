@@ -272,6 +272,26 @@ def test_hybrid_dnum(oracle_mod):
         assert np.array_equal(o.decode(o.decrypt(sk, c3)), (v1 * v2) % T65537)
 
 
+def test_modup_one_prime_digits_consistent(oracle_mod):
+    """With one prime per digit the lift's float estimate of x / q_j rounds to
+    1 for x close to q_j; the lifted residues must still represent one integer
+    (x or x - q_j) in every prime of Q|P."""
+    qs, ps = small_primes(12, 3, 1, 50)
+    o = oracle_mod.Oracle(12, T65537, qs, ps, dnum=3)
+    n = o.n
+    rng = np.random.default_rng(3)
+    x = np.stack([rng.integers(0, q, size=n, dtype=np.uint64) for q in qs])
+    for j, q in enumerate(qs):  # values whose float ratio to q rounds to 1.0
+        x[j, :64] = q - 1 - np.arange(64, dtype=np.uint64)
+    lift = o.modup(x)
+    PQ = list(qs) + list(ps)
+    for d, qd in enumerate(qs):
+        for k in list(range(64)) + [100, 2000]:
+            v = int(x[d, k])
+            got = [int(lift[d, m, k]) for m in range(len(PQ))]
+            assert got in ([v % m for m in PQ], [(v - qd) % m for m in PQ]), (d, k)
+
+
 def test_xsalsa20_against_libsodium(oracle_mod):
     """Pin the XSalsa20 keystream to libsodium's crypto_secretbox (PyNaCl):
     secretbox XORs the message with keystream bytes from offset 32."""
