@@ -61,6 +61,7 @@ typedef struct {
     uint32_t t_count;         /* optional KLSS base (reference key switch), may be 0 */
     const uint64_t* t_primes;
     uint32_t gamma;           /* KLSS Ri block size */
+    uint32_t digit_primes;    /* key-switch digit size alpha; 0 = ceil(q_count / dnum) */
 } kbfv_params;
 
 /* Parameter set from per-prime bit sizes (SEAL-style coeff_modulus sizes):
@@ -205,6 +206,30 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
 /* same for consecutive ciphertexts (stride 2*q_count*N words) */
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
+/* ---- levels: fewer live ciphertext primes --------------------------------
+ * A ciphertext at level l holds the first l primes of Q (2 x l limbs, NTT form).
+ * kbfv_context_at_level: the context for l live primes (l = q_count returns
+ * ctx itself); owned by ctx and freed with it. It shares the top level's keys:
+ * its multiply reads the top-level relinearisation key through a limb map (digit
+ * d keeps the top level's primes [d*alpha, (d+1)*alpha) that are still live,
+ * plus P), its decryption the top-level secret key. Keys and encryptions are made
+ * on the top-level context. No counterpart in the reference (its rescale is
+ * CKKS-style flooring, include/BFVScheme.cuh:400-502). */
+int kbfv_context_at_level(kbfv_context* ctx, uint32_t live_q, kbfv_context** out);
+/* BFV modulus switch: divide by the last live prime and round, c' = round(c / q_l),
+ * in NTT form (SEAL's divide_and_round_q_last). ctx_level is the input's level
+ * context (q_count >= 2); d_out receives count ciphertexts of q_count - 1 limbs
+ * and must not overlap d_ct. */
+int kbfv_mod_switch(kbfv_context* ctx_level, const uint64_t* d_ct, uint64_t* d_out, uint32_t count,
+                    kbfv_stream stream);
+/* Multiply + relinearise a batch whose pairs sit at different levels: pair i has
+ * live_q[i] live primes (both inputs and the output at that level). One call on
+ * one stream: pairs are grouped by level and each group runs as one batched
+ * launch sequence of that level's context. d_rlk is the top-level key. */
+int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32_t* live_q,
+                          const uint64_t* const* ct_a, const uint64_t* const* ct_b, uint64_t* const* out,
+                          uint32_t count, kbfv_stream stream);
 
 /* ---- key switch over the auxiliary T base (the reference's own method) ---
  * Available when the context has T primes (kbfv_params.t_count), q_count is a

@@ -60,6 +60,7 @@ class _Params(C.Structure):
         ("t_count", C.c_uint32),
         ("t_primes", U64P),
         ("gamma", C.c_uint32),
+        ("digit_primes", C.c_uint32),
     ]
 
 
@@ -130,6 +131,9 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_ntt_fwd_batch": (I, [VP, C.POINTER(VP), u32, u32, u32, VP]),
         "kbfv_ntt_inv_batch": (I, [VP, C.POINTER(VP), u32, u32, u32, VP]),
         "kbfv_add_plain": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_context_at_level": (I, [VP, u32, C.POINTER(VP)]),
+        "kbfv_mod_switch": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_mul_relin_levels": (I, [VP, VP, C.POINTER(u32), C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
         "kbfv_rlk_to_klss": (I, [VP, VP, VP, VP]),
         "kbfv_klss_modup_qj_to_t": (I, [VP, VP, VP, u32, VP]),
         "kbfv_klss_modup_pq_to_t": (I, [VP, VP, VP, u32, VP]),
@@ -202,6 +206,7 @@ class Params:
     p: Optional[Sequence[int]] = None
     t_primes: Sequence[int] = ()
     gamma: int = 1
+    digit_primes: int = 0
 
 
 class BFVContext:
@@ -211,8 +216,9 @@ class BFVContext:
     ``K`` (= p_count), ``slots`` (= N), ``plain_modulus``.
     """
 
-    def __init__(self, params: Optional[Params] = None, *, _handle=None, **kw):
+    def __init__(self, params: Optional[Params] = None, *, _handle=None, _owner=None, **kw):
         L = lib()
+        self._owner = _owner  # level contexts belong to their top-level context
         if _handle is not None:
             self._h = _handle
         else:
@@ -230,7 +236,7 @@ class BFVContext:
 
             pr = _Params(params.log_n, params.plain_modulus, params.q_count, arr(params.q), params.q_bits,
                          params.p_count, arr(params.p), params.p_bits, params.dnum, len(params.t_primes),
-                         arr(list(params.t_primes)), params.gamma)
+                         arr(list(params.t_primes)), params.gamma, params.digit_primes)
             h = VP()
             _check(L.kbfv_context_create(C.byref(pr), C.byref(h)))
             self._h = h
@@ -276,9 +282,20 @@ class BFVContext:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h is not None and _lib is not None:
+        if h is not None and _lib is not None and getattr(self, "_owner", None) is None:
             _lib.kbfv_context_destroy(h)
         self._h = None
+
+    def at_level(self, live_q: int) -> "BFVContext":
+        """the context for ciphertexts with the first live_q primes of Q (owned by this one)"""
+        if live_q == self.q_count and self._owner is None:
+            return self
+        cache = self.__dict__.setdefault("_levels", {})
+        if live_q not in cache:
+            h = VP()
+            _check(lib().kbfv_context_at_level(self._h, live_q, C.byref(h)))
+            cache[live_q] = BFVContext(_handle=h, _owner=self)
+        return cache[live_q]
 
     def __del__(self):
         try:
@@ -542,15 +559,15 @@ class BFVScheme:
         return ct
 
     def decryptMsg(self, sk: SecretKey, ct: Ciphertext, stream=None) -> Plaintext:
-        ctx = self.context
+        ctx = ct.ctx  # the ciphertext's level
         pt = Plaintext(ctx, count=ct.count)
         _check(lib().kbfv_decrypt(ctx.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), _ptr(pt.mx_device),
                                   ct.count, _stream_ptr(stream)))
         return pt
 
     def add(self, c1: Ciphertext, c2: Ciphertext, stream=None) -> Ciphertext:
-        out = Ciphertext(self.context, count=c1.count)
-        _check(lib().kbfv_add(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device),
+        out = Ciphertext(c1.ctx, count=c1.count)
+        _check(lib().kbfv_add(c1.ctx.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device),
                               _ptr(out.cipher_device), c1.count, _stream_ptr(stream)))
         return out
 
@@ -590,13 +607,13 @@ class BFVScheme:
         """Batched ct1[i] * ct2[i] with relinearisation (multAndEqual_23 without the shortcut)."""
         if self.rlk is None:
             raise KbfvError(-5, "rotKey_23 not exists")
-        out = out if out is not None else Ciphertext(self.context, count=c1.count)
+        out = out if out is not None else Ciphertext(c1.ctx, count=c1.count)
         if self.relin == "klss":
             _check(lib().kbfv_mul_relin_klss(self.context.handle, _ptr(self.rlk_t), _ptr(c1.cipher_device),
                                              _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count,
                                              _stream_ptr(stream)))
-        else:
-            _check(lib().kbfv_mul_relin(self.context.handle, _ptr(self.rlk), _ptr(c1.cipher_device),
+        else:  # at the ciphertexts' level, with the top-level key
+            _check(lib().kbfv_mul_relin(c1.ctx.handle, _ptr(self.rlk), _ptr(c1.cipher_device),
                                         _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count,
                                         _stream_ptr(stream)))
         return out
@@ -608,12 +625,37 @@ class BFVScheme:
         O = (VP * n)(*out_ptrs)
         _check(lib().kbfv_mul_relin_batch(self.context.handle, _ptr(self.rlk), A, B, O, n, _stream_ptr(stream)))
 
+    def mod_switch(self, ct: Ciphertext, stream=None) -> Ciphertext:
+        """drop the last live prime (divide and round); the result lives at ct.ctx's level - 1"""
+        top = ct.ctx._owner or ct.ctx
+        lower = top.at_level(ct.ctx.q_count - 1)
+        out = Ciphertext(lower, count=ct.count)
+        _check(lib().kbfv_mod_switch(ct.ctx.handle, _ptr(ct.cipher_device), _ptr(out.cipher_device), ct.count,
+                                     _stream_ptr(stream)))
+        return out
+
+    def mod_switch_to(self, ct: Ciphertext, live_q: int, stream=None) -> Ciphertext:
+        while ct.ctx.q_count > live_q:
+            ct = self.mod_switch(ct, stream)
+        return ct
+
+    def mult_relin_levels(self, pairs, stream=None):
+        """[(ct_a, ct_b)] at possibly different levels -> products, one call"""
+        n = len(pairs)
+        outs = [Ciphertext(a.ctx, count=1) for a, _ in pairs]
+        lv = (C.c_uint32 * n)(*[a.ctx.q_count for a, _ in pairs])
+        A = (VP * n)(*[_ptr(a.cipher_device) for a, _ in pairs])
+        B = (VP * n)(*[_ptr(b.cipher_device) for _, b in pairs])
+        O = (VP * n)(*[_ptr(o.cipher_device) for o in outs])
+        _check(lib().kbfv_mul_relin_levels(self.context.handle, _ptr(self.rlk), lv, A, B, O, n, _stream_ptr(stream)))
+        return outs
+
     def multAndEqual_23(self, c1: Ciphertext, c2: Ciphertext, stream=None):
         self.mult_relin(c1, c2, out=c1, stream=stream)
 
     def noise_budget(self, sk: SecretKey, ct: Ciphertext) -> float:
         v = C.c_double()
-        _check(lib().kbfv_noise_budget(self.context.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), C.byref(v)))
+        _check(lib().kbfv_noise_budget(ct.ctx.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), C.byref(v)))
         return float(v.value)
 
 

@@ -46,6 +46,10 @@ struct DevConsts {
     const uint64_t *p_mod_q, *pinv_q, *pinv_qs, *phatinv_p, *phatinv_ps, *phat_mod_q;
     const uint64_t *dig_hatinv, *dig_hatinvs, *dig_hat_mod, *dig_q_mod;
     const uint64_t* dig_vq_mod;  // [d][v = 0..alpha][npq]: v * Q_d mod p_m
+    int key_nq, key_npq;         // limb layout of the relinearisation key (top level's Q and Q|P counts)
+    // modulus switch: q_last^-1 mod q_i (+ Shoup), floor(q_last / 2) mod q_i, for i < nq - 1
+    const uint64_t *ms_qlinv, *ms_qlinvs, *ms_half_mod;
+    uint64_t ms_half;
     // Gaussian table
     const uint64_t* gauss_cdt;
     int gauss_bound;
@@ -103,6 +107,9 @@ struct Context {
     KlssConsts kc{};
     // seed used by keygen / encryption calls that pass no seed (kbfv_set_seed)
     uint8_t seed[32] = {0};
+    // levels: contexts for fewer live primes, owned by the top level (index = live primes)
+    const Context* parent = nullptr;
+    std::vector<void*> levels;
 };
 
 }  // namespace kbfv

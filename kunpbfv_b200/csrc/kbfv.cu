@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -157,9 +158,14 @@ static void build_context(Context& c, const kbfv_params& prm) {
     c.nr = c.nq + 1;
     c.nt = (int)prm.t_count;
     c.gamma = prm.gamma ? (int)prm.gamma : 1;
-    c.dnum = prm.dnum ? (int)prm.dnum : 1;
-    KB_REQUIRE(c.dnum <= c.nq, KBFV_ERR_INVALID, "dnum exceeds q_count");
-    c.alpha = (c.nq + c.dnum - 1) / c.dnum;
+    if (prm.digit_primes) {  // explicit digit size (levels keep the top level's digits)
+        c.alpha = (int)prm.digit_primes;
+        c.dnum = (c.nq + c.alpha - 1) / c.alpha;
+    } else {
+        c.dnum = prm.dnum ? (int)prm.dnum : 1;
+        KB_REQUIRE(c.dnum <= c.nq, KBFV_ERR_INVALID, "dnum exceeds q_count");
+        c.alpha = (c.nq + c.dnum - 1) / c.dnum;
+    }
     KB_REQUIRE(H::is_prime(c.t) && (c.t - 1) % (2 * c.n) == 0, KBFV_ERR_PARAMS,
                "plain modulus must be a prime congruent to 1 mod 2N");
 
@@ -196,6 +202,8 @@ static void build_context(Context& c, const kbfv_params& prm) {
     dc.dnum = c.dnum; dc.alpha = c.alpha; dc.npq = c.nq + c.np; dc.nqr = c.nq + c.nr;
     dc.idx_p = c.nq; dc.idx_r = c.nq + c.np; dc.idx_t = c.nq + c.np + c.nr; dc.idx_pt = nall - 1;
     dc.t = c.t;
+    dc.key_nq = c.nq;
+    dc.key_npq = c.nq + c.np;
 
     Blob blob;
     std::vector<uint64_t> mu_hi(nall), mu_lo(nall);
@@ -412,6 +420,18 @@ static void build_context(Context& c, const kbfv_params& prm) {
         for (int i = 0; i < 14; i++) o_kl[i] = blob.add(*tabs[i]);
         c.kc.nt = nt; c.kc.gamma = g; c.kc.nri = nri; c.kc.nqj = nqj;
     }
+    // modulus switch by the last prime
+    std::vector<uint64_t> msi(c.nq, 0), msis(c.nq, 0), msh(c.nq, 0);
+    {
+        const uint64_t ql = Q[c.nq - 1];
+        dc.ms_half = ql >> 1;
+        for (int i = 0; i + 1 < c.nq; i++) {
+            msi[i] = H::invmod(ql % Q[i], Q[i]);
+            msis[i] = H::shoup(msi[i], Q[i]);
+            msh[i] = dc.ms_half % Q[i];
+        }
+    }
+    size_t o_ms[3] = {blob.add(msi), blob.add(msis), blob.add(msh)};
     std::vector<uint64_t> cdt;
     gaussian_cdt(3.2, 19, cdt);
     dc.gauss_bound = 19;
@@ -437,6 +457,7 @@ static void build_context(Context& c, const kbfv_params& prm) {
     dc.phatinv_ps = U(o_ks[4]); dc.phat_mod_q = U(o_ks[5]); dc.dig_hatinv = U(o_ks[6]);
     dc.dig_hatinvs = U(o_ks[7]); dc.dig_hat_mod = U(o_ks[8]); dc.dig_q_mod = U(o_ks[9]);
     dc.dig_vq_mod = U(o_ks[10]);
+    dc.ms_qlinv = U(o_ms[0]); dc.ms_qlinvs = U(o_ms[1]); dc.ms_half_mod = U(o_ms[2]);
     dc.gauss_cdt = U(o_cdt);
     if (c.klss_ok) {
         KlssConsts& k = c.kc;
@@ -714,9 +735,11 @@ struct KeyIPSrc {
         const int item = row / (2 * npq), w = row % (2 * npq), h = w / npq, m = w % npq;
         KeyIPRow r;
         r.dig = sd2 + (((size_t)item * dc.dnum * npq + m) << logn);
-        r.key = rlk + (((size_t)h * npq + m) << logn);
+        // key limbs: [digit][a|b][Q|P] of the top level; a level reads its live Q limbs and P
+        const int km = m < dc.nq ? m : dc.key_nq + (m - dc.nq);
+        r.key = rlk + (((size_t)h * dc.key_npq + km) << logn);
         r.ds = (size_t)npq << logn;
-        r.ks = (size_t)2 * npq << logn;
+        r.ks = (size_t)2 * dc.key_npq << logn;
         r.dnum = dc.dnum;
         r.q = dc.mods[m]; r.mh = dc.mu_hi[m]; r.ml = dc.mu_lo[m];
         return r;
@@ -935,6 +958,59 @@ struct PtrPolysIO {
     }
 };
 
+static void require_top(const Context& c) {
+    KB_REQUIRE(!c.parent, KBFV_ERR_LEVEL, "keys and encryptions are made on the top-level context");
+}
+
+// ---- modulus switch (divide by the last prime and round) ---------------------
+struct LastLimbSrc {  // row = polynomial: its last limb
+    const uint64_t* ct;
+    int logn, nq;
+    __device__ __forceinline__ int prime(int) const { return nq - 1; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        return PtrRow{const_cast<uint64_t*>(ct) + (((size_t)row * nq + nq - 1) << logn)};
+    }
+};
+struct ModSwitchRow {
+    const uint64_t* last;
+    uint64_t ql, half, q, mh, half_i;
+    // [x + floor(ql/2)]_ql - floor(ql/2), taken mod q_i: the rounding correction
+    __device__ __forceinline__ uint64_t load(int j) const {
+        const uint64_t x = csub(last[j] + half, ql);
+        return sub_mod(barrett64(x, q, mh), half_i, q);
+    }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct ModSwitchSrc {  // rows (poly, i < nq-1)
+    const uint64_t* last;  // [poly][N], coefficient form, < q_last
+    DevConsts dc;
+    __device__ __forceinline__ int prime(int row) const { return row % (dc.nq - 1); }
+    __device__ __forceinline__ ModSwitchRow bind(int row) const {
+        const int nout = dc.nq - 1, poly = row / nout, i = row % nout;
+        ModSwitchRow r;
+        r.last = last + ((size_t)poly << dc.logn);
+        r.ql = dc.mods[dc.nq - 1];
+        r.half = dc.ms_half;
+        r.q = dc.mods[i]; r.mh = dc.mu_hi[i];
+        r.half_i = dc.ms_half_mod[i];
+        return r;
+    }
+};
+// out[poly][i] = (ct[poly][i] - corr[poly][i]) * q_last^-1 mod q_i
+__global__ void mod_switch_combine_kernel(DevConsts c, const uint64_t* __restrict__ ct,
+                                          const uint64_t* __restrict__ corr, uint64_t* __restrict__ out,
+                                          size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int nout = c.nq - 1;
+    const size_t row = i >> c.logn, j = i & (((size_t)1 << c.logn) - 1);
+    const size_t poly = row / nout;
+    const int l = (int)(row % nout);
+    const uint64_t q = c.mods[l];
+    const uint64_t x = ct[((poly * c.nq + l) << c.logn) + j];
+    out[i] = shoup(x + q - corr[i], c.ms_qlinv[l], c.ms_qlinvs[l], q);
+}
+
 static void require_klss(const Context& c) {
     KB_REQUIRE(c.klss_ok, KBFV_ERR_INVALID,
                "context has no T-base key switch (needs T primes, q_count divisible by p_count, dnum = q_count / p_count)");
@@ -1006,6 +1082,8 @@ int kbfv_context_destroy(kbfv_context* ctx) {
         if (!ctx) return;
         Context& c = ctx->c;
         cudaDeviceSynchronize();
+        for (void* lv : c.levels)
+            if (lv) kbfv_context_destroy((kbfv_context*)lv);
         if (c.pool) cudaFree(c.pool);
         if (c.scratch) cudaFree(c.scratch);
         if (c.ptrs_event) cudaEventDestroy(c.ptrs_event);
@@ -1232,6 +1310,7 @@ int kbfv_keygen_secret(kbfv_context* ctx, const uint8_t seed[32], int secret_kin
                        kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
+        require_top(c);
         if (!seed) seed = c.seed;
         KB_REQUIRE(d_sk, KBFV_ERR_INVALID, "null argument");
         const int npq = c.nq + c.np;
@@ -1253,6 +1332,7 @@ int kbfv_keygen_public(kbfv_context* ctx, const uint8_t seed[32], const uint64_t
                        kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
+        require_top(c);
         if (!seed) seed = c.seed;
         KB_REQUIRE(d_sk && d_pk, KBFV_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
@@ -1272,6 +1352,7 @@ int kbfv_keygen_relin(kbfv_context* ctx, const uint8_t seed[32], const uint64_t*
                       kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
+        require_top(c);
         if (!seed) seed = c.seed;
         KB_REQUIRE(d_sk && d_rlk, KBFV_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
@@ -1340,6 +1421,7 @@ int kbfv_encrypt(kbfv_context* ctx, const uint8_t seed[32], uint64_t enc_id, con
                  uint64_t* d_ct, uint32_t count, kbfv_stream stream) {
     return guarded([&] {
         Context& c = CX(ctx);
+        require_top(c);
         if (!seed) seed = c.seed;
         KB_REQUIRE(d_pk && d_m && d_ct, KBFV_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
@@ -1812,6 +1894,106 @@ int kbfv_add_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_m,
                                                                 c.nq);
             }
             check_launch("add_plain");
+        }
+    });
+}
+
+
+// ---- levels ---------------------------------------------------------------
+int kbfv_context_at_level(kbfv_context* ctx, uint32_t live_q, kbfv_context** out) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(out, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE(!c.parent, KBFV_ERR_INVALID, "levels are taken from the top-level context");
+        KB_REQUIRE(live_q >= 1 && live_q <= (uint32_t)c.nq, KBFV_ERR_LEVEL, "live prime count out of range");
+        if (live_q == (uint32_t)c.nq) {
+            *out = ctx;
+            return;
+        }
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.levels.size() < (size_t)c.nq) c.levels.resize(c.nq, nullptr);
+        if (!c.levels[live_q]) {
+            kbfv_params prm;
+            std::memset(&prm, 0, sizeof prm);
+            prm.log_n = (uint32_t)c.logn;
+            prm.plain_modulus = c.t;
+            prm.q_count = live_q;
+            prm.q = c.mods.data();
+            prm.p_count = (uint32_t)c.np;
+            prm.p = c.mods.data() + c.nq;
+            prm.digit_primes = (uint32_t)c.alpha;
+            auto* h = new kbfv_context();
+            try {
+                build_context(h->c, prm);
+            } catch (...) {
+                if (h->c.pool) cudaFree(h->c.pool);
+                delete h;
+                throw;
+            }
+            h->c.parent = &c;
+            h->c.dc.key_nq = c.nq;
+            h->c.dc.key_npq = c.nq + c.np;
+            std::memcpy(h->c.seed, c.seed, 32);
+            c.levels[live_q] = h;
+        }
+        *out = (kbfv_context*)c.levels[live_q];
+    });
+}
+
+int kbfv_mod_switch(kbfv_context* ctx, const uint64_t* d_ct, uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(c.nq >= 2, KBFV_ERR_LEVEL, "a ciphertext with one live prime cannot be switched down");
+        KB_REQUIRE(d_ct && d_out, KBFV_ERR_INVALID, "null argument");
+        const size_t in_words = (size_t)count * 2 * c.nq * c.n, out_words = (size_t)count * 2 * (c.nq - 1) * c.n;
+        KB_REQUIRE(d_out + out_words <= d_ct || d_ct + in_words <= d_out, KBFV_ERR_INVALID,
+                   "output must not overlap the input");
+        cudaStream_t st = S(stream);
+        const DevConsts& dc = c.dc;
+        const int nout = c.nq - 1;
+        const uint32_t chunk = 32;
+        for (uint32_t off = 0; off < count; off += chunk) {
+            const int cnt = (int)std::min<uint32_t>(chunk, count - off);
+            const int polys = cnt * 2;
+            uint64_t* last = (uint64_t*)ensure_scratch(c, (size_t)polys * (1 + nout) * c.n * 8);
+            uint64_t* corr = last + ((size_t)polys << c.logn);
+            const uint64_t* in = d_ct + (size_t)off * 2 * c.nq * c.n;
+            uint64_t* o = d_out + (size_t)off * 2 * nout * c.n;
+            ntt_inv(dc, LastLimbSrc{in, c.logn, c.nq}, rows_io(dc, last, c.nq - 1, 1), polys, st);
+            ntt_fwd(dc, ModSwitchSrc{last, dc}, rows_io(dc, corr, 0, nout), polys * nout, st);
+            const size_t total = (size_t)polys * nout * c.n;
+            mod_switch_combine_kernel<<<blocks_for(total, 256), 256, 0, st>>>(dc, in, corr, o, total);
+            check_launch("mod_switch");
+        }
+    });
+}
+
+int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32_t* live_q,
+                          const uint64_t* const* ct_a, const uint64_t* const* ct_b, uint64_t* const* out,
+                          uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(!c.parent, KBFV_ERR_INVALID, "call on the top-level context");
+        KB_REQUIRE(live_q && ct_a && ct_b && out, KBFV_ERR_INVALID, "null pointer array");
+        std::map<uint32_t, std::vector<uint32_t>> groups;
+        for (uint32_t i = 0; i < count; i++) {
+            KB_REQUIRE(live_q[i] >= 1 && live_q[i] <= (uint32_t)c.nq, KBFV_ERR_LEVEL, "live prime count out of range");
+            groups[live_q[i]].push_back(i);
+        }
+        for (auto it = groups.rbegin(); it != groups.rend(); ++it) {  // highest level first
+            kbfv_context* lv = nullptr;
+            int rc = kbfv_context_at_level(ctx, it->first, &lv);
+            if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+            std::vector<const uint64_t*> A, B;
+            std::vector<uint64_t*> O;
+            for (uint32_t i : it->second) {
+                A.push_back(ct_a[i]);
+                B.push_back(ct_b[i]);
+                O.push_back(out[i]);
+            }
+            rc = kbfv_mul_relin_batch(lv, d_rlk, A.data(), B.data(), O.data(), (uint32_t)A.size(), stream);
+            if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
         }
     });
 }

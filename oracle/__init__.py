@@ -57,6 +57,7 @@ def _declare(L: C.CDLL) -> None:
         "orc_destroy": (V, [C.c_void_p]),
         "orc_set_ref_compat": (V, [C.c_void_p, C.c_int]),
         "orc_klss_relinearize": (V, [C.c_void_p, U64P, U64P, U64P]),
+        "orc_mod_switch": (V, [C.c_void_p, U64P, U64P, C.c_int]),
         "orc_prime_count": (C.c_int, [C.c_void_p]),
         "orc_primes": (V, [C.c_void_p, U64P]),
         "orc_psi": (C.c_uint64, [C.c_void_p, C.c_int]),
@@ -171,7 +172,8 @@ def gaussian_cdt(sigma: float = 3.2, bound: int = 19) -> np.ndarray:
 class Oracle:
     """An oracle context for one parameter set (see ``orc_create``)."""
 
-    def __init__(self, log_n: int, t: int, q, p, dnum: int = 1, tk=(), gamma: int = 1):
+    def __init__(self, log_n: int, t: int, q, p, dnum: int = 1, tk=(), gamma: int = 1, alpha: int = 0):
+        """alpha > 0 fixes the key-switch digit size (digits = ceil(nq / alpha))."""
         L = lib()
         self.log_n = log_n
         self.n = 1 << log_n
@@ -179,11 +181,12 @@ class Oracle:
         self.nq, self.np_ = len(q), len(p)
         self.nr = self.nq + 1
         self.nt = len(tk)
-        self.dnum = dnum
+        self.dnum = -(-len(q) // alpha) if alpha else dnum
         qa = np.array(q, dtype=np.uint64)
         pa = np.array(p if len(p) else [0], dtype=np.uint64)
         ta = np.array(tk if len(tk) else [0], dtype=np.uint64)
-        self._h = L.orc_create(log_n, t, _p(qa), len(q), _p(pa), len(p), dnum, _p(ta), len(tk), gamma)
+        self._h = L.orc_create(log_n, t, _p(qa), len(q), _p(pa), len(p), -alpha if alpha else dnum, _p(ta), len(tk),
+                               gamma)
         if not self._h:
             raise ValueError("oracle context creation failed (not enough R primes)")
         cnt = L.orc_prime_count(self._h)
@@ -272,6 +275,9 @@ class Oracle:
 
     def moddown(self, x, npoly: int = 2):
         return self._call("orc_moddown", x, out_shape=(npoly, self.nq, self.n), extra=(npoly,))
+
+    def mod_switch(self, ct, npoly: int = 2):
+        return self._call("orc_mod_switch", ct, out_shape=(npoly, self.nq - 1, self.n), extra=(npoly,))
 
     # ---- KLSS
     def klss_blocks(self):

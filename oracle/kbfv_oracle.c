@@ -347,8 +347,13 @@ orc_ctx* orc_create(uint32_t log_n, u64 t, const u64* q, int nq, const u64* p, i
     orc_ctx* c = calloc(1, sizeof *c);
     c->n = (u64)1 << log_n; c->logn = (int)log_n; c->t = t;
     c->nq = nq; c->np = np; c->nr = nq + 1; c->nt = nt; c->gamma = gamma > 0 ? gamma : 1;
-    c->dnum = dnum > 0 ? dnum : 1;
-    c->alpha = (nq + c->dnum - 1) / c->dnum;
+    if (dnum < 0) {  /* digit size given: alpha = -dnum */
+        c->alpha = -dnum;
+        c->dnum = (nq + c->alpha - 1) / c->alpha;
+    } else {
+        c->dnum = dnum > 0 ? dnum : 1;
+        c->alpha = (nq + c->dnum - 1) / c->dnum;
+    }
     c->nall = nq + np + c->nr + nt + 1;
     c->mods = malloc(c->nall * 8);
     int k = 0;
@@ -770,6 +775,39 @@ void orc_moddown(const orc_ctx* c, const u64* in, u64* out, int npoly) {
             }
         }
     }
+}
+
+/* BFV modulus switch by the last prime q_l: c' = round(c / q_l) over the
+ * remaining primes, in NTT form. Restates SEAL's divide_and_round_q_last_ntt
+ * (the reference has only a CKKS-style flooring rescale, BFVScheme.cuh:400-502):
+ * x = INTT(c_l); r_i = ([x + floor(q_l/2)]_{q_l} - floor(q_l/2)) mod q_i;
+ * c'_i = (c_i - NTT_i(r_i)) * q_l^-1 mod q_i. */
+void orc_mod_switch(const orc_ctx* c, const u64* ct, u64* out, int npoly) {
+    u64 n = c->n;
+    int nq = c->nq, nout = nq - 1;
+    u64 ql = c->mods[nq - 1], half = ql >> 1;
+    u64* last = malloc(n * 8);
+    u64* corr = malloc(n * 8);
+    for (int pl = 0; pl < npoly; pl++) {
+        const u64* x = ct + (size_t)pl * nq * n;
+        u64* y = out + (size_t)pl * nout * n;
+        memcpy(last, x + (size_t)(nq - 1) * n, n * 8);
+        ntt_inv_limbs(c, nq - 1, last, 1);
+        for (int i = 0; i < nout; i++) {
+            u64 qi = c->mods[i], hi = half % qi, inv = invmod(ql % qi, qi);
+            for (u64 k = 0; k < n; k++) {
+                u64 v = (last[k] + half) % ql % qi;
+                corr[k] = v >= hi ? v - hi : v + qi - hi;
+            }
+            ntt_fwd_limbs(c, i, corr, 1);
+            for (u64 k = 0; k < n; k++) {
+                u64 d = x[(size_t)i * n + k] + qi - corr[k];
+                if (d >= qi) d -= qi;
+                y[(size_t)i * n + k] = mulmod(d, inv, qi);
+            }
+        }
+    }
+    free(last); free(corr);
 }
 
 /* ======================================================================= */

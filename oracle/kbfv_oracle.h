@@ -34,7 +34,8 @@ uint64_t orc_root_2n(uint64_t q, uint64_t n);
 int      orc_root_is_primitive(uint64_t psi, uint64_t q, uint64_t n);
 
 /* ---- context ----------------------------------------------------------- */
-/* q: nq ciphertext primes; p: np special primes; dnum: key-switch digits;
+/* q: nq ciphertext primes; p: np special primes; dnum: key-switch digits
+ * (dnum < 0: digit size alpha = -dnum primes, digits = ceil(nq / alpha));
  * tk: optional KLSS T primes (nt may be 0), gamma: KLSS Ri block size.
  * The R base is derived here by the reference rule (nq+1 primes below min q). */
 orc_ctx* orc_create(uint32_t log_n, uint64_t t, const uint64_t* q, int nq,
@@ -69,6 +70,8 @@ void orc_delta_m(const orc_ctx* c, const uint64_t* m, uint64_t* out_q);
 void orc_modup(const orc_ctx* c, const uint64_t* d2, uint64_t* out);
 /* in: 2 polys x (nq+np) limbs coefficient form -> 2 polys x nq limbs */
 void orc_moddown(const orc_ctx* c, const uint64_t* in, uint64_t* out, int npoly);
+/* BFV modulus switch by the last prime: npoly polys of nq limbs (NTT) -> nq - 1 limbs */
+void orc_mod_switch(const orc_ctx* c, const uint64_t* ct, uint64_t* out, int npoly);
 /* KLSS restatement (reference's own key-switch base conversions) */
 int  orc_klss_ri_blocks(const orc_ctx* c);
 int  orc_klss_qj_blocks(const orc_ctx* c);

@@ -1,0 +1,138 @@
+"""Levels on the B200: the modulus switch, multiplies at lower levels with the
+top-level key, and the uneven batch of config C4 (N=32768, 14 x 60-bit q +
+2 x 60-bit special primes, digits of 5 primes, pairs at depths 0-3 in one call)."""
+import functools
+
+import numpy as np
+import pytest
+
+from tests.gpu_util import dev, host
+
+pytestmark = pytest.mark.gpu
+
+T = 65537
+SEED = b"\x33" * 32
+
+
+@functools.lru_cache(maxsize=None)
+def small():
+    """N=4096, 6 x 50-bit q, 2 x 52-bit p, digits of 2 primes; product and oracle."""
+    import kunpbfv_b200 as kb
+    import oracle
+    p = oracle.primes_bits(4096, 52, 2)
+    q = oracle.primes_bits(4096, 50, 6, skip=p)
+    ctx = kb.BFVContext(log_n=12, plain_modulus=T, q_count=6, q=q, p_count=2, p=p, dnum=3)
+    assert ctx.alpha == 2
+    sk = kb.SecretKey(ctx, SEED)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    top = oracle.Oracle(12, T, q, p, alpha=2)
+    osk = top.keygen_secret(SEED)
+    return ctx, sk, sch, top, osk, q, p
+
+
+def test_mod_switch_bit_exact():
+    import kunpbfv_b200 as kb
+    import oracle
+    ctx, sk, sch, top, osk, q, p = small()
+    rng = np.random.default_rng(1)
+    v = rng.integers(0, T, size=(3, ctx.N), dtype=np.uint64)
+    ct = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v))), enc_id=40)
+    cur = ct
+    want = host(ct.cipher_device).reshape(3, 2, 6, ctx.N)
+    for live in (5, 4, 3, 2, 1):
+        cur = sch.mod_switch(cur)
+        assert cur.ctx.q_count == live
+        o = oracle.Oracle(12, T, q[:live + 1], p, alpha=2)
+        want = np.stack([o.mod_switch(want[i]) for i in range(3)])
+        assert np.array_equal(host(cur.cipher_device).reshape(want.shape), want), live
+        dec = host(cur.ctx.decode(sch.decryptMsg(sk, cur).mx_device)).reshape(3, ctx.N)
+        assert np.array_equal(dec, v), live
+    with pytest.raises(kb.KbfvError):
+        sch.mod_switch(cur)  # one live prime left
+
+
+def test_level_multiply_bit_exact():
+    """At every level the product equals the oracle's multiply with the top-level
+    key restricted to the live primes, and decrypts exactly."""
+    import kunpbfv_b200 as kb
+    import oracle
+    ctx, sk, sch, top, osk, q, p = small()
+    orlk = top.keygen_relin(SEED, osk)
+    assert np.array_equal(host(sch.rlk).reshape(orlk.shape), orlk)
+    rng = np.random.default_rng(2)
+    v1 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=50)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=60)
+    for live in (6, 5, 4, 3):
+        o = oracle.Oracle(12, T, q[:live], p, alpha=2)
+        rl = np.stack([np.stack([np.concatenate([orlk[d][h][:live], orlk[d][h][6:]]) for h in range(2)])
+                       for d in range(o.dnum)])
+        out = sch.mult_relin(c1, c2)
+        got = host(out.cipher_device).reshape(2, 2, live, ctx.N)
+        h1 = host(c1.cipher_device).reshape(2, 2, live, ctx.N)
+        h2 = host(c2.cipher_device).reshape(2, 2, live, ctx.N)
+        for i in range(2):
+            assert np.array_equal(got[i], o.mul_relin(h1[i], h2[i], rl)), (live, i)
+        dec = host(out.ctx.decode(sch.decryptMsg(sk, out).mx_device)).reshape(2, ctx.N)
+        assert np.array_equal(dec, (v1 * v2) % T), live
+        if live > 3:
+            c1, c2 = sch.mod_switch(c1), sch.mod_switch(c2)
+
+
+def test_level_context_rules():
+    import kunpbfv_b200 as kb
+    ctx, sk, sch, *_ = small()
+    lv = ctx.at_level(4)
+    assert lv.q_count == 4 and lv.q == ctx.q[:4] and lv.p == ctx.p and lv.alpha == 2 and lv.dnum == 2
+    assert ctx.at_level(4) is lv and ctx.at_level(6) is ctx
+    with pytest.raises(kb.KbfvError):
+        ctx.at_level(7)
+    with pytest.raises(kb.KbfvError):  # keys are made on the top level
+        kb.BFVScheme(lv, SEED).addMultKey_23(sk)
+
+
+def test_c4_uneven_batch():
+    """16 pairs at depths 0-3 (14, 13, 12, 11 live primes) in one call; every
+    product equals the pair multiplied alone at its level and decrypts exactly;
+    one pair per level is also checked against the oracle."""
+    import kunpbfv_b200 as kb
+    import oracle
+    ctx = kb.BFVContext.from_bits(15, [60] * 14, [60, 60], T, dnum=3)
+    assert ctx.alpha == 5
+    sk = kb.SecretKey(ctx, SEED)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    rng = np.random.default_rng(4)
+    pairs, vals = [], []
+    for j in range(16):
+        depth = j % 4
+        v1 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+        v2 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+        a = sch.mod_switch_to(sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=100 + 2 * j), 14 - depth)
+        b = sch.mod_switch_to(sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=101 + 2 * j), 14 - depth)
+        pairs.append((a, b))
+        vals.append((v1 * v2) % T)
+    outs = sch.mult_relin_levels(pairs)
+    for j, ((a, b), o) in enumerate(zip(pairs, outs)):
+        assert o.ctx.q_count == 14 - j % 4
+        dec = host(o.ctx.decode(sch.decryptMsg(sk, o).mx_device)).reshape(-1)
+        assert np.array_equal(dec, vals[j]), j
+        if j < 8:
+            alone = sch.mult_relin(a, b)
+            assert np.array_equal(host(alone.cipher_device), host(o.cipher_device)), j
+    # the oracle on the deepest and the top pair
+    top = oracle.Oracle(15, T, ctx.q, ctx.p, alpha=5)
+    osk = top.keygen_secret(SEED)
+    assert np.array_equal(host(sk.sx_device).reshape(osk.shape), osk)
+    orlk = top.keygen_relin(SEED, osk)
+    for j in (0, 3):
+        live = 14 - j
+        o = oracle.Oracle(15, T, ctx.q[:live], ctx.p, alpha=5)
+        rl = np.stack([np.stack([np.concatenate([orlk[d][h][:live], orlk[d][h][14:]]) for h in range(2)])
+                       for d in range(o.dnum)])
+        a, b = (host(x.cipher_device).reshape(2, live, ctx.N) for x in pairs[j])
+        assert np.array_equal(host(outs[j].cipher_device).reshape(2, live, ctx.N), o.mul_relin(a, b, rl)), j

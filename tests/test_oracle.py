@@ -292,6 +292,71 @@ def test_modup_one_prime_digits_consistent(oracle_mod):
             assert got in ([v % m for m in PQ], [(v - qd) % m for m in PQ]), (d, k)
 
 
+def _levels_setup(oracle_mod):
+    """6 x 50-bit q, 2 x 52-bit special primes, digits of 2 primes (dnum 3), N=4096."""
+    p = oracle_mod.primes_bits(4096, 52, 2)
+    q = oracle_mod.primes_bits(4096, 50, 6, skip=p)
+    top = oracle_mod.Oracle(12, T65537, q, p, alpha=2)
+    key = b"\x33" * 32
+    sk = top.keygen_secret(key)
+    return top, q, p, key, sk, top.keygen_public(key, sk), top.keygen_relin(key, sk)
+
+
+def _crt_rows(rows, mods):
+    Q = 1
+    for m in mods:
+        Q *= m
+    acc = [0] * rows.shape[1]
+    for i, m in enumerate(mods):
+        f = (Q // m) * pow(Q // m, -1, m)
+        for k, v in enumerate(rows[i]):
+            acc[k] += int(v) * f
+    return [a % Q for a in acc], Q
+
+
+def test_mod_switch_is_divide_and_round(oracle_mod):
+    """c' = (c - r) / q_l with r = c mod q_l centred: checked with big integers."""
+    top, q, p, key, sk, pk, rlk = _levels_setup(oracle_mod)
+    rng = np.random.default_rng(8)
+    ct = top.encrypt(key, 5, pk, top.encode(rng.integers(0, T65537, size=top.n, dtype=np.uint64)))
+    out = top.mod_switch(ct)
+    lower = oracle_mod.Oracle(12, T65537, q[:5], p, alpha=2)
+    ql, h = q[5], q[5] >> 1
+    for poly in range(2):
+        coef = np.stack([top.ntt_inv(i, ct[poly][i]) for i in range(6)])
+        big, _ = _crt_rows(coef, q)
+        got = np.stack([lower.ntt_inv(i, out[poly][i]) for i in range(5)])
+        gbig, Q5 = _crt_rows(got, q[:5])
+        for k in range(0, top.n, 97):
+            r = (big[k] + h) % ql - h
+            assert (big[k] - r) % ql == 0
+            assert gbig[k] == ((big[k] - r) // ql) % Q5, k
+
+
+def test_levels_decrypt_and_multiply(oracle_mod):
+    """Encrypt at the top level, switch down, multiply at each level with the
+    top-level key restricted to the live primes (digits keep their top-level
+    primes; the last digit may be partial), decrypt exactly."""
+    top, q, p, key, sk, pk, rlk = _levels_setup(oracle_mod)
+    rng = np.random.default_rng(9)
+    v1 = rng.integers(0, T65537, size=top.n, dtype=np.uint64)
+    v2 = rng.integers(0, T65537, size=top.n, dtype=np.uint64)
+    c1 = top.encrypt(key, 1, pk, top.encode(v1))
+    c2 = top.encrypt(key, 2, pk, top.encode(v2))
+    nq = len(q)
+    for live in (6, 5, 4, 3):
+        o = oracle_mod.Oracle(12, T65537, q[:live], p, alpha=2)
+        skl = np.concatenate([sk[:live], sk[nq:]])
+        assert np.array_equal(o.decode(o.decrypt(skl, c1)), v1)
+        dl = o.dnum
+        rl = np.stack([np.stack([np.concatenate([rlk[d][h][:live], rlk[d][h][nq:]]) for h in range(2)])
+                       for d in range(dl)])
+        prod = o.mul_relin(c1, c2, rl)
+        assert np.array_equal(o.decode(o.decrypt(skl, prod)), (v1 * v2) % T65537), live
+        if live > 3:
+            c1, c2 = o.mod_switch(c1), o.mod_switch(c2)
+
+
 def test_xsalsa20_against_libsodium(oracle_mod):
     """Pin the XSalsa20 keystream to libsodium's crypto_secretbox (PyNaCl):
     secretbox XORs the message with keystream bytes from offset 32."""
