@@ -207,6 +207,21 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);
 
+/* ---- key switching over a gadget decomposition of base 2^w --------------
+ * No counterpart in the reference. a1*a2 = sum_i [a1*a2]_{q_i} * g_i (mod Q),
+ * g_i = Q/q_i * [(Q/q_i)^-1]_{q_i}; each residue is cut into J = ceil(60 / w)
+ * pieces of w bits (small integers, the same in every prime), so no base
+ * conversion is needed and the key-switch noise is about J * q_count * 2^w *
+ * sigma * N / P. Key: q_count * J components [a|b] over Q|P (NTT form, layout
+ * [i*J + j][a|b][Q|P]): b = e - a*s + 2^{wj} * P * [prime == q_i] * s^2.
+ * 4 <= w <= 30. Works at levels (kbfv_context_at_level) with the top-level key. */
+int kbfv_keygen_relin_gadget(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint32_t log_base,
+                             uint64_t* d_gk, kbfv_stream stream);
+int kbfv_relinearize_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_base, const uint64_t* d_tensor,
+                            uint64_t* d_ct, uint32_t count, kbfv_stream stream);
+int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_base, const uint64_t* d_ct_a,
+                          const uint64_t* d_ct_b, uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
 /* ---- levels: fewer live ciphertext primes --------------------------------
  * A ciphertext at level l holds the first l primes of Q (2 x l limbs, NTT form).
  * kbfv_context_at_level: the context for l live primes (l = q_count returns

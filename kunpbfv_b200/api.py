@@ -132,6 +132,9 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_ntt_inv_batch": (I, [VP, C.POINTER(VP), u32, u32, u32, VP]),
         "kbfv_add_plain": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_context_at_level": (I, [VP, u32, C.POINTER(VP)]),
+        "kbfv_keygen_relin_gadget": (I, [VP, U8P, VP, u32, VP, VP]),
+        "kbfv_relinearize_gadget": (I, [VP, VP, u32, VP, VP, u32, VP]),
+        "kbfv_mul_relin_gadget": (I, [VP, VP, u32, VP, VP, VP, u32, VP]),
         "kbfv_mod_switch": (I, [VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_levels": (I, [VP, VP, C.POINTER(u32), C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
         "kbfv_rlk_to_klss": (I, [VP, VP, VP, VP]),
@@ -506,11 +509,14 @@ class Tensor3:
 class BFVScheme:
     """BFVScheme (include/BFVScheme.h:12-178) over one context."""
 
-    def __init__(self, ctx: BFVContext, seed: bytes = b"\x00" * 32, relin: str = "hybrid"):
-        """relin: "hybrid" (digit lift over Q|P, the default) or "klss" (the
-        reference's key switch over the T base; needs a context with T primes)."""
-        if relin not in ("hybrid", "klss"):
-            raise ValueError("relin must be 'hybrid' or 'klss'")
+    def __init__(self, ctx: BFVContext, seed: bytes = b"\x00" * 32, relin: str = "hybrid", gadget_log_base: int = 20):
+        """relin: "hybrid" (digit lift over Q|P, the default), "klss" (the
+        reference's key switch over the T base; needs a context with T primes)
+        or "gadget" (base-2^gadget_log_base decomposition of every residue)."""
+        if relin not in ("hybrid", "klss", "gadget"):
+            raise ValueError("relin must be 'hybrid', 'klss' or 'gadget'")
+        self.gadget_log_base = gadget_log_base
+        self.gk = None
         self.context = ctx
         self.seed = bytes(seed)
         self.relin = relin
@@ -537,6 +543,16 @@ class BFVScheme:
                                        _stream_ptr(stream)))
         if self.relin == "klss":
             self.convert_rlk_klss(stream)
+        if self.relin == "gadget":
+            self.addGadgetKey(sk, self.gadget_log_base, stream)
+
+    def addGadgetKey(self, sk: SecretKey, log_base: int = 20, stream=None):
+        ctx = self.context
+        pieces = -(-60 // log_base)
+        self.gadget_log_base = log_base
+        self.gk = ctx.zeros(ctx.q_count * pieces, 2, ctx.q_count + ctx.p_count, ctx.N)
+        _check(lib().kbfv_keygen_relin_gadget(ctx.handle, _u8(self.seed), _ptr(sk.sx_device), log_base,
+                                              _ptr(self.gk), _stream_ptr(stream)))
 
     def convert_rlk_klss(self, stream=None):
         """The T-form copy of self.rlk (addMultKey_23's conversion, KeySwitch_23.cuh:55-65)."""
@@ -585,21 +601,24 @@ class BFVScheme:
                                     _ptr(ct.cipher_device), ct.count, _stream_ptr(stream)))
 
     def mult(self, c1: Ciphertext, c2: Ciphertext, stream=None) -> Tensor3:
-        out = Tensor3(self.context, count=c1.count)
-        _check(lib().kbfv_mul(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device), _ptr(out.data),
+        out = Tensor3(c1.ctx, count=c1.count)
+        _check(lib().kbfv_mul(c1.ctx.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device), _ptr(out.data),
                               c1.count, _stream_ptr(stream)))
         return out
 
     def relinearize(self, t3: Tensor3, stream=None) -> Ciphertext:
         if self.rlk is None:
             raise KbfvError(-5, "rotKey_23 not exists")
-        cnt = t3.data.numel() // (3 * self.context.q_count * self.context.N)
-        out = Ciphertext(self.context, count=cnt)
-        if self.relin == "klss":
+        cnt = t3.data.numel() // (3 * t3.ctx.q_count * t3.ctx.N)
+        out = Ciphertext(t3.ctx, count=cnt)
+        if self.relin == "gadget":
+            _check(lib().kbfv_relinearize_gadget(t3.ctx.handle, _ptr(self.gk), self.gadget_log_base, _ptr(t3.data),
+                                                 _ptr(out.cipher_device), cnt, _stream_ptr(stream)))
+        elif self.relin == "klss":
             _check(lib().kbfv_relinearize_klss(self.context.handle, _ptr(self.rlk_t), _ptr(t3.data),
                                                _ptr(out.cipher_device), cnt, _stream_ptr(stream)))
         else:
-            _check(lib().kbfv_relinearize(self.context.handle, _ptr(self.rlk), _ptr(t3.data),
+            _check(lib().kbfv_relinearize(t3.ctx.handle, _ptr(self.rlk), _ptr(t3.data),
                                           _ptr(out.cipher_device), cnt, _stream_ptr(stream)))
         return out
 
@@ -608,7 +627,11 @@ class BFVScheme:
         if self.rlk is None:
             raise KbfvError(-5, "rotKey_23 not exists")
         out = out if out is not None else Ciphertext(c1.ctx, count=c1.count)
-        if self.relin == "klss":
+        if self.relin == "gadget":
+            _check(lib().kbfv_mul_relin_gadget(c1.ctx.handle, _ptr(self.gk), self.gadget_log_base,
+                                               _ptr(c1.cipher_device), _ptr(c2.cipher_device), _ptr(out.cipher_device),
+                                               c1.count, _stream_ptr(stream)))
+        elif self.relin == "klss":
             _check(lib().kbfv_mul_relin_klss(self.context.handle, _ptr(self.rlk_t), _ptr(c1.cipher_device),
                                              _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count,
                                              _stream_ptr(stream)))

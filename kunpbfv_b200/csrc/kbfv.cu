@@ -726,22 +726,49 @@ struct KeyIPRow {
     __device__ __forceinline__ void store(int, uint64_t) const {}
 };
 struct KeyIPSrc {
-    const uint64_t* sd2;  // [item][dnum][npq]
-    const uint64_t* rlk;  // [dnum][2][npq]
+    const uint64_t* sd2;  // [item][ndig][npq]
+    const uint64_t* rlk;  // [ndig][2][npq]
     DevConsts dc;
+    int ndig;             // digits: dnum (hybrid) or q_count * pieces (gadget)
     __device__ __forceinline__ int prime(int row) const { return row % dc.npq; }
     __device__ __forceinline__ KeyIPRow bind(int row) const {
         const int npq = dc.npq, logn = dc.logn;
         const int item = row / (2 * npq), w = row % (2 * npq), h = w / npq, m = w % npq;
         KeyIPRow r;
-        r.dig = sd2 + (((size_t)item * dc.dnum * npq + m) << logn);
+        r.dig = sd2 + (((size_t)item * ndig * npq + m) << logn);
         // key limbs: [digit][a|b][Q|P] of the top level; a level reads its live Q limbs and P
         const int km = m < dc.nq ? m : dc.key_nq + (m - dc.nq);
         r.key = rlk + (((size_t)h * dc.key_npq + km) << logn);
         r.ds = (size_t)npq << logn;
         r.ks = (size_t)2 * dc.key_npq << logn;
-        r.dnum = dc.dnum;
+        r.dnum = ndig;
         r.q = dc.mods[m]; r.mh = dc.mu_hi[m]; r.ml = dc.mu_lo[m];
+        return r;
+    }
+};
+
+// Gadget decomposition source: rows (item, digit g = i*J + j, m) -> the j-th
+// w-bit piece of limb i of a1*a2 (coefficient form), the same small integer in
+// every prime m of Q|P.
+struct GadgetRow {
+    const uint64_t* x;
+    int shift;
+    uint64_t mask;
+    __device__ __forceinline__ uint64_t load(int j) const { return (x[j] >> shift) & mask; }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct GadgetDigitSrc {
+    const uint64_t* sd2;  // [item][nq]
+    DevConsts dc;
+    int pieces, w;
+    __device__ __forceinline__ int prime(int row) const { return row % dc.npq; }
+    __device__ __forceinline__ GadgetRow bind(int row) const {
+        const int ndig = dc.nq * pieces;
+        const int item = row / (ndig * dc.npq), g = (row / dc.npq) % ndig;
+        GadgetRow r;
+        r.x = sd2 + (((size_t)item * dc.nq + g / pieces) << dc.logn);
+        r.shift = w * (g % pieces);
+        r.mask = (w >= 64) ? ~0ULL : (((uint64_t)1 << w) - 1);
         return r;
     }
 };
@@ -894,7 +921,7 @@ static void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb,
     ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                    count * dc.dnum * dc.npq, st);
     // K6b: inner product with the key fused into INTT over Q|P
-    ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
+    ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
     // K7: mod down + add (cross | b1b2) fused into NTT over Q, written to the outputs
     ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
 }
@@ -1284,7 +1311,7 @@ static void hsalsa_host(const uint8_t key[32], const uint8_t nonce16[16], uint32
 }
 
 enum { DOM_SK = 1, DOM_PK_A = 2, DOM_PK_E = 3, DOM_RLK_A = 4, DOM_RLK_E = 5, DOM_ENC_V = 6, DOM_ENC_E0 = 7,
-       DOM_ENC_E1 = 8 };
+       DOM_ENC_E1 = 8, DOM_GK_A = 9, DOM_GK_E = 10 };
 
 static void sample_small(Context& c, const uint8_t seed[32], uint32_t domain, uint64_t id0, int kind, int prime0,
                          int limbs, uint64_t* out, size_t item_stride, int items, cudaStream_t st) {
@@ -1370,6 +1397,41 @@ int kbfv_keygen_relin(kbfv_context* ctx, const uint8_t seed[32], const uint64_t*
             ntt_fwd(c.dc, io, io, npq, st);
             rlk_combine_kernel<<<blocks_for(lpq, 256), 256, 0, st>>>(c.dc, a, d_sk, b, d, lpq);
             check_launch("rlk_combine");
+        }
+    });
+}
+
+static int gadget_pieces(int w) { return (60 + w - 1) / w; }
+
+int kbfv_keygen_relin_gadget(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint32_t log_base,
+                             uint64_t* d_gk, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_top(c);
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(d_sk && d_gk, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE(log_base >= 4 && log_base <= 30, KBFV_ERR_INVALID, "gadget base 2^w needs 4 <= w <= 30");
+        const int w = (int)log_base, J = gadget_pieces(w);
+        cudaStream_t st = S(stream);
+        const int npq = c.nq + c.np;
+        const size_t lpq = (size_t)npq * c.n;
+        for (int i = 0; i < c.nq; i++) {
+            uint64_t pm = 1;  // P mod q_i
+            for (int k = 0; k < c.np; k++) pm = H::mulmod(pm, c.mods[c.nq + k] % c.mods[i], c.mods[i]);
+            for (int j = 0; j < J; j++) {
+                const uint32_t sub = (uint32_t)(i * J + j);
+                uint64_t* a = d_gk + (size_t)sub * 2 * lpq;
+                uint64_t* b = a + lpq;
+                sample_uniform(c, seed, DOM_GK_A, sub, 0, 0, npq, a, 0, 1, st);
+                SalsaKey k = subkey_for(seed, DOM_GK_E, sub);
+                sample_small_kernel<1><<<blocks_for(c.n / 8, 128), 128, 0, st>>>(c.dc, k, 0, 0, npq, b, 0, 1);
+                check_launch("sample_gauss");
+                RowsIO io = rows_io(c.dc, b, 0, npq);
+                ntt_fwd(c.dc, io, io, npq, st);
+                const uint64_t g = H::mulmod(pm, H::powmod(2, (uint64_t)w * j, c.mods[i]), c.mods[i]);
+                gk_combine_kernel<<<blocks_for(lpq, 256), 256, 0, st>>>(c.dc, a, d_sk, b, i, g, lpq);
+                check_launch("gk_combine");
+            }
         }
     });
 }
@@ -1577,7 +1639,7 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
             check_launch("modup");
             ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                            cnt * dc.dnum * dc.npq, st);
-            ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
+            ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
             std::vector<uint64_t*> O(cnt);
             std::vector<const uint64_t*> Z(cnt);
             for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
@@ -1994,6 +2056,101 @@ int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32
             }
             rc = kbfv_mul_relin_batch(lv, d_rlk, A.data(), B.data(), O.data(), (uint32_t)A.size(), stream);
             if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+        }
+    });
+}
+
+
+// ---- key switching over a gadget decomposition ------------------------------
+// G1: pieces of a1*a2 (coefficient form, sd2) fused into the forward NTT over Q|P;
+// G2: inner product with the gadget key fused into the inverse NTT; G3: mod down
+// + add fused into the forward NTT over Q, written to the outputs.
+static size_t gadget_sg_bytes(const Context& c, int count, int w) {
+    return (size_t)count * c.nq * gadget_pieces(w) * (c.nq + c.np) * c.n * 8;
+}
+static int gadget_chunk(const Context& c, int w) {
+    const size_t per = gadget_sg_bytes(c, 1, w);
+    return (int)std::max<size_t>(1, std::min<size_t>(kMaxBatch, ((size_t)4 << 30) / per));
+}
+
+static void gadget_keyswitch(Context& c, const uint64_t* gk, int w, int count, const MulScratch& m, uint64_t* sg,
+                             cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    const int J = gadget_pieces(w), ndig = c.nq * J;
+    // fully reduced NTT outputs: the key product sums ndig terms below q^2
+    ntt_fwd<GadgetDigitSrc, RowsIO, true>(dc, GadgetDigitSrc{m.sd2, dc, J, w}, rows_io(dc, sg, 0, dc.npq),
+                                         count * ndig * dc.npq, st);
+    ntt_inv(dc, KeyIPSrc{sg, gk, dc, ndig}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
+}
+
+int kbfv_relinearize_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_base, const uint64_t* d_tensor,
+                            uint64_t* d_ct, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_gk, KBFV_ERR_NO_KEY, "gadget key missing");
+        KB_REQUIRE(log_base >= 4 && log_base <= 30, KBFV_ERR_INVALID, "gadget base 2^w needs 4 <= w <= 30");
+        KB_REQUIRE(c.nq * gadget_pieces((int)log_base) < 256, KBFV_ERR_INVALID, "too many gadget digits");
+        const int w = (int)log_base;
+        cudaStream_t st = S(stream);
+        const DevConsts& dc = c.dc;
+        const size_t lq = (size_t)c.nq * c.n;
+        const int chunk = gadget_chunk(c, w);
+        for (uint32_t off = 0; off < count; off += chunk) {
+            const int cnt = (int)std::min<uint32_t>(chunk, count - off);
+            const size_t mb = mul_scratch_layout(c, cnt, nullptr).bytes;
+            uint8_t* base = ensure_scratch(c, mb + gadget_sg_bytes(c, cnt, w));
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            uint64_t* sg = (uint64_t*)(base + mb);
+            const uint64_t* tz = d_tensor + (size_t)off * 3 * lq;
+            uint64_t* out = d_ct + (size_t)off * 2 * lq;
+            ntt_inv(dc, TensorA2{tz, dc.logn, dc.nq}, rows_io(dc, m.sd2, 0, dc.nq), cnt * dc.nq, st);
+            gadget_keyswitch(c, d_gk, w, cnt, m, sg, st);
+            std::vector<uint64_t*> O(cnt);
+            std::vector<const uint64_t*> Z(cnt);
+            for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
+            PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
+            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            for (int i = 0; i < cnt; i++) {
+                const size_t tot = 2 * lq;
+                add_kernel<<<blocks_for(tot, 256), 256, 0, st>>>(dc, out + (size_t)i * 2 * lq, tz + (size_t)i * 3 * lq + lq,
+                                                                 out + (size_t)i * 2 * lq, tot, dc.nq);
+            }
+            check_launch("relin_add");
+        }
+    });
+}
+
+int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_base, const uint64_t* d_ct_a,
+                          const uint64_t* d_ct_b, uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_gk, KBFV_ERR_NO_KEY, "gadget key missing");
+        KB_REQUIRE(log_base >= 4 && log_base <= 30, KBFV_ERR_INVALID, "gadget base 2^w needs 4 <= w <= 30");
+        KB_REQUIRE(c.nq * gadget_pieces((int)log_base) < 256, KBFV_ERR_INVALID, "too many gadget digits");
+        const int w = (int)log_base;
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        const int chunk = gadget_chunk(c, w);
+        for (uint32_t off = 0; off < count; off += chunk) {
+            const int cnt = (int)std::min<uint32_t>(chunk, count - off);
+            std::vector<const uint64_t*> A(cnt), B(cnt);
+            std::vector<uint64_t*> O(cnt);
+            for (int i = 0; i < cnt; i++) {
+                A[i] = d_ct_a + (size_t)(off + i) * 2 * lq;
+                B[i] = d_ct_b + (size_t)(off + i) * 2 * lq;
+                O[i] = d_out + (size_t)(off + i) * 2 * lq;
+            }
+            PtrBatch pb = make_batch(A.data(), B.data(), O.data(), cnt);
+            const size_t mb = mul_scratch_layout(c, cnt, nullptr).bytes;
+            uint8_t* base = ensure_scratch(c, mb + gadget_sg_bytes(c, cnt, w));
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            uint64_t* sg = (uint64_t*)(base + mb);
+            mul_front(c, pb, cnt, m, st);
+            k5_launch(c, cnt, m, nullptr, 2, st);
+            gadget_keyswitch(c, d_gk, w, cnt, m, sg, st);
+            ntt_fwd(c.dc, ModDownAddSrc{m.se, m.sd, c.dc}, OutCtDst{pb, c.dc.logn, c.dc.nq}, cnt * 2 * c.dc.nq, st);
         }
     });
 }

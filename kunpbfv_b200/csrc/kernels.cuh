@@ -502,6 +502,18 @@ __global__ void rlk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, 
     eb[i] = v;
 }
 
+// gadget key component: b = e - a*s + [l == prime] * g * s^2 (g = P * 2^{wj} mod q_prime)
+__global__ void gk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
+                                  uint64_t* __restrict__ eb, int prime, uint64_t g, size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int l = (int)(i >> c.logn);
+    const uint64_t q = c.mods[l], mh = c.mu_hi[l], ml = c.mu_lo[l];
+    uint64_t v = sub_mod(eb[i], mul_mod(a[i], s[i], q, mh, ml), q);
+    if (l == prime) v = add_mod(v, mul_mod(mul_mod(s[i], s[i], q, mh, ml), g, q, mh, ml), q);
+    eb[i] = v;
+}
+
 // encrypt: a = v*pk.a + e0, b = v*pk.b + e1 + dm (encryptZero/encryptMsg,
 // include/BFVScheme.cuh:87-146). work: items x [v | e0 | e1 | dm] x nq (NTT form)
 __global__ void enc_combine_kernel(DevConsts c, const uint64_t* __restrict__ pk, const uint64_t* __restrict__ work,

@@ -58,6 +58,9 @@ def _declare(L: C.CDLL) -> None:
         "orc_set_ref_compat": (V, [C.c_void_p, C.c_int]),
         "orc_klss_relinearize": (V, [C.c_void_p, U64P, U64P, U64P]),
         "orc_mod_switch": (V, [C.c_void_p, U64P, U64P, C.c_int]),
+        "orc_gadget_pieces": (C.c_int, [C.c_int]),
+        "orc_keygen_relin_gadget": (V, [C.c_void_p, U8P, U64P, C.c_int, U64P]),
+        "orc_relinearize_gadget": (V, [C.c_void_p, U64P, U64P, C.c_int, U64P]),
         "orc_prime_count": (C.c_int, [C.c_void_p]),
         "orc_primes": (V, [C.c_void_p, U64P]),
         "orc_psi": (C.c_uint64, [C.c_void_p, C.c_int]),
@@ -275,6 +278,20 @@ class Oracle:
 
     def moddown(self, x, npoly: int = 2):
         return self._call("orc_moddown", x, out_shape=(npoly, self.nq, self.n), extra=(npoly,))
+
+    def keygen_relin_gadget(self, key, sk, w: int):
+        J = int(lib().orc_gadget_pieces(w))
+        out = np.zeros((self.nq * J, 2, self.nq + self.np_, self.n), dtype=np.uint64)
+        sk = np.ascontiguousarray(sk, dtype=np.uint64)
+        lib().orc_keygen_relin_gadget(self._h, _p(_key(key)), _p(sk), w, _p(out))
+        return out
+
+    def relinearize_gadget(self, d, gk, w: int):
+        d = np.ascontiguousarray(d, dtype=np.uint64)
+        gk = np.ascontiguousarray(gk, dtype=np.uint64)
+        out = np.zeros((2, self.nq, self.n), dtype=np.uint64)
+        lib().orc_relinearize_gadget(self._h, _p(d), _p(gk), w, _p(out))
+        return out
 
     def mod_switch(self, ct, npoly: int = 2):
         return self._call("orc_mod_switch", ct, out_shape=(npoly, self.nq - 1, self.n), extra=(npoly,))

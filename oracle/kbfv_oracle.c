@@ -1148,7 +1148,7 @@ void orc_sample_hwt(const orc_ctx* c, const uint8_t key[32], uint32_t domain, ui
 /* scheme                                                                  */
 /* ======================================================================= */
 enum { DOM_SK = 1, DOM_PK_A = 2, DOM_PK_E = 3, DOM_RLK_A = 4, DOM_RLK_E = 5,
-       DOM_ENC_V = 6, DOM_ENC_E0 = 7, DOM_ENC_E1 = 8 };
+       DOM_ENC_V = 6, DOM_ENC_E0 = 7, DOM_ENC_E1 = 8, DOM_GK_A = 9, DOM_GK_E = 10 };
 
 static void small_to_rns(const orc_ctx* c, const int64_t* s, int p0, int nl, u64* out) {
     for (int l = 0; l < nl; l++) {
@@ -1367,6 +1367,81 @@ void orc_relinearize(const orc_ctx* c, const u64* d, const u64* rlk, u64* ct) {
         ct[lq + i] = addmod(d[2 * lq + i], dn[lq + i], q); /* b = b1b2 + b' */
     }
     free(d2); free(up); free(acc); free(dn);
+}
+
+/* ---- key switching over a gadget decomposition of base 2^w --------------
+ * d2 = sum_i [d2]_{q_i} * g_i (mod Q) with g_i = Q/q_i * [(Q/q_i)^-1]_{q_i};
+ * each residue [d2]_{q_i} < 2^60 is cut into J = ceil(60 / w) pieces of w bits,
+ * z_{ij} < 2^w, the same small integer in every prime. Key component (i, j):
+ * a uniform, b = e - a*s + 2^{wj} * P * [l == i] * s^2 mod p_l over Q|P. The
+ * product sum_{ij} NTT(z_ij) * key_ij is reduced by P (mod-down) as in the
+ * hybrid method. No counterpart in the reference. */
+int orc_gadget_pieces(int w) { return (60 + w - 1) / w; }
+
+void orc_keygen_relin_gadget(const orc_ctx* c, const uint8_t key[32], const u64* sk, int w, u64* gk) {
+    u64 n = c->n;
+    int nq = c->nq, np = c->np, npq = nq + np, J = orc_gadget_pieces(w);
+    int idx[128];
+    for (int i = 0; i < npq; i++) idx[i] = i;
+    int64_t* e = malloc(n * sizeof(int64_t));
+    for (int i = 0; i < nq; i++)
+        for (int j = 0; j < J; j++) {
+            uint32_t sub = (uint32_t)(i * J + j);
+            u64* a = gk + (size_t)sub * 2 * npq * n;
+            u64* b = a + (size_t)npq * n;
+            orc_sample_uniform(c, key, DOM_GK_A, 0, sub, idx, npq, a);
+            orc_sample_gaussian(c, key, DOM_GK_E, 0, sub, e);
+            small_to_rns(c, e, 0, npq, b);
+            ntt_fwd_limbs(c, 0, b, npq);
+            for (int l = 0; l < npq; l++) {
+                u64 q = c->mods[l];
+                u64 g = l == i ? mulmod(c->p_mod_q[l], powmod(2, (u64)w * j, q), q) : 0;
+                for (u64 k = 0; k < n; k++) {
+                    size_t id = (size_t)l * n + k;
+                    u64 v = submod(b[id], mulmod(a[id], sk[id], q), q);
+                    if (g) v = addmod(v, mulmod(mulmod(sk[id], sk[id], q), g, q), q);
+                    b[id] = v;
+                }
+            }
+        }
+    free(e);
+}
+
+void orc_relinearize_gadget(const orc_ctx* c, const u64* d, const u64* gk, int w, u64* ct) {
+    u64 n = c->n;
+    int nq = c->nq, np = c->np, npq = nq + np, J = orc_gadget_pieces(w);
+    size_t lq = (size_t)nq * n, lpq = (size_t)npq * n;
+    u64 mask = (w >= 64) ? ~0ULL : (((u64)1 << w) - 1);
+    u64* d2 = malloc(lq * 8);
+    u64* z = malloc(lpq * 8);
+    u64* acc = calloc(2 * lpq, 8);
+    u64* dn = malloc(2 * lq * 8);
+    memcpy(d2, d, lq * 8);
+    ntt_inv_limbs(c, 0, d2, nq);
+    for (int i = 0; i < nq; i++)
+        for (int j = 0; j < J; j++) {
+            for (int m = 0; m < npq; m++)
+                for (u64 k = 0; k < n; k++) z[(size_t)m * n + k] = (d2[(size_t)i * n + k] >> (w * j)) & mask;
+            ntt_fwd_limbs(c, 0, z, npq);
+            const u64* ka = gk + (size_t)(i * J + j) * 2 * lpq;
+            const u64* kb = ka + lpq;
+            for (size_t x = 0; x < lpq; x++) {
+                u64 q = c->mods[x / n];
+                acc[x] = addmod(acc[x], mulmod(z[x], ka[x], q), q);
+                acc[lpq + x] = addmod(acc[lpq + x], mulmod(z[x], kb[x], q), q);
+            }
+        }
+    ntt_inv_limbs(c, 0, acc, npq);
+    ntt_inv_limbs(c, 0, acc + lpq, npq);
+    orc_moddown(c, acc, dn, 2);
+    ntt_fwd_limbs(c, 0, dn, nq);
+    ntt_fwd_limbs(c, 0, dn + lq, nq);
+    for (size_t x = 0; x < lq; x++) {
+        u64 q = c->mods[x / n];
+        ct[x] = addmod(d[lq + x], dn[x], q);
+        ct[lq + x] = addmod(d[2 * lq + x], dn[lq + x], q);
+    }
+    free(d2); free(z); free(acc); free(dn);
 }
 
 void orc_mul_relin(const orc_ctx* c, const u64* ct1, const u64* ct2, const u64* rlk, u64* ct) {

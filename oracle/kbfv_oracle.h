@@ -70,6 +70,11 @@ void orc_delta_m(const orc_ctx* c, const uint64_t* m, uint64_t* out_q);
 void orc_modup(const orc_ctx* c, const uint64_t* d2, uint64_t* out);
 /* in: 2 polys x (nq+np) limbs coefficient form -> 2 polys x nq limbs */
 void orc_moddown(const orc_ctx* c, const uint64_t* in, uint64_t* out, int npoly);
+/* key switching over a gadget decomposition of base 2^w (J = ceil(60 / w) pieces
+ * per ciphertext prime); gk: nq * J x [a | b] x (nq+np) limbs, NTT form */
+int  orc_gadget_pieces(int w);
+void orc_keygen_relin_gadget(const orc_ctx* c, const uint8_t key[32], const uint64_t* sk, int w, uint64_t* gk);
+void orc_relinearize_gadget(const orc_ctx* c, const uint64_t* d, const uint64_t* gk, int w, uint64_t* ct);
 /* BFV modulus switch by the last prime: npoly polys of nq limbs (NTT) -> nq - 1 limbs */
 void orc_mod_switch(const orc_ctx* c, const uint64_t* ct, uint64_t* out, int npoly);
 /* KLSS restatement (reference's own key-switch base conversions) */

@@ -136,3 +136,70 @@ def test_c4_uneven_batch():
                        for d in range(o.dnum)])
         a, b = (host(x.cipher_device).reshape(2, live, ctx.N) for x in pairs[j])
         assert np.array_equal(host(outs[j].cipher_device).reshape(2, live, ctx.N), o.mul_relin(a, b, rl)), j
+
+
+def test_gadget_key_switch_bit_exact():
+    """Key switching over a base-2^20 gadget decomposition: the key equals the
+    oracle's, the multiply equals the oracle's at the top level and at level 4
+    (top-level key, first 4 x 3 components), decryptions exact."""
+    import kunpbfv_b200 as kb
+    import oracle
+    ctx, sk, sch, top, osk, q, p = small()
+    gs = kb.BFVScheme(ctx, SEED, relin="gadget", gadget_log_base=20)
+    gs.addEncKey(sk)
+    gs.addMultKey_23(sk)
+    ogk = top.keygen_relin_gadget(SEED, osk, 20)
+    assert np.array_equal(host(gs.gk).reshape(ogk.shape), ogk)
+    rng = np.random.default_rng(7)
+    v1 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+    c1 = gs.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=70)
+    c2 = gs.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=80)
+    for live in (6, 4):
+        o = oracle.Oracle(12, T, q[:live], p, alpha=2)
+        gl = np.stack([np.stack([np.concatenate([ogk[g][h][:live], ogk[g][h][6:]]) for h in range(2)])
+                       for g in range(live * 3)])
+        out = gs.mult_relin(c1, c2)
+        h1 = host(c1.cipher_device).reshape(2, 2, live, ctx.N)
+        h2 = host(c2.cipher_device).reshape(2, 2, live, ctx.N)
+        got = host(out.cipher_device).reshape(2, 2, live, ctx.N)
+        for i in range(2):
+            assert np.array_equal(got[i], o.relinearize_gadget(o.mul_tensor(h1[i], h2[i]), gl, 20)), (live, i)
+        # split form: tensor then gadget relinearisation
+        t3 = gs.mult(c1, c2)
+        assert np.array_equal(host(gs.relinearize(t3).cipher_device).reshape(got.shape), got)
+        dec = host(out.ctx.decode(gs.decryptMsg(sk, out).mx_device)).reshape(2, ctx.N)
+        assert np.array_equal(dec, (v1 * v2) % T), live
+        c1, c2 = gs.mod_switch_to(c1, 4), gs.mod_switch_to(c2, 4)
+
+
+def test_c4_gadget_at_each_depth():
+    """Config C4's external product over a base-2^20 gadget decomposition at
+    N=32768, 14 x 60-bit q + 2 x 60-bit p: pairs at depths 0-3 decrypt exactly;
+    the top pair equals the oracle."""
+    import kunpbfv_b200 as kb
+    import oracle
+    ctx = kb.BFVContext.from_bits(15, [60] * 14, [60, 60], T, dnum=3)
+    sk = kb.SecretKey(ctx, SEED)
+    gs = kb.BFVScheme(ctx, SEED, relin="gadget", gadget_log_base=20)
+    gs.addEncKey(sk)
+    gs.addMultKey_23(sk)
+    rng = np.random.default_rng(5)
+    outs = []
+    for depth in range(4):
+        v1 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+        v2 = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+        a = gs.mod_switch_to(gs.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=300 + 4 * depth), 14 - depth)
+        b = gs.mod_switch_to(gs.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=302 + 4 * depth), 14 - depth)
+        out = gs.mult_relin(a, b)
+        dec = host(out.ctx.decode(gs.decryptMsg(sk, out).mx_device)).reshape(2, ctx.N)
+        assert np.array_equal(dec, (v1 * v2) % T), depth
+        outs.append((a, b, out))
+    top = oracle.Oracle(15, T, ctx.q, ctx.p, alpha=5)
+    osk = top.keygen_secret(SEED)
+    ogk = top.keygen_relin_gadget(SEED, osk, 20)
+    a, b, out = outs[0]
+    ha = host(a.cipher_device).reshape(2, 2, 14, ctx.N)[0]
+    hb = host(b.cipher_device).reshape(2, 2, 14, ctx.N)[0]
+    want = top.relinearize_gadget(top.mul_tensor(ha, hb), ogk, 20)
+    assert np.array_equal(host(out.cipher_device).reshape(2, 2, 14, ctx.N)[0], want)

@@ -357,6 +357,37 @@ def test_levels_decrypt_and_multiply(oracle_mod):
             c1, c2 = o.mod_switch(c1), o.mod_switch(c2)
 
 
+def test_gadget_key_switch(oracle_mod):
+    """Key switching over a base-2^20 gadget decomposition (3 pieces per 60-bit
+    prime) decrypts exactly, at the top level and at a lower level with the
+    key restricted to the live primes, with far less noise than the hybrid
+    method's one-digit key switch."""
+    top, q, p, key, sk, pk, rlk = _levels_setup(oracle_mod)
+    w = 20
+    gk = top.keygen_relin_gadget(key, sk, w)
+    J = 3
+    assert gk.shape == (6 * J, 2, 8, top.n)
+    rng = np.random.default_rng(12)
+    v1 = rng.integers(0, T65537, size=top.n, dtype=np.uint64)
+    v2 = rng.integers(0, T65537, size=top.n, dtype=np.uint64)
+    c1 = top.encrypt(key, 1, pk, top.encode(v1))
+    c2 = top.encrypt(key, 2, pk, top.encode(v2))
+    d = top.mul_tensor(c1, c2)
+    out = top.relinearize_gadget(d, gk, w)
+    assert np.array_equal(top.decode(top.decrypt(sk, out)), (v1 * v2) % T65537)
+    hyb = top.relinearize(d, rlk)
+    assert top.noise_budget(sk, out) >= top.noise_budget(sk, hyb) - 1
+    # level 4 (two primes switched away) with the first 4 * J key components
+    o = oracle_mod.Oracle(12, T65537, q[:4], p, alpha=2)
+    a, b = top.mod_switch(c1), top.mod_switch(c2)
+    o5 = oracle_mod.Oracle(12, T65537, q[:5], p, alpha=2)
+    a, b = o5.mod_switch(a), o5.mod_switch(b)
+    gl = np.stack([np.stack([np.concatenate([gk[g][h][:4], gk[g][h][6:]]) for h in range(2)]) for g in range(4 * J)])
+    skl = np.concatenate([sk[:4], sk[6:]])
+    res = o.relinearize_gadget(o.mul_tensor(a, b), gl, w)
+    assert np.array_equal(o.decode(o.decrypt(skl, res)), (v1 * v2) % T65537)
+
+
 def test_xsalsa20_against_libsodium(oracle_mod):
     """Pin the XSalsa20 keystream to libsodium's crypto_secretbox (PyNaCl):
     secretbox XORs the message with keystream bytes from offset 32."""
