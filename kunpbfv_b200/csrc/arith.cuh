@@ -66,6 +66,21 @@ __device__ __forceinline__ uint64_t barrett128(u128 x, uint64_t q, uint64_t mu_h
     return r;
 }
 
+// Product-sized values, x < 2^(2k+2) with k = bit length of q (k <= 60): the
+// quotient comes from one 64x64 high product, t = floor(x / 2^(k-2)) and
+// mu = floor(2^(62+k) / q) < 2^64; the estimate is low by at most 3, so two
+// conditional subtractions (2q, then q) give [0, q).
+__device__ __forceinline__ uint64_t barrett_prod(u128 x, uint64_t q, uint64_t mu) {
+    const int s = 62 - __clzll(q);  // k - 2
+    const uint64_t t = (x.lo >> s) | (x.hi << (64 - s));
+    uint64_t r = x.lo - __umul64hi(t, mu) * q;
+    r = csub(r, q << 1);
+    return csub(r, q);
+}
+__device__ __forceinline__ uint64_t mul_mod_prod(uint64_t a, uint64_t b, uint64_t q, uint64_t mu) {
+    return barrett_prod(mul_wide(a, b), q, mu);
+}
+
 // 64-bit value mod q with the high word of mu: floor(a * mu_hi / 2^64) errs by at most 1
 __device__ __forceinline__ uint64_t barrett64(uint64_t a, uint64_t q, uint64_t mu_hi) {
     uint64_t r = a - __umul64hi(a, mu_hi) * q;

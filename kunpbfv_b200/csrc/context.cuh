@@ -24,6 +24,7 @@ struct DevConsts {
     const uint64_t* mods;
     const uint64_t* mu_hi;
     const uint64_t* mu_lo;
+    const uint64_t* mu_prod;  // floor(2^(62+k) / q), k = bit length (barrett_prod)
     const tw_t* tw_fwd;   // [prime][N]
     const tw_t* tw_inv;   // [prime][N]; [0] = n^-1, [1] = psi_br^-1[1] * n^-1
     // HPS base extension Q -> R

@@ -208,7 +208,13 @@ static void build_context(Context& c, const kbfv_params& prm) {
     Blob blob;
     std::vector<uint64_t> mu_hi(nall), mu_lo(nall);
     for (int i = 0; i < nall; i++) H::barrett_mu(c.mods[i], mu_hi[i], mu_lo[i]);
+    std::vector<uint64_t> mu_prod(nall);
+    for (int i = 0; i < nall; i++) {
+        const int k = 64 - __builtin_clzll(c.mods[i]);
+        mu_prod[i] = (uint64_t)(((unsigned __int128)1 << (62 + k)) / c.mods[i]);
+    }
     size_t o_mods = blob.add(c.mods), o_muh = blob.add(mu_hi), o_mul = blob.add(mu_lo);
+    size_t o_mup = blob.add(mu_prod);
 
     // twiddles: fwd[i] = psi^brv(i); inv[i] = psi^-brv(i), inv[0] = n^-1, inv[1] *= n^-1
     std::vector<tw_t> twf((size_t)nall << c.logn), twi((size_t)nall << c.logn);
@@ -443,7 +449,7 @@ static void build_context(Context& c, const kbfv_params& prm) {
     uint8_t* base = (uint8_t*)c.pool;
     auto U = [&](size_t o) { return (const uint64_t*)(base + o); };
     auto D = [&](size_t o) { return (const double*)(base + o); };
-    dc.mods = U(o_mods); dc.mu_hi = U(o_muh); dc.mu_lo = U(o_mul);
+    dc.mods = U(o_mods); dc.mu_hi = U(o_muh); dc.mu_lo = U(o_mul); dc.mu_prod = U(o_mup);
     dc.tw_fwd = (const tw_t*)(base + o_twf); dc.tw_inv = (const tw_t*)(base + o_twi);
     dc.q2r_hatinv = U(o_q2r[0]); dc.q2r_hatinvs = U(o_q2r[1]); dc.q2r_hat = U(o_q2r[2]);
     dc.q2r_alpha = U(o_q2r[3]); dc.q2r_inv = D(o_q2r[4]);
@@ -671,13 +677,13 @@ struct QRRowsIO {
 struct TensorRow {
     const uint64_t *a1, *b1, *a2, *b2;
     int k;
-    uint64_t q, mh, ml;
+    uint64_t q, mh, ml;  // mh: barrett_prod constant (inputs are fully reduced)
     __device__ __forceinline__ uint64_t load(int j) const {
-        if (k == 0) return mul_mod(a1[j], a2[j], q, mh, ml);
-        if (k == 2) return mul_mod(b1[j], b2[j], q, mh, ml);
+        if (k == 0) return mul_mod_prod(a1[j], a2[j], q, mh);
+        if (k == 2) return mul_mod_prod(b1[j], b2[j], q, mh);
         u128 acc = mul_wide(a1[j], b2[j]);
-        mac(acc, b1[j], a2[j]);
-        return barrett128(acc, q, mh, ml);
+        mac(acc, b1[j], a2[j]);  // < 2 q^2
+        return barrett_prod(acc, q, mh);
     }
     __device__ __forceinline__ void store(int, uint64_t) const {}
 };
@@ -695,7 +701,7 @@ struct TensorSrc {
         TensorRow t;
         t.k = k;
         const int pi = l < nq ? l : dc.idx_r + (l - nq);
-        t.q = dc.mods[pi]; t.mh = dc.mu_hi[pi]; t.ml = dc.mu_lo[pi];
+        t.q = dc.mods[pi]; t.mh = dc.mu_prod[pi]; t.ml = 0;
         if (l < nq) {
             const uint64_t* A = pb.a[item];
             const uint64_t* B = pb.b[item];
@@ -717,8 +723,9 @@ struct KeyIPRow {
     const uint64_t* key;  // limb m, half h of digit 0 (digit stride ks)
     size_t ds, ks;
     int dnum;
-    uint64_t q, mh, ml;
+    uint64_t q, mh, ml, mp;
     __device__ __forceinline__ uint64_t load(int j) const {
+        if (dnum == 1) return mul_mod_prod(dig[j], key[j], q, mp);  // digits fully reduced
         u128 acc{0, 0};
         for (int d = 0; d < dnum; d++) mac(acc, dig[d * ds + j], key[d * ks + j]);
         return barrett128(acc, q, mh, ml);
@@ -742,7 +749,7 @@ struct KeyIPSrc {
         r.ds = (size_t)npq << logn;
         r.ks = (size_t)2 * dc.key_npq << logn;
         r.dnum = ndig;
-        r.q = dc.mods[m]; r.mh = dc.mu_hi[m]; r.ml = dc.mu_lo[m];
+        r.q = dc.mods[m]; r.mh = dc.mu_hi[m]; r.ml = dc.mu_lo[m]; r.mp = dc.mu_prod[m];
         return r;
     }
 };
@@ -894,8 +901,8 @@ static void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratc
     ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), count * 4 * dc.nq, st);
     // K2: Q -> R (centred)
     launch_bconv(dc, q2r_tables(dc), m.sa, m.sb, count * 4, (size_t)dc.nq << dc.logn, (size_t)dc.nr << dc.logn, st);
-    // K3: NTT over R in place (outputs in [0, 8q): the tensor reduces its products)
-    ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr),
+    // K3: NTT over R in place, fully reduced (the tensor's products use barrett_prod)
+    ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr),
                                    count * 4 * dc.nr, st);
     // K4: tensor (Q part from the NTT-form inputs, R part from K3) fused into INTT over Q|R
     TensorSrc ts{pb, m.sb, dc};
@@ -917,8 +924,8 @@ static void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb,
     const DevConsts& dc = c.dc;
     mul_front(c, pb, count, m, st);
     k5_launch(c, count, m, nullptr, 1, st);
-    // K6a: NTT over Q|P of the lifted digits, in place ([0, 8q): the key product reduces)
-    ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
+    // K6a: NTT over Q|P of the lifted digits, in place, fully reduced (key product uses barrett_prod)
+    ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                    count * dc.dnum * dc.npq, st);
     // K6b: inner product with the key fused into INTT over Q|P
     ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
@@ -954,8 +961,8 @@ static void klss_keyswitch(Context& c, const uint64_t* rlk_t, int count, const M
     klss_block_to_t_kernel<<<dim3((unsigned)(c.n / 128), (unsigned)kc.nqj, (unsigned)count), 128, 0, st>>>(
         dc, kc, m.sd2, m.st1, 0, (size_t)c.nq << c.logn, (size_t)kc.nqj * c.nt << c.logn);
     check_launch("klss_qj_to_t");
-    // NTT over T ([0, 8q): the external product reduces its sums)
-    ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.st1, dc.idx_t, c.nt), rows_io(dc, m.st1, dc.idx_t, c.nt),
+    // NTT over T
+    ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.st1, dc.idx_t, c.nt), rows_io(dc, m.st1, dc.idx_t, c.nt),
                                    count * kc.nqj * c.nt, st);
     // external product over T fused into INTT over T (external_product_T)
     ntt_inv(dc, ExtProdSrc{m.st1, rlk_t, dc, c.nt, kc.nri, kc.nqj, kc.nqj}, rows_io(dc, m.st2, dc.idx_t, c.nt),
@@ -1519,7 +1526,8 @@ struct DecSrc {
     struct Row {
         const uint64_t *a, *b, *s;
         uint64_t q, mh, ml;
-        __device__ __forceinline__ uint64_t load(int j) const { return add_mod(mul_mod(a[j], s[j], q, mh, ml), b[j], q); }
+        // a and s fully reduced: one-high-product Barrett (mh holds its constant)
+        __device__ __forceinline__ uint64_t load(int j) const { return add_mod(mul_mod_prod(a[j], s[j], q, mh), b[j], q); }
         __device__ __forceinline__ void store(int, uint64_t) const {}
     };
     __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
@@ -1530,7 +1538,7 @@ struct DecSrc {
         r.a = ct + item * 2 * lq + ((size_t)l << dc.logn);
         r.b = r.a + lq;
         r.s = sk + ((size_t)l << dc.logn);
-        r.q = dc.mods[l]; r.mh = dc.mu_hi[l]; r.ml = dc.mu_lo[l];
+        r.q = dc.mods[l]; r.mh = dc.mu_prod[l]; r.ml = 0;
         return r;
     }
 };
@@ -1637,7 +1645,7 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
             DISPATCH_MAXQ(dc.nq, L_MU);
 #undef L_MU
             check_launch("modup");
-            ntt_fwd<RowsIO, RowsIO, false>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
+            ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                            cnt * dc.dnum * dc.npq, st);
             ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
             std::vector<uint64_t*> O(cnt);
