@@ -7,8 +7,8 @@
 //
 // Shape: one CTA transforms one block of 2^LOGB points held in shared memory
 // (N = 2^14 -> 1024 threads x 16 points, 136 KiB of padded smem). Each thread
-// runs register groups of 8 (N = 2^14) or 16 points (smaller N) through 3 or 4
-// butterfly stages between shared-memory exchanges. Larger rings (2^15, 2^16)
+// runs register groups of 16 points through 4 butterfly stages between
+// shared-memory exchanges (N = 2^14: stages 4 + 4 + 4 + 2, three exchanges). Larger rings (2^15, 2^16)
 // add one elementwise radix-2/4 column pass in front of (forward) or behind
 // (inverse) the block kernels. Moduli must be below 2^60 (lazy range 8q < 2^63).
 //
@@ -65,36 +65,53 @@ __device__ __forceinline__ uint64_t reduce_from(uint64_t v, uint64_t q, int log_
 }
 
 // R forward stages on 2^R registers; stage s0+u uses psi_br[2^(s0+u) + (hi << u) + h].
+// Stage and butterfly loops are expanded by template recursion so that every
+// register index is a compile-time constant.
+template <int R, int U, int H>
+__device__ __forceinline__ void fwd_stage_h(uint64_t* x, const tw_t* __restrict__ tw, int bidx, uint64_t q,
+                                            uint64_t q4) {
+    if constexpr (H < (1 << U)) {
+        constexpr int half = 1 << (R - 1 - U);
+        const tw_t w = tw[bidx + H];
+#pragma unroll
+        for (int k = 0; k < half; k++) ct_bfly(x[H * 2 * half + k], x[H * 2 * half + k + half], w, q, q4);
+        fwd_stage_h<R, U, H + 1>(x, tw, bidx, q, q4);
+    }
+}
+template <int R, int U>
+__device__ __forceinline__ void fwd_stages(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi, uint64_t q,
+                                           uint64_t q4) {
+    if constexpr (U < R) {
+        fwd_stage_h<R, U, 0>(x, tw, (1 << (s0 + U)) + (hi << U), q, q4);
+        fwd_stages<R, U + 1>(x, tw, s0, hi, q, q4);
+    }
+}
 template <int R>
 __device__ __forceinline__ void fwd_group(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi,
                                           uint64_t q, uint64_t q4) {
-#pragma unroll
-    for (int u = 0; u < R; u++) {
-        const int half = 1 << (R - 1 - u);
-        const int bidx = (1 << (s0 + u)) + (hi << u);
-#pragma unroll
-        for (int h = 0; h < (1 << u); h++) {
-            const tw_t w = tw[bidx + h];
-#pragma unroll
-            for (int k = 0; k < half; k++) {
-                const int i0 = h * 2 * half + k;
-                ct_bfly(x[i0], x[i0 + half], w, q, q4);
-            }
-        }
-    }
+    fwd_stages<R, 0>(x, tw, s0, hi, q, q4);
 }
 
 // R inverse stages (reverse order). `fold` (only with s0 == 0, hi == 0) applies
 // n^-1 at global stage 0 using tw[0] = n^-1, tw[1] = psi_br^-1[1] * n^-1 and
 // fully reduces.
-template <int R>
-__device__ __forceinline__ void inv_group(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi,
-                                          uint64_t q, uint64_t q4, bool fold) {
+template <int R, int U, int H>
+__device__ __forceinline__ void inv_stage_h(uint64_t* x, const tw_t* __restrict__ tw, int bidx, uint64_t q,
+                                            uint64_t q4) {
+    if constexpr (H < (1 << U)) {
+        constexpr int half = 1 << (R - 1 - U);
+        const tw_t w = tw[bidx + H];
 #pragma unroll
-    for (int u = R - 1; u >= 0; u--) {
-        const int half = 1 << (R - 1 - u);
-        const int bidx = (1 << (s0 + u)) + (hi << u);
-        if (fold && u == 0) {
+        for (int k = 0; k < half; k++) gs_bfly(x[H * 2 * half + k], x[H * 2 * half + k + half], w, q, q4);
+        inv_stage_h<R, U, H + 1>(x, tw, bidx, q, q4);
+    }
+}
+template <int R, int U>
+__device__ __forceinline__ void inv_stages(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi, uint64_t q,
+                                           uint64_t q4, bool fold) {
+    if constexpr (U >= 0) {
+        constexpr int half = 1 << (R - 1 - U);
+        if (U == 0 && fold) {
             const tw_t ni = tw[0];
             const tw_t w1 = tw[1];
 #pragma unroll
@@ -104,17 +121,15 @@ __device__ __forceinline__ void inv_group(uint64_t* x, const tw_t* __restrict__ 
                 x[k + half] = reduce_from(shoup4(a + q4 - b, w1.x, w1.y, q), q, 2);
             }
         } else {
-#pragma unroll
-            for (int h = 0; h < (1 << u); h++) {
-                const tw_t w = tw[bidx + h];
-#pragma unroll
-                for (int k = 0; k < half; k++) {
-                    const int i0 = h * 2 * half + k;
-                    gs_bfly(x[i0], x[i0 + half], w, q, q4);
-                }
-            }
+            inv_stage_h<R, U, 0>(x, tw, (1 << (s0 + U)) + (hi << U), q, q4);
         }
+        inv_stages<R, U - 1>(x, tw, s0, hi, q, q4, fold);
     }
+}
+template <int R>
+__device__ __forceinline__ void inv_group(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi,
+                                          uint64_t q, uint64_t q4, bool fold) {
+    inv_stages<R, R - 1>(x, tw, s0, hi, q, q4, fold);
 }
 
 // ---------------------------------------------------------------------------
@@ -133,8 +148,9 @@ struct BlockShape {
     static constexpr int NB = 1 << LOGB;
     static constexpr int THREADS = NB / 16;
     static constexpr int SMEM_BYTES = (NB + NB / 16) * 8;
-    // radix of the register groups: 8 points at 1024 threads (64 registers), else 16
-    static constexpr int RAD = LOGB >= 14 ? 3 : 4;
+    // radix of the register groups: 16 points (the template-expanded groups keep
+    // a 1024-thread block within 64 registers)
+    static constexpr int RAD = 4;
 };
 
 struct PassCtx {
