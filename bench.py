@@ -454,14 +454,14 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     bfly = rows * (N // 2) * LOG_N
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of this launch at
     # 2048 rows, from one ncu capture of `bench.py --kernel ntt16k --rows 2048`
-    traffic = 270467840 + 220812032 if rows == 2048 else None
+    traffic = 270470912 + 208796416 if rows == 2048 else None
     res["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                        "frac": round(ach / peak, 4), "traffic": traffic,
                        "kernel": f"ntt_fwd_block_kernel<14> on {rows} rows ({peak_kind} peak)",
                        "ms_per_launch": round(ms_ntt, 4),
                        "algorithmic_bytes": alg,
                        "note": "60-bit Shoup butterflies are bound by the IMAD pipe, not HBM: ncu shows "
-                               "fmaheavy busy ~65% of elapsed with math-pipe throttling the top stall",
+                               "fmaheavy busy ~66% of elapsed with math-pipe throttling the top stall",
                        "butterflies_per_s": round(bfly / (ms_ntt / 1e3), 0)}
     del x
 
