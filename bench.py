@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--skip-extras", action="store_true", help="only the headline workload")
-    ap.add_argument("--kernel", default=None, choices=["ntt16k", "ntt16k_inv", "pipeline1"],
+    ap.add_argument("--kernel", default=None, choices=["ntt16k", "ntt16k_inv", "pipeline1", "arith"],
                     help="run one kernel on a profiling-sized case and exit (for ncu)")
     ap.add_argument("--rows", type=int, default=1024, help="rows for the ntt16k profiling cases")
     ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
@@ -58,10 +58,15 @@ def parse():
 
 def run_kernel_case(args):
     """Profiling cases: the forward / inverse NTT block kernel on --rows rows of
-    N=16384 (1024 rows = 128 MiB, above L2), or batched multiplies of --pairs pairs."""
+    N=16384 (1024 rows = 128 MiB, above L2), batched multiplies of --pairs pairs,
+    or the arithmetic-rate probe of the 64-bit modular primitives."""
     import torch
 
     import kunpbfv_b200 as kb
+    if args.kernel == "arith":
+        from kunpbfv_b200.api import PROBE_KINDS, probe_arith
+        print(json.dumps({name: round(probe_arith(k), 1) for k, name in enumerate(PROBE_KINDS)}))
+        return
     qs, ps = c3_primes()
     ctx = kb.BFVContext(log_n=LOG_N, plain_modulus=T, q_count=NQ, q=qs, p_count=NP, p=ps, dnum=1)
     if args.kernel.startswith("ntt16k"):

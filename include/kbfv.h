@@ -75,6 +75,12 @@ int kbfv_params_destroy(kbfv_params* params);
 
 const char* kbfv_last_error(void);
 const char* kbfv_version(void);
+/* Throughput of one 64-bit modular primitive on the current device (Gop/s):
+ * independent register chains, no memory traffic. kind 0: 64x64->128
+ * multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64, 3: forward NTT butterfly,
+ * 4: Shoup product, 5: 128-bit Barrett, 6: one-high-product Barrett,
+ * 7: 32x32->64 multiply-add. The roofline of the IMAD-bound kernels. */
+int kbfv_probe_arith(int kind, uint32_t iters, double* gops);
 
 /* ---- context ---------------------------------------------------------
  * BFVContext::BFVContext(size_t N) (include/BFVcontext.cuh:13-101):
@@ -221,6 +227,24 @@ int kbfv_relinearize_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t lo
                             uint64_t* d_ct, uint32_t count, kbfv_stream stream);
 int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_base, const uint64_t* d_ct_a,
                           const uint64_t* d_ct_b, uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
+/* ---- Galois automorphisms: rotations and conjugation ---------------------
+ * BFVScheme::addLeftRotKey_23 / leftRotateAndEqual_23 / rightRotateAndEqual_23 /
+ * addConjKey_23 (include/KeySwitch_23.cuh:71-166, 544-584): the automorphism
+ * X -> X^g (g = 5^r mod 2N for a left rotation by r, the reference's rotGroups,
+ * include/BFVcontext.cuh:788-799; g = 2N - 1 for conjugation) followed by a key
+ * switch from s(X^g) back to s. In NTT form the automorphism is a permutation
+ * of the evaluation points. The key (layout of the relinearisation key) encrypts
+ * P * s(X^g) per digit. The reference applies the coefficient-domain automorphism
+ * to its NTT-form secret key when it builds rotation keys (KeySwitch_23.cuh:133),
+ * so its rotations do not decrypt; these do.
+ * kbfv_galois_element: 5^rot_slots mod 2N, or 2N - 1 for rot_slots < 0. */
+uint64_t kbfv_galois_element(const kbfv_context* ctx, int64_t rot_slots);
+int kbfv_keygen_galois(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint64_t galois_elt,
+                       uint64_t* d_gk, kbfv_stream stream);
+/* out = key_switch(automorphism(ct)); out may equal ct */
+int kbfv_apply_galois(kbfv_context* ctx, const uint64_t* d_gk, uint64_t galois_elt, const uint64_t* d_ct,
+                      uint64_t* d_out, uint32_t count, kbfv_stream stream);
 
 /* ---- levels: fewer live ciphertext primes --------------------------------
  * A ciphertext at level l holds the first l primes of Q (2 x l limbs, NTT form).

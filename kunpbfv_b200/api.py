@@ -132,6 +132,10 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_ntt_inv_batch": (I, [VP, C.POINTER(VP), u32, u32, u32, VP]),
         "kbfv_add_plain": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_context_at_level": (I, [VP, u32, C.POINTER(VP)]),
+        "kbfv_probe_arith": (I, [I, u32, C.POINTER(C.c_double)]),
+        "kbfv_galois_element": (u64, [VP, C.c_int64]),
+        "kbfv_keygen_galois": (I, [VP, U8P, VP, u64, VP, VP]),
+        "kbfv_apply_galois": (I, [VP, VP, u64, VP, VP, u32, VP]),
         "kbfv_keygen_relin_gadget": (I, [VP, U8P, VP, u32, VP, VP]),
         "kbfv_relinearize_gadget": (I, [VP, VP, u32, VP, VP, u32, VP]),
         "kbfv_mul_relin_gadget": (I, [VP, VP, u32, VP, VP, VP, u32, VP]),
@@ -517,6 +521,7 @@ class BFVScheme:
             raise ValueError("relin must be 'hybrid', 'klss' or 'gadget'")
         self.gadget_log_base = gadget_log_base
         self.gk = None
+        self.galois_keys = {}  # Galois element -> key (rotKey_vec_23 / ConjKey_23)
         self.context = ctx
         self.seed = bytes(seed)
         self.relin = relin
@@ -648,6 +653,43 @@ class BFVScheme:
         O = (VP * n)(*out_ptrs)
         _check(lib().kbfv_mul_relin_batch(self.context.handle, _ptr(self.rlk), A, B, O, n, _stream_ptr(stream)))
 
+    # ---- rotations and conjugation (Galois automorphisms)
+    def galois_element(self, rot_slots: int) -> int:
+        return int(lib().kbfv_galois_element(self.context.handle, rot_slots))
+
+    def addGaloisKey(self, sk: SecretKey, g: int, stream=None):
+        if g in self.galois_keys:
+            return
+        ctx = self.context
+        key = ctx.zeros(ctx.dnum, 2, ctx.q_count + ctx.p_count, ctx.N)
+        _check(lib().kbfv_keygen_galois(ctx.handle, _u8(self.seed), _ptr(sk.sx_device), g, _ptr(key),
+                                        _stream_ptr(stream)))
+        self.galois_keys[g] = key
+
+    def addLeftRotKey_23(self, sk: SecretKey, rot_num: int, stream=None):
+        self.addGaloisKey(sk, self.galois_element(rot_num), stream)
+
+    def addConjKey_23(self, sk: SecretKey, stream=None):
+        self.addGaloisKey(sk, 2 * self.context.N - 1, stream)
+
+    def apply_galois(self, ct: Ciphertext, g: int, out: Optional[Ciphertext] = None, stream=None) -> Ciphertext:
+        if g not in self.galois_keys:
+            raise KbfvError(-5, "rotKey_23 not exists")
+        out = out if out is not None else Ciphertext(ct.ctx, count=ct.count)
+        _check(lib().kbfv_apply_galois(ct.ctx.handle, _ptr(self.galois_keys[g]), g, _ptr(ct.cipher_device),
+                                       _ptr(out.cipher_device), ct.count, _stream_ptr(stream)))
+        return out
+
+    def leftRotateAndEqual_23(self, ct: Ciphertext, rot_slots: int, stream=None):
+        self.apply_galois(ct, self.galois_element(rot_slots), out=ct, stream=stream)
+
+    def rightRotateAndEqual_23(self, ct: Ciphertext, rot_slots: int, stream=None):
+        """the reference's conversion: a left rotation by N/2 - 2^rot_slots (KeySwitch_23.cuh:580-584)"""
+        self.leftRotateAndEqual_23(ct, self.context.N // 2 - (1 << rot_slots), stream)
+
+    def conjugate_23(self, ct: Ciphertext, stream=None):
+        self.apply_galois(ct, 2 * self.context.N - 1, out=ct, stream=stream)
+
     def mod_switch(self, ct: Ciphertext, stream=None) -> Ciphertext:
         """drop the last live prime (divide and round); the result lives at ct.ctx's level - 1"""
         top = ct.ctx._owner or ct.ctx
@@ -680,6 +722,17 @@ class BFVScheme:
         v = C.c_double()
         _check(lib().kbfv_noise_budget(ct.ctx.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), C.byref(v)))
         return float(v.value)
+
+
+PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64", "forward NTT butterfly",
+               "Shoup product", "128-bit Barrett", "one-high-product Barrett", "32x32->64 multiply-add"]
+
+
+def probe_arith(kind: int, iters: int = 4096) -> float:
+    """Gop/s of one modular primitive on the current GPU (kbfv_probe_arith)."""
+    v = C.c_double()
+    _check(lib().kbfv_probe_arith(kind, iters, C.byref(v)))
+    return float(v.value)
 
 
 def salsa20_stream(key: bytes, nonce: bytes, nbytes: int, block0: int = 0, compat: bool = False, stream=None):

@@ -1045,9 +1045,68 @@ __global__ void mod_switch_combine_kernel(DevConsts c, const uint64_t* __restric
     out[i] = shoup(x + q - corr[i], c.ms_qlinv[l], c.ms_qlinvs[l], q);
 }
 
+// rows (item, l) of the a-part of ciphertexts, read through the Galois permutation
+struct GaloisRow {
+    const uint64_t* p;
+    uint64_t g;
+    int logn;
+    __device__ __forceinline__ uint64_t load(int j) const { return p[galois_perm((uint32_t)j, g, logn)]; }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct GaloisASrc {
+    const uint64_t* ct;  // [item][a|b][nq]
+    uint64_t g;
+    int logn, nq;
+    __device__ __forceinline__ int prime(int row) const { return row % nq; }
+    __device__ __forceinline__ GaloisRow bind(int row) const {
+        const int item = row / nq, l = row % nq;
+        return GaloisRow{ct + (((size_t)item * 2 * nq + l) << logn), g, logn};
+    }
+};
+
 static void require_klss(const Context& c) {
     KB_REQUIRE(c.klss_ok, KBFV_ERR_INVALID,
                "context has no T-base key switch (needs T primes, q_count divisible by p_count, dnum = q_count / p_count)");
+}
+
+// ---- arithmetic-rate probe: independent register chains of one primitive -------
+// kind 0: 64x64->128 multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64,
+// 3: forward butterfly (approximate-quotient Shoup), 4: fully reduced Shoup,
+// 5: 128-bit Barrett, 6: one-high-product Barrett, 7: 32x32->64 multiply-add.
+constexpr int kProbeChains = 8;
+template <int KIND>
+__global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_t mh, uint64_t ml, uint64_t mp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t a[kProbeChains], b[kProbeChains];
+    u128 acc[kProbeChains];
+#pragma unroll
+    for (int c = 0; c < kProbeChains; c++) {
+        a[c] = (0x9E3779B97F4A7C15ULL * (uint64_t)(t * kProbeChains + c + 1)) % q;
+        b[c] = (0xC2B2AE3D27D4EB4FULL * (uint64_t)(t * kProbeChains + c + 7)) % q;
+        acc[c] = u128{0, 0};
+    }
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int c = 0; c < kProbeChains; c++) {
+            if (KIND == 0) mac(acc[c], a[c], b[c]);
+            if (KIND == 1) acc[c].lo += a[c] * b[c];
+            if (KIND == 2) acc[c].lo += __umul64hi(a[c], b[c]);
+            if (KIND == 3) {
+                uint64_t x = a[c], y = b[c];
+                ct_bfly(x, y, tw_t{b[c], a[c]}, q, q << 2);
+                acc[c].lo += x ^ y;
+            }
+            if (KIND == 4) acc[c].lo += shoup(a[c], b[c], a[c] ^ b[c], q);
+            if (KIND == 5) acc[c].lo += barrett128(u128{a[c], b[c] >> 4}, q, mh, ml);
+            if (KIND == 6) acc[c].lo += barrett_prod(mul_wide(a[c], b[c]), q, mp);
+            if (KIND == 7) acc[c].lo += (uint64_t)(uint32_t)a[c] * (uint32_t)b[c];
+            a[c] = (a[c] + (acc[c].lo & 15)) & 0x0fffffffffffffffULL;
+        }
+    }
+    uint64_t r = 0;
+#pragma unroll
+    for (int c = 0; c < kProbeChains; c++) r ^= acc[c].lo ^ acc[c].hi ^ a[c];
+    out[t] = r;
 }
 
 // ===========================================================================
@@ -1318,7 +1377,7 @@ static void hsalsa_host(const uint8_t key[32], const uint8_t nonce16[16], uint32
 }
 
 enum { DOM_SK = 1, DOM_PK_A = 2, DOM_PK_E = 3, DOM_RLK_A = 4, DOM_RLK_E = 5, DOM_ENC_V = 6, DOM_ENC_E0 = 7,
-       DOM_ENC_E1 = 8, DOM_GK_A = 9, DOM_GK_E = 10 };
+       DOM_ENC_E1 = 8, DOM_GK_A = 9, DOM_GK_E = 10, DOM_GAL_A = 11, DOM_GAL_E = 12 };
 
 static void sample_small(Context& c, const uint8_t seed[32], uint32_t domain, uint64_t id0, int kind, int prime0,
                          int limbs, uint64_t* out, size_t item_stride, int items, cudaStream_t st) {
@@ -2159,6 +2218,129 @@ int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_
             k5_launch(c, cnt, m, nullptr, 2, st);
             gadget_keyswitch(c, d_gk, w, cnt, m, sg, st);
             ntt_fwd(c.dc, ModDownAddSrc{m.se, m.sd, c.dc}, OutCtDst{pb, c.dc.logn, c.dc.nq}, cnt * 2 * c.dc.nq, st);
+        }
+    });
+}
+
+
+int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
+    return guarded([&] {
+        KB_REQUIRE(kind >= 0 && kind <= 7 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
+        int dev = 0, sms = 0;
+        KB_CHECK_CUDA(cudaGetDevice(&dev));
+        KB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const unsigned blocks = (unsigned)sms * 8, threads = 256;
+        uint64_t* out = nullptr;
+        KB_CHECK_CUDA(cudaMalloc(&out, (size_t)blocks * threads * 8));
+        const uint64_t q = 1152921504606584833ULL;  // 60-bit
+        uint64_t mh, ml;
+        H::barrett_mu(q, mh, ml);
+        const uint64_t mp = (uint64_t)(((unsigned __int128)1 << 122) / q);
+        cudaEvent_t e0, e1;
+        KB_CHECK_CUDA(cudaEventCreate(&e0));
+        KB_CHECK_CUDA(cudaEventCreate(&e1));
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; rep++) {  // the first launch warms up
+            KB_CHECK_CUDA(cudaEventRecord(e0));
+            switch (kind) {
+#define P_K(K) case K: probe_arith_kernel<K><<<blocks, threads>>>(out, (int)iters, q, mh, ml, mp); break;
+                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7)
+#undef P_K
+            }
+            KB_CHECK_CUDA(cudaEventRecord(e1));
+            KB_CHECK_CUDA(cudaEventSynchronize(e1));
+        }
+        KB_CHECK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(out);
+        check_launch("probe_arith");
+        *gops = (double)blocks * threads * iters * kProbeChains / (ms * 1e6);
+    });
+}
+
+
+// ---- Galois automorphisms (rotations, conjugation) ---------------------------
+uint64_t kbfv_galois_element(const kbfv_context* ctx, int64_t rot_slots) {
+    if (!ctx) return 0;
+    const Context& c = const_cast<kbfv_context*>(ctx)->c;
+    const uint64_t m = 2 * c.n;
+    if (rot_slots < 0) return m - 1;  // conjugation
+    uint64_t g = 1;
+    for (int64_t i = 0; i < rot_slots; i++) g = g * 5 % m;
+    return g;
+}
+
+int kbfv_keygen_galois(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* d_sk, uint64_t galois_elt,
+                       uint64_t* d_gk, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_top(c);
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(d_sk && d_gk, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE((galois_elt & 1) && galois_elt < 2 * c.n, KBFV_ERR_INVALID, "Galois element must be odd and below 2N");
+        cudaStream_t st = S(stream);
+        const int npq = c.nq + c.np;
+        const size_t lpq = (size_t)npq * c.n;
+        uint64_t* sg = (uint64_t*)ensure_scratch(c, lpq * 8);
+        galois_ntt_kernel<<<blocks_for(lpq, 256), 256, 0, st>>>(c.dc, d_sk, sg, galois_elt, lpq);
+        check_launch("galois_sk");
+        for (int d = 0; d < c.dnum; d++) {
+            uint64_t* a = d_gk + (size_t)d * 2 * lpq;
+            uint64_t* b = a + lpq;
+            sample_uniform(c, seed, DOM_GAL_A, (uint32_t)d, galois_elt, 0, npq, a, 0, 1, st);
+            SalsaKey k = subkey_for(seed, DOM_GAL_E, (uint32_t)d);
+            sample_small_kernel<1><<<blocks_for(c.n / 8, 128), 128, 0, st>>>(c.dc, k, galois_elt, 0, npq, b, 0, 1);
+            check_launch("sample_gauss");
+            RowsIO io = rows_io(c.dc, b, 0, npq);
+            ntt_fwd(c.dc, io, io, npq, st);
+            ksk_combine_kernel<<<blocks_for(lpq, 256), 256, 0, st>>>(c.dc, a, d_sk, sg, b, d, lpq);
+            check_launch("ksk_combine");
+        }
+    });
+}
+
+int kbfv_apply_galois(kbfv_context* ctx, const uint64_t* d_gk, uint64_t galois_elt, const uint64_t* d_ct,
+                      uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_gk, KBFV_ERR_NO_KEY, "Galois key missing");
+        KB_REQUIRE(d_ct && d_out, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE((galois_elt & 1) && galois_elt < 2 * c.n, KBFV_ERR_INVALID, "Galois element must be odd and below 2N");
+        cudaStream_t st = S(stream);
+        const DevConsts& dc = c.dc;
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+            MulScratch m = mul_scratch_layout(c, cnt, base);
+            const uint64_t* in = d_ct + (size_t)off * 2 * lq;
+            uint64_t* out = d_out + (size_t)off * 2 * lq;
+            // g(b) first (the output may overwrite the input): sb holds [item][nq]
+            for (int i = 0; i < cnt; i++)
+                galois_ntt_kernel<<<blocks_for(lq, 256), 256, 0, st>>>(dc, in + (size_t)i * 2 * lq + lq,
+                                                                        m.sb + (size_t)i * lq, galois_elt, lq);
+            check_launch("galois_b");
+            // g(a) read through the permutation by the inverse NTT, then the hybrid key switch
+            ntt_inv(dc, GaloisASrc{in, galois_elt, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), cnt * dc.nq, st);
+            dim3 grid((unsigned)(c.n / 128), (unsigned)cnt);
+#define L_MU(M) modup_kernel<M><<<grid, 128, 0, st>>>(dc, m.sa, m.sd2)
+            DISPATCH_MAXQ(dc.nq, L_MU);
+#undef L_MU
+            check_launch("modup");
+            ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
+                                          cnt * dc.dnum * dc.npq, st);
+            ntt_inv(dc, KeyIPSrc{m.sd2, d_gk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
+            std::vector<uint64_t*> O(cnt);
+            std::vector<const uint64_t*> Z(cnt);
+            for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
+            PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
+            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            for (int i = 0; i < cnt; i++)
+                add_kernel<<<blocks_for(lq, 256), 256, 0, st>>>(dc, out + (size_t)i * 2 * lq + lq, m.sb + (size_t)i * lq,
+                                                                out + (size_t)i * 2 * lq + lq, lq, dc.nq);
+            check_launch("galois_add");
         }
     });
 }

@@ -514,6 +514,37 @@ __global__ void gk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, c
     eb[i] = v;
 }
 
+// Galois automorphism X -> X^g in NTT form: index i holds A(psi^(2 brv(i) + 1)),
+// so the automorphism reads index perm(i) with 2 brv(perm(i)) + 1 = (2 brv(i) + 1) g mod 2N.
+__device__ __forceinline__ uint32_t galois_perm(uint32_t i, uint64_t g, int logn) {
+    const uint32_t bi = __brev(i) >> (32 - logn);
+    const uint64_t e = ((2 * (uint64_t)bi + 1) * g) & ((2ULL << logn) - 1);
+    return __brev((uint32_t)(e >> 1)) >> (32 - logn);
+}
+// out[poly][l][i] = in[poly][l][perm(i)]  (polys x limbs rows of N; out != in)
+__global__ void galois_ntt_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                  uint64_t g, size_t total) {
+    const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= total) return;
+    const size_t row = x >> c.logn;
+    const uint32_t i = (uint32_t)(x & (((size_t)1 << c.logn) - 1));
+    out[x] = in[(row << c.logn) + galois_perm(i, g, c.logn)];
+}
+// key-switch key component for a target polynomial t (NTT form over Q|P):
+// b = e - a*s + [l in digit] * P * t
+__global__ void ksk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
+                                   const uint64_t* __restrict__ target, uint64_t* __restrict__ eb, int digit,
+                                   size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int l = (int)(i >> c.logn);
+    const uint64_t q = c.mods[l], mh = c.mu_hi[l], ml = c.mu_lo[l];
+    uint64_t v = sub_mod(eb[i], mul_mod(a[i], s[i], q, mh, ml), q);
+    const int lo = digit * c.alpha, hi = min(lo + c.alpha, c.nq);
+    if (l >= lo && l < hi) v = add_mod(v, mul_mod(target[i], c.p_mod_q[l], q, mh, ml), q);
+    eb[i] = v;
+}
+
 // encrypt: a = v*pk.a + e0, b = v*pk.b + e1 + dm (encryptZero/encryptMsg,
 // include/BFVScheme.cuh:87-146). work: items x [v | e0 | e1 | dm] x nq (NTT form)
 __global__ void enc_combine_kernel(DevConsts c, const uint64_t* __restrict__ pk, const uint64_t* __restrict__ work,

@@ -59,6 +59,9 @@ def _declare(L: C.CDLL) -> None:
         "orc_klss_relinearize": (V, [C.c_void_p, U64P, U64P, U64P]),
         "orc_mod_switch": (V, [C.c_void_p, U64P, U64P, C.c_int]),
         "orc_gadget_pieces": (C.c_int, [C.c_int]),
+        "orc_galois_ntt": (V, [C.c_void_p, C.c_uint64, U64P, U64P, C.c_int]),
+        "orc_keygen_galois": (V, [C.c_void_p, U8P, U64P, C.c_uint64, U64P]),
+        "orc_apply_galois": (V, [C.c_void_p, U64P, C.c_uint64, U64P, U64P]),
         "orc_keygen_relin_gadget": (V, [C.c_void_p, U8P, U64P, C.c_int, U64P]),
         "orc_relinearize_gadget": (V, [C.c_void_p, U64P, U64P, C.c_int, U64P]),
         "orc_prime_count": (C.c_int, [C.c_void_p]),
@@ -291,6 +294,25 @@ class Oracle:
         gk = np.ascontiguousarray(gk, dtype=np.uint64)
         out = np.zeros((2, self.nq, self.n), dtype=np.uint64)
         lib().orc_relinearize_gadget(self._h, _p(d), _p(gk), w, _p(out))
+        return out
+
+    def galois_ntt(self, g: int, x):
+        x = np.ascontiguousarray(x, dtype=np.uint64)
+        out = np.zeros_like(x)
+        lib().orc_galois_ntt(self._h, g, _p(x), _p(out), x.size // self.n)
+        return out
+
+    def keygen_galois(self, key, sk, g: int):
+        out = np.zeros((self.dnum, 2, self.nq + self.np_, self.n), dtype=np.uint64)
+        sk = np.ascontiguousarray(sk, dtype=np.uint64)
+        lib().orc_keygen_galois(self._h, _p(_key(key)), _p(sk), g, _p(out))
+        return out
+
+    def apply_galois(self, gk, g: int, ct):
+        gk = np.ascontiguousarray(gk, dtype=np.uint64)
+        ct = np.ascontiguousarray(ct, dtype=np.uint64)
+        out = np.zeros((2, self.nq, self.n), dtype=np.uint64)
+        lib().orc_apply_galois(self._h, _p(gk), g, _p(ct), _p(out))
         return out
 
     def mod_switch(self, ct, npoly: int = 2):

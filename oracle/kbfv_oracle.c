@@ -1148,7 +1148,7 @@ void orc_sample_hwt(const orc_ctx* c, const uint8_t key[32], uint32_t domain, ui
 /* scheme                                                                  */
 /* ======================================================================= */
 enum { DOM_SK = 1, DOM_PK_A = 2, DOM_PK_E = 3, DOM_RLK_A = 4, DOM_RLK_E = 5,
-       DOM_ENC_V = 6, DOM_ENC_E0 = 7, DOM_ENC_E1 = 8, DOM_GK_A = 9, DOM_GK_E = 10 };
+       DOM_ENC_V = 6, DOM_ENC_E0 = 7, DOM_ENC_E1 = 8, DOM_GK_A = 9, DOM_GK_E = 10, DOM_GAL_A = 11, DOM_GAL_E = 12 };
 
 static void small_to_rns(const orc_ctx* c, const int64_t* s, int p0, int nl, u64* out) {
     for (int l = 0; l < nl; l++) {
@@ -1442,6 +1442,73 @@ void orc_relinearize_gadget(const orc_ctx* c, const u64* d, const u64* gk, int w
         ct[lq + x] = addmod(d[2 * lq + x], dn[lq + x], q);
     }
     free(d2); free(z); free(acc); free(dn);
+}
+
+/* ---- Galois automorphisms X -> X^g (g odd mod 2N) -------------------------
+ * In NTT form an automorphism permutes the evaluation points: index i holds
+ * A(psi^e_i), e_i = 2 brv(i) + 1, and (A o X^g)(psi^e) = A(psi^(e g)), so
+ * out[i] = in[j] with e_j = e_i * g mod 2N, the same for every prime.
+ * Rotations use g = 5^r mod 2N (the reference's rotGroups, BFVcontext.cuh:788-799),
+ * conjugation g = 2N - 1. */
+static u64 brv_bits(u64 x, int bits) {
+    u64 r = 0;
+    for (int b = 0; b < bits; b++) { r = (r << 1) | (x & 1); x >>= 1; }
+    return r;
+}
+void orc_galois_ntt(const orc_ctx* c, u64 g, const u64* in, u64* out, int nlimbs) {
+    u64 n = c->n, m = 2 * n;
+    int logn = (int)c->logn;
+    u64* perm = malloc(n * 8);
+    for (u64 i = 0; i < n; i++) {
+        u64 e = (2 * brv_bits(i, logn) + 1) * (g % m) % m;
+        perm[i] = brv_bits((e - 1) / 2, logn);
+    }
+    for (int l = 0; l < nlimbs; l++)
+        for (u64 i = 0; i < n; i++) out[(size_t)l * n + i] = in[(size_t)l * n + perm[i]];
+    free(perm);
+}
+
+/* key switching key from s(X^g) to s: digit d: a uniform, b = e - a s + P * [l in digit d] * s(X^g),
+ * layout as the relinearisation key; randomness keyed by (DOM_GAL_*, id = g, sub = d) */
+void orc_keygen_galois(const orc_ctx* c, const uint8_t key[32], const u64* sk, u64 g, u64* gk) {
+    u64 n = c->n;
+    int nq = c->nq, np = c->np, npq = nq + np;
+    int idx[128];
+    for (int i = 0; i < npq; i++) idx[i] = i;
+    u64* sg = malloc((size_t)npq * n * 8);
+    orc_galois_ntt(c, g, sk, sg, npq);
+    int64_t* e = malloc(n * sizeof(int64_t));
+    for (int d = 0; d < c->dnum; d++) {
+        int lo = d * c->alpha, hi = lo + c->alpha; if (hi > nq) hi = nq;
+        u64* a = gk + (size_t)d * 2 * npq * n;
+        u64* b = a + (size_t)npq * n;
+        orc_sample_uniform(c, key, DOM_GAL_A, g, (uint32_t)d, idx, npq, a);
+        orc_sample_gaussian(c, key, DOM_GAL_E, g, (uint32_t)d, e);
+        small_to_rns(c, e, 0, npq, b);
+        ntt_fwd_limbs(c, 0, b, npq);
+        for (int l = 0; l < npq; l++) {
+            u64 q = c->mods[l];
+            for (u64 k = 0; k < n; k++) {
+                size_t id = (size_t)l * n + k;
+                u64 v = submod(b[id], mulmod(a[id], sk[id], q), q);
+                if (l >= lo && l < hi) v = addmod(v, mulmod(sg[id], c->p_mod_q[l], q), q);
+                b[id] = v;
+            }
+        }
+    }
+    free(e); free(sg);
+}
+
+/* ct (2 x nq, NTT) -> automorphism then key switch back to s: key switch of
+ * [g(a) | 0 | g(b)] as a tensor (leftRotateAndEqual_23, KeySwitch_23.cuh:544-578,
+ * restated with the automorphism applied before the key switch) */
+void orc_apply_galois(const orc_ctx* c, const u64* gk, u64 g, const u64* ct, u64* out) {
+    size_t lq = (size_t)c->nq * c->n;
+    u64* t = calloc(3 * lq, 8);
+    orc_galois_ntt(c, g, ct, t, c->nq);
+    orc_galois_ntt(c, g, ct + lq, t + 2 * lq, c->nq);
+    orc_relinearize(c, t, gk, out);
+    free(t);
 }
 
 void orc_mul_relin(const orc_ctx* c, const u64* ct1, const u64* ct2, const u64* rlk, u64* ct) {

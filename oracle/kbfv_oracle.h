@@ -75,6 +75,11 @@ void orc_moddown(const orc_ctx* c, const uint64_t* in, uint64_t* out, int npoly)
 int  orc_gadget_pieces(int w);
 void orc_keygen_relin_gadget(const orc_ctx* c, const uint8_t key[32], const uint64_t* sk, int w, uint64_t* gk);
 void orc_relinearize_gadget(const orc_ctx* c, const uint64_t* d, const uint64_t* gk, int w, uint64_t* ct);
+/* Galois automorphism X -> X^g on NTT-form limbs; key switching key from s(X^g)
+ * to s (layout of the relinearisation key); automorphism + key switch of a ciphertext */
+void orc_galois_ntt(const orc_ctx* c, uint64_t g, const uint64_t* in, uint64_t* out, int nlimbs);
+void orc_keygen_galois(const orc_ctx* c, const uint8_t key[32], const uint64_t* sk, uint64_t g, uint64_t* gk);
+void orc_apply_galois(const orc_ctx* c, const uint64_t* gk, uint64_t g, const uint64_t* ct, uint64_t* out);
 /* BFV modulus switch by the last prime: npoly polys of nq limbs (NTT) -> nq - 1 limbs */
 void orc_mod_switch(const orc_ctx* c, const uint64_t* ct, uint64_t* out, int npoly);
 /* KLSS restatement (reference's own key-switch base conversions) */

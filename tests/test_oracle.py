@@ -388,6 +388,41 @@ def test_gadget_key_switch(oracle_mod):
     assert np.array_equal(o.decode(o.decrypt(skl, res)), (v1 * v2) % T65537)
 
 
+def test_galois_automorphisms(oracle_mod):
+    """Automorphism X -> X^g in NTT form + key switch decrypts to m(X^g) for
+    rotations (g = 5^r) and conjugation (g = 2N - 1); the NTT-form permutation
+    equals the coefficient-form automorphism."""
+    qs, ps = small_primes(12, 3, 1, 50)
+    o = oracle_mod.Oracle(12, T65537, qs, ps)
+    n = o.n
+    key = b"\x05" * 32
+    sk = o.keygen_secret(key)
+    pk = o.keygen_public(key, sk)
+    rng = np.random.default_rng(0)
+    m = o.encode(rng.integers(0, T65537, size=n, dtype=np.uint64))
+    ct = o.encrypt(key, 1, pk, m)
+
+    def auto(poly, g, mod):
+        out = np.zeros(n, dtype=object)
+        for i in range(n):
+            e = (i * g) % (2 * n)
+            if e < n:
+                out[e] = (out[e] + int(poly[i])) % mod
+            else:
+                out[e - n] = (out[e - n] - int(poly[i])) % mod
+        return out.astype(np.uint64)
+
+    x = rng.integers(0, qs[0], size=n, dtype=np.uint64)
+    for g in (5, 25, 2 * n - 1):
+        # permutation in NTT form == automorphism in coefficient form
+        got = o.ntt_inv(0, o.galois_ntt(g, o.ntt_fwd(0, x)))
+        assert np.array_equal(got, auto(x, g, qs[0]))
+        gk = o.keygen_galois(key, sk, g)
+        r = o.apply_galois(gk, g, ct)
+        assert np.array_equal(o.decode(o.decrypt(sk, r)), o.decode(auto(m, g, T65537)))
+        assert o.noise_budget(sk, r) > 10
+
+
 def test_xsalsa20_against_libsodium(oracle_mod):
     """Pin the XSalsa20 keystream to libsodium's crypto_secretbox (PyNaCl):
     secretbox XORs the message with keystream bytes from offset 32."""
