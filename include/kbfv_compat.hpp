@@ -12,12 +12,15 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "kbfv.h"
 
@@ -150,6 +153,8 @@ public:
     BFVContext& context;
     uint64_tt* publicKey = nullptr;
     uint64_tt* rlk_23 = nullptr;
+    std::map<uint64_t, uint64_tt*> galoisKeys;  // rotKey_vec_23 and ConjKey_23, by Galois element
+    Ciphertext cipher_const_1;                  // kept for callers that read it (bfv_demo.cu); unused here
     uint64_t enc_counter = 0;
     uint8_t seed[32];
 
@@ -162,6 +167,7 @@ public:
     ~BFVScheme() {
         if (publicKey) cudaFree(publicKey);
         if (rlk_23) cudaFree(rlk_23);
+        for (auto& kv : galoisKeys) cudaFree(kv.second);
     }
 
     void mallocMemory() { check(kbfv_reserve(context.handle, 1)); }
@@ -178,8 +184,35 @@ public:
         check(kbfv_keygen_relin(context.handle, seed, reinterpret_cast<const uint64_t*>(sk.sx_device),
                                 reinterpret_cast<uint64_t*>(rlk_23), stream));
     }
-    // rotation keys are outside this path; accepted and ignored
-    void addLeftRotKey_23(SecretKey&, long, cudaStream_t = 0) {}
+    // rotation / conjugation keys (KeySwitch_23.cuh:71-166): Galois element 5^r or 2N - 1
+    void addGaloisKey(SecretKey& sk, uint64_t g, cudaStream_t stream = 0) {
+        if (galoisKeys.count(g)) return;
+        uint64_tt* key = nullptr;
+        const size_t words = (size_t)context.dnum * 2 * (context.q_num + context.p_num) * context.N;
+        check_cuda(cudaMalloc(&key, sizeof(uint64_tt) * words));
+        check(kbfv_keygen_galois(context.handle, seed, reinterpret_cast<const uint64_t*>(sk.sx_device), g,
+                                 reinterpret_cast<uint64_t*>(key), stream));
+        galoisKeys[g] = key;
+    }
+    void addLeftRotKey_23(SecretKey& sk, long rot_num, cudaStream_t stream = 0) {
+        addGaloisKey(sk, kbfv_galois_element(context.handle, rot_num), stream);
+    }
+    void addConjKey_23(SecretKey& sk, cudaStream_t stream = 0) { addGaloisKey(sk, 2 * (uint64_t)context.N - 1, stream); }
+    void applyGalois(Ciphertext& cipher, uint64_t g) {
+        auto it = galoisKeys.find(g);
+        if (it == galoisKeys.end()) throw std::invalid_argument("rotKey_23 not exists");
+        check(kbfv_apply_galois(context.handle, reinterpret_cast<const uint64_t*>(it->second), g,
+                                reinterpret_cast<const uint64_t*>(cipher.cipher_device),
+                                reinterpret_cast<uint64_t*>(cipher.cipher_device), 1, 0));
+    }
+    void leftRotateAndEqual_23(Ciphertext& cipher, long rotSlots) {
+        applyGalois(cipher, kbfv_galois_element(context.handle, rotSlots));
+    }
+    // the reference's conversion (KeySwitch_23.cuh:580-584)
+    void rightRotateAndEqual_23(Ciphertext& cipher, long rotSlots) {
+        leftRotateAndEqual_23(cipher, context.N / 2 - (1L << rotSlots));
+    }
+    void conjugate_23(Ciphertext& cipher) { applyGalois(cipher, 2 * (uint64_t)context.N - 1); }
 
     void encryptMsg(Ciphertext& cipher, Plaintext& message, cudaStream_t stream = 0) {
         if (!publicKey) throw std::invalid_argument("public key not generated");
@@ -201,6 +234,27 @@ public:
                        reinterpret_cast<uint64_t*>(res.cipher_device), 1, 0));
     }
     void addAndEqual(Ciphertext& c1, Ciphertext& c2) { add(c1, c1, c2); }
+    // adds the constant c to every slot (BFVScheme.cuh:220-224)
+    void addConstAndEqual(Ciphertext& cipher, uint64_tt c) {
+        uint64_tt* d = nullptr;
+        check_cuda(cudaMalloc(&d, sizeof(uint64_tt) * context.N));
+        std::vector<uint64_tt> h((size_t)context.N, c % context.plain_modulus);
+        check_cuda(cudaMemcpy(d, h.data(), sizeof(uint64_tt) * context.N, cudaMemcpyHostToDevice));
+        int rc = kbfv_encode(context.handle, reinterpret_cast<const uint64_t*>(d), reinterpret_cast<uint64_t*>(d), 1, 0);
+        if (rc == KBFV_OK)
+            rc = kbfv_add_plain(context.handle, reinterpret_cast<const uint64_t*>(cipher.cipher_device),
+                                reinterpret_cast<const uint64_t*>(d), reinterpret_cast<uint64_t*>(cipher.cipher_device),
+                                1, 0);
+        cudaFree(d);
+        check(rc);
+    }
+    // b += NTT(Delta * m) with m the plaintext's coefficients (BFVScheme.cuh:192-217)
+    void addConstAndEqual(Ciphertext& cipher, Plaintext& cnst) {
+        cipher.l = std::min(cipher.l, cnst.l);
+        check(kbfv_add_plain(context.handle, reinterpret_cast<const uint64_t*>(cipher.cipher_device),
+                             reinterpret_cast<const uint64_t*>(cnst.mx_device),
+                             reinterpret_cast<uint64_t*>(cipher.cipher_device), 1, 0));
+    }
     void multConstAndEqual(Ciphertext& cipher, Plaintext& cnst) {
         if (cipher.l == 0) throw std::invalid_argument("Ciphertexts are on level 0");
         check(kbfv_mul_plain(context.handle, reinterpret_cast<const uint64_t*>(cipher.cipher_device),

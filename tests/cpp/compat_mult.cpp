@@ -18,6 +18,7 @@ int main(int argc, char** argv) {
     scheme.addEncKey(sk);
     scheme.addMultKey_23(sk);
     scheme.addLeftRotKey_23(sk, 1);
+    scheme.addLeftRotKey_23(sk, 2);
 
     const int N = (int)context.N, L = context.L, slots = context.slots;
     const uint64_tt t = context.plain_modulus;
@@ -55,6 +56,36 @@ int main(int argc, char** argv) {
         const uint64_tt want = (uint64_tt)((unsigned __int128)mes1[i] * mes2[i] % t * mes1[i] % t);
         if (dec[i] != want) bad++;
     }
+    // rotations: left by 1 twice equals left by 2; plaintext and constant additions
+    Ciphertext c3(N, L, L, slots), c4(N, L, L, slots);
+    scheme.encryptMsg(c3, plain2);
+    scheme.encryptMsg(c4, plain2);
+    scheme.leftRotateAndEqual_23(c3, 1);
+    scheme.leftRotateAndEqual_23(c3, 1);
+    scheme.leftRotateAndEqual_23(c4, 2);
+    std::vector<uint64_tt> r3(slots), r4(slots), r5(slots);
+    scheme.decryptMsg(plain_dec, sk, c3);
+    context.decode(plain_dec, d_dec);
+    check_cuda(cudaMemcpy(r3.data(), d_dec, sizeof(uint64_tt) * slots, cudaMemcpyDeviceToHost));
+    scheme.decryptMsg(plain_dec, sk, c4);
+    context.decode(plain_dec, d_dec);
+    check_cuda(cudaMemcpy(r4.data(), d_dec, sizeof(uint64_tt) * slots, cudaMemcpyDeviceToHost));
+    int moved = 0;
+    for (int i = 0; i < slots; ++i) {
+        if (r3[i] != r4[i]) bad++;
+        if (r3[i] != mes2[i]) moved++;
+    }
+    if (moved == 0) bad++;  // a rotation that changed nothing
+    Ciphertext c5(N, L, L, slots);
+    scheme.encryptMsg(c5, plain2);
+    scheme.addConstAndEqual(c5, plain1);  // plain1 holds mes1's coefficients
+    scheme.addConstAndEqual(c5, (uint64_tt)5);
+    scheme.decryptMsg(plain_dec, sk, c5);
+    context.decode(plain_dec, d_dec);
+    check_cuda(cudaMemcpy(r5.data(), d_dec, sizeof(uint64_tt) * slots, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < slots; ++i)
+        if (r5[i] != (mes1[i] + mes2[i] + 5) % t) bad++;
+
     printf("N=%d slots=%d wrong=%d first: ", N, slots, bad);
     for (int i = 0; i < 4; ++i) printf("%llu ", dec[i]);
     printf("\n");
