@@ -193,6 +193,18 @@ int kbfv_add(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64
  * b += NTT(Delta * m) for plaintexts m of N coefficients mod t */
 int kbfv_add_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_m, uint64_t* d_out,
                    uint32_t count, kbfv_stream stream);
+/* limb-wise ops on `count` ciphertexts (2 x q_count limbs each, NTT form):
+ * sub / subAndEqual, negateAndEqual, multConstAndEqual(Ciphertext&, uint64_tt) and
+ * multConstAndAddCipherEqual (include/BFVScheme.cuh:246-330); the scalar is taken
+ * mod each q_l. d_out may equal an input. */
+int kbfv_sub(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64_t* d_out, uint32_t count,
+             kbfv_stream stream);
+int kbfv_negate(kbfv_context* ctx, const uint64_t* d_x, uint64_t* d_out, uint32_t count, kbfv_stream stream);
+int kbfv_mul_scalar(kbfv_context* ctx, const uint64_t* d_x, uint64_t cnst, uint64_t* d_out, uint32_t count,
+                    kbfv_stream stream);
+/* d_acc += d_x * cnst */
+int kbfv_mul_scalar_add(kbfv_context* ctx, const uint64_t* d_x, uint64_t cnst, uint64_t* d_acc, uint32_t count,
+                        kbfv_stream stream);
 /* BFVScheme::multConstAndEqual (include/BFVScheme.cuh:226-245) with an encode_ntt plaintext */
 int kbfv_mul_plain(kbfv_context* ctx, const uint64_t* d_ct, const uint64_t* d_pt_ntt, uint64_t* d_out,
                    uint32_t count, kbfv_stream stream);
@@ -245,6 +257,22 @@ int kbfv_keygen_galois(kbfv_context* ctx, const uint8_t seed[32], const uint64_t
 /* out = key_switch(automorphism(ct)); out may equal ct */
 int kbfv_apply_galois(kbfv_context* ctx, const uint64_t* d_gk, uint64_t galois_elt, const uint64_t* d_ct,
                       uint64_t* d_out, uint32_t count, kbfv_stream stream);
+
+/* ---- wire format ----------------------------------------------------------
+ * No counterpart in the reference (it has no serialization). A 56-byte header
+ * (magic "KBFVWIRE", version 1, kind, log_n, q_count, p_count, count, aux, a
+ * digest of the context's Q, P and t, payload words per object) followed by the
+ * objects' words, little-endian, in the device layout. Kinds: 1 ciphertext,
+ * 2 plaintext coefficients, 3 secret key, 4 public key, 5 relinearisation key,
+ * 6 Galois key (aux = Galois element), 7 gadget key (aux = log2 of the base),
+ * 8 T-base key. Loading checks the header against the context (a ciphertext at
+ * a lower level loads into that level's context) and fails with
+ * KBFV_ERR_INVALID on any mismatch or truncation. */
+size_t kbfv_wire_bytes(const kbfv_context* ctx, int kind, uint64_t aux, uint32_t count);
+int kbfv_wire_save(kbfv_context* ctx, int kind, uint64_t aux, const uint64_t* d_obj, uint32_t count, void* h_buf,
+                   size_t h_bytes, kbfv_stream stream);
+int kbfv_wire_load(kbfv_context* ctx, int kind, const void* h_buf, size_t h_bytes, uint64_t* d_obj, uint32_t max_count,
+                   uint32_t* count, uint64_t* aux, kbfv_stream stream);
 
 /* ---- levels: fewer live ciphertext primes --------------------------------
  * A ciphertext at level l holds the first l primes of Q (2 x l limbs, NTT form).

@@ -134,6 +134,13 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_context_at_level": (I, [VP, u32, C.POINTER(VP)]),
         "kbfv_probe_arith": (I, [I, u32, C.POINTER(C.c_double)]),
         "kbfv_galois_element": (u64, [VP, C.c_int64]),
+        "kbfv_sub": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_wire_bytes": (C.c_size_t, [VP, I, u64, u32]),
+        "kbfv_wire_save": (I, [VP, I, u64, VP, u32, VP, C.c_size_t, VP]),
+        "kbfv_wire_load": (I, [VP, I, VP, C.c_size_t, VP, u32, C.POINTER(u32), C.POINTER(u64), VP]),
+        "kbfv_negate": (I, [VP, VP, VP, u32, VP]),
+        "kbfv_mul_scalar": (I, [VP, VP, u64, VP, u32, VP]),
+        "kbfv_mul_scalar_add": (I, [VP, VP, u64, VP, u32, VP]),
         "kbfv_keygen_galois": (I, [VP, U8P, VP, u64, VP, VP]),
         "kbfv_apply_galois": (I, [VP, VP, u64, VP, VP, u32, VP]),
         "kbfv_keygen_relin_gadget": (I, [VP, U8P, VP, u32, VP, VP]),
@@ -596,6 +603,34 @@ class BFVScheme:
         _check(lib().kbfv_add(self.context.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device),
                               _ptr(c1.cipher_device), c1.count, _stream_ptr(stream)))
 
+    def sub(self, c1: Ciphertext, c2: Ciphertext, stream=None) -> Ciphertext:
+        out = Ciphertext(c1.ctx, count=c1.count)
+        _check(lib().kbfv_sub(c1.ctx.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device), _ptr(out.cipher_device),
+                              c1.count, _stream_ptr(stream)))
+        return out
+
+    def subAndEqual(self, c1: Ciphertext, c2: Ciphertext, stream=None):
+        _check(lib().kbfv_sub(c1.ctx.handle, _ptr(c1.cipher_device), _ptr(c2.cipher_device), _ptr(c1.cipher_device),
+                              c1.count, _stream_ptr(stream)))
+
+    def negateAndEqual(self, ct: Ciphertext, stream=None):
+        _check(lib().kbfv_negate(ct.ctx.handle, _ptr(ct.cipher_device), _ptr(ct.cipher_device), ct.count,
+                                 _stream_ptr(stream)))
+
+    def multScalarAndEqual(self, ct: Ciphertext, cnst: int, stream=None):
+        """multConstAndEqual(Ciphertext&, uint64_tt) (BFVScheme.cuh:247-268)"""
+        _check(lib().kbfv_mul_scalar(ct.ctx.handle, _ptr(ct.cipher_device), cnst, _ptr(ct.cipher_device), ct.count,
+                                     _stream_ptr(stream)))
+
+    def multConstAndAddCipherEqual(self, c1: Ciphertext, c2: Ciphertext, cnst: int, stream=None):
+        """c1 += c2 * cnst (BFVScheme.cuh:272-288)"""
+        _check(lib().kbfv_mul_scalar_add(c1.ctx.handle, _ptr(c2.cipher_device), cnst, _ptr(c1.cipher_device),
+                                         c1.count, _stream_ptr(stream)))
+
+    def squareAndEqual(self, ct: Ciphertext, stream=None):
+        """squareAndEqual (KeySwitch_23.cuh:422-466): ct * ct, relinearised"""
+        self.mult_relin(ct, ct, out=ct, stream=stream)
+
     def addConstAndEqual(self, ct: Ciphertext, pt: Plaintext, stream=None):
         """ct.b += NTT(Delta * m) (BFVScheme.cuh:192-217)"""
         _check(lib().kbfv_add_plain(self.context.handle, _ptr(ct.cipher_device), _ptr(pt.mx_device),
@@ -722,6 +757,30 @@ class BFVScheme:
         v = C.c_double()
         _check(lib().kbfv_noise_budget(ct.ctx.handle, _ptr(sk.sx_device), _ptr(ct.cipher_device), C.byref(v)))
         return float(v.value)
+
+
+WIRE_KINDS = {"ciphertext": 1, "plaintext": 2, "secret_key": 3, "public_key": 4, "relin_key": 5, "galois_key": 6,
+              "gadget_key": 7, "klss_key": 8}
+
+
+def wire_save(ctx: BFVContext, kind: str, tensor, count: int = 1, aux: int = 0) -> bytes:
+    """serialize device objects (kbfv_wire_save) -> bytes"""
+    k = WIRE_KINDS[kind]
+    nbytes = lib().kbfv_wire_bytes(ctx.handle, k, aux, count)
+    if not nbytes:
+        raise KbfvError(-1, f"{kind} is not available for this context")
+    buf = (C.c_uint8 * nbytes)()
+    _check(lib().kbfv_wire_save(ctx.handle, k, aux, _ptr(tensor), count, buf, nbytes, None))
+    return bytes(buf)
+
+
+def wire_load(ctx: BFVContext, kind: str, data: bytes, out, max_count: int = 1):
+    """deserialize into the device tensor `out`; returns (count, aux)"""
+    k = WIRE_KINDS[kind]
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+    cnt, aux = C.c_uint32(), C.c_uint64()
+    _check(lib().kbfv_wire_load(ctx.handle, k, buf, len(data), _ptr(out), max_count, C.byref(cnt), C.byref(aux), None))
+    return cnt.value, aux.value
 
 
 PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64", "forward NTT butterfly",

@@ -2345,6 +2345,145 @@ int kbfv_apply_galois(kbfv_context* ctx, const uint64_t* d_gk, uint64_t galois_e
     });
 }
 
+
+// ---- scalar and linear ops (BFVScheme.cuh:246-330: multConstAndEqual(uint64),
+// multConstAndAddCipherEqual, sub / subAndEqual, negateAndEqual) -------------
+static int linear_op(kbfv_context* ctx, const uint64_t* x, const uint64_t* y, uint64_t* out, uint64_t cnst,
+                     int op, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(x && out && (op == 1 || op == 2 || y), KBFV_ERR_INVALID, "null argument");
+        const size_t total = (size_t)count * 2 * c.nq * c.n;
+        if (!total) return;
+        ScalarTab tab{};
+        for (int l = 0; op >= 2 && l < c.nq; l++) {
+            tab.c[l] = cnst % c.mods[l];
+            tab.cs[l] = H::shoup(tab.c[l], c.mods[l]);
+        }
+        linear_kernel<<<blocks_for(total, 256), 256, 0, S(stream)>>>(c.dc, x, y, out, total, c.nq, op, tab);
+        check_launch("linear");
+    });
+}
+int kbfv_sub(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64_t* d_out, uint32_t count,
+             kbfv_stream stream) {
+    return linear_op(ctx, d_x, d_y, d_out, 0, 0, count, stream);
+}
+int kbfv_negate(kbfv_context* ctx, const uint64_t* d_x, uint64_t* d_out, uint32_t count, kbfv_stream stream) {
+    return linear_op(ctx, d_x, nullptr, d_out, 0, 1, count, stream);
+}
+int kbfv_mul_scalar(kbfv_context* ctx, const uint64_t* d_x, uint64_t cnst, uint64_t* d_out, uint32_t count,
+                    kbfv_stream stream) {
+    return linear_op(ctx, d_x, nullptr, d_out, cnst, 2, count, stream);
+}
+int kbfv_mul_scalar_add(kbfv_context* ctx, const uint64_t* d_x, uint64_t cnst, uint64_t* d_acc, uint32_t count,
+                        kbfv_stream stream) {
+    return linear_op(ctx, d_x, d_acc, d_acc, cnst, 3, count, stream);
+}
+
+
+// ---- wire format: versioned little-endian container for ciphertexts and keys ----
+namespace {
+struct WireHeader {
+    char magic[8];         // "KBFVWIRE"
+    uint32_t version;      // 1
+    uint32_t kind;         // kbfv_wire_kind
+    uint32_t log_n, q_count, p_count, count;
+    uint64_t aux;          // Galois element (kind 6) or gadget log base (kind 7)
+    uint64_t prime_digest; // FNV-1a over Q (live primes), P and t
+    uint64_t words;        // payload words per object
+};
+static_assert(sizeof(WireHeader) == 56, "wire header layout");
+
+uint64_t prime_digest(const Context& c) {
+    uint64_t h = 1469598103934665603ULL;
+    auto mix = [&](uint64_t v) {
+        for (int b = 0; b < 8; b++) {
+            h ^= (v >> (8 * b)) & 0xff;
+            h *= 1099511628211ULL;
+        }
+    };
+    for (int i = 0; i < c.nq + c.np; i++) mix(c.mods[i]);
+    mix(c.t);
+    return h;
+}
+
+// payload words per object, 0 for an unknown kind
+uint64_t wire_words(const Context& c, int kind, uint64_t aux) {
+    const uint64_t n = c.n, lq = (uint64_t)c.nq * n, lpq = (uint64_t)(c.nq + c.np) * n;
+    switch (kind) {
+        case 1: return 2 * lq;                                // ciphertext [a|b] over Q, NTT
+        case 2: return n;                                     // plaintext coefficients mod t
+        case 3: return lpq;                                   // secret key over Q|P, NTT
+        case 4: return 2 * lq;                                // public key
+        case 5: return (uint64_t)c.dnum * 2 * lpq;            // relinearisation key
+        case 6: return (uint64_t)c.dnum * 2 * lpq;            // Galois key
+        case 7: return aux >= 4 && aux <= 30 ? (uint64_t)c.nq * ((60 + aux - 1) / aux) * 2 * lpq : 0;  // gadget key
+        case 8: return c.klss_ok ? (uint64_t)2 * c.kc.nqj * c.kc.nri * c.nt * n : 0;  // T-base key
+        default: return 0;
+    }
+}
+}  // namespace
+
+size_t kbfv_wire_bytes(const kbfv_context* ctx, int kind, uint64_t aux, uint32_t count) {
+    if (!ctx) return 0;
+    const Context& c = const_cast<kbfv_context*>(ctx)->c;
+    const uint64_t w = wire_words(c, kind, aux);
+    return w ? sizeof(WireHeader) + (size_t)w * count * 8 : 0;
+}
+
+int kbfv_wire_save(kbfv_context* ctx, int kind, uint64_t aux, const uint64_t* d_obj, uint32_t count, void* h_buf,
+                   size_t h_bytes, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        const uint64_t w = wire_words(c, kind, aux);
+        KB_REQUIRE(w, KBFV_ERR_INVALID, "unknown object kind for this context");
+        KB_REQUIRE(d_obj && h_buf, KBFV_ERR_INVALID, "null argument");
+        const size_t need = sizeof(WireHeader) + (size_t)w * count * 8;
+        KB_REQUIRE(h_bytes >= need, KBFV_ERR_INVALID, "buffer too small");
+        WireHeader hd{};
+        std::memcpy(hd.magic, "KBFVWIRE", 8);
+        hd.version = 1;
+        hd.kind = (uint32_t)kind;
+        hd.log_n = (uint32_t)c.logn;
+        hd.q_count = (uint32_t)c.nq;
+        hd.p_count = (uint32_t)c.np;
+        hd.count = count;
+        hd.aux = aux;
+        hd.prime_digest = prime_digest(c);
+        hd.words = w;
+        std::memcpy(h_buf, &hd, sizeof hd);
+        KB_CHECK_CUDA(cudaMemcpyAsync((uint8_t*)h_buf + sizeof hd, d_obj, (size_t)w * count * 8, cudaMemcpyDeviceToHost,
+                                      S(stream)));
+        KB_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+    });
+}
+
+int kbfv_wire_load(kbfv_context* ctx, int kind, const void* h_buf, size_t h_bytes, uint64_t* d_obj, uint32_t max_count,
+                   uint32_t* count, uint64_t* aux, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(h_buf && d_obj, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE(h_bytes >= sizeof(WireHeader), KBFV_ERR_INVALID, "truncated header");
+        WireHeader hd;
+        std::memcpy(&hd, h_buf, sizeof hd);
+        KB_REQUIRE(std::memcmp(hd.magic, "KBFVWIRE", 8) == 0 && hd.version == 1, KBFV_ERR_INVALID,
+                   "not a version-1 kbfv wire object");
+        KB_REQUIRE((int)hd.kind == kind, KBFV_ERR_INVALID, "object kind differs from the requested one");
+        KB_REQUIRE(hd.log_n == (uint32_t)c.logn && hd.q_count == (uint32_t)c.nq && hd.p_count == (uint32_t)c.np &&
+                       hd.prime_digest == prime_digest(c),
+                   KBFV_ERR_INVALID, "object was written for another parameter set or level");
+        const uint64_t w = wire_words(c, kind, hd.aux);
+        KB_REQUIRE(w && hd.words == w, KBFV_ERR_INVALID, "payload size does not match the parameter set");
+        KB_REQUIRE(hd.count <= max_count, KBFV_ERR_INVALID, "more objects than the destination holds");
+        KB_REQUIRE(h_bytes >= sizeof hd + (size_t)w * hd.count * 8, KBFV_ERR_INVALID, "truncated payload");
+        KB_CHECK_CUDA(cudaMemcpyAsync(d_obj, (const uint8_t*)h_buf + sizeof hd, (size_t)w * hd.count * 8,
+                                      cudaMemcpyHostToDevice, S(stream)));
+        KB_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        if (count) *count = hd.count;
+        if (aux) *aux = hd.aux;
+    });
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

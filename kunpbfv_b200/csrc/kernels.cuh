@@ -295,6 +295,26 @@ __global__ void add_kernel(DevConsts c, const uint64_t* __restrict__ x, const ui
     out[i] = add_mod(x[i], y[i], c.mods[l]);
 }
 
+// limb-wise linear ops over ciphertexts (rows of N, limb = row % limbs):
+// op 0: out = x - y; 1: out = -x; 2: out = x * c_l; 3: out = y + x * c_l
+// (c_l = cnst mod q_l with its Shoup constant, passed by value)
+struct ScalarTab {
+    uint64_t c[kMaxQ], cs[kMaxQ];
+};
+__global__ void linear_kernel(DevConsts c, const uint64_t* x, const uint64_t* y, uint64_t* out, size_t total,
+                              int limbs, int op, ScalarTab tab) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int l = (int)((i >> c.logn) % limbs);
+    const uint64_t q = c.mods[l];
+    uint64_t v;
+    if (op == 0) v = sub_mod(x[i], y[i], q);
+    else if (op == 1) v = x[i] ? q - x[i] : 0;
+    else if (op == 2) v = shoup(x[i], tab.c[l], tab.cs[l], q);
+    else v = add_mod(y[i], shoup(x[i], tab.c[l], tab.cs[l], q), q);
+    out[i] = v;
+}
+
 // ct (items x 2 x nq) times pt (items x nq)
 __global__ void mul_plain_kernel(DevConsts c, const uint64_t* __restrict__ ct, const uint64_t* __restrict__ pt,
                                  uint64_t* __restrict__ out, size_t total) {

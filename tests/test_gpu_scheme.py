@@ -209,3 +209,38 @@ def test_ntt_batch_pointer_arrays():
     ctx.ntt_inv_batch(d, ctx.q_count, 0)
     for p, x in zip(polys, d):
         assert np.array_equal(host(x).reshape(p.shape), p)
+
+
+def test_linear_ops_and_square():
+    """sub, negate, scalar multiply (+add), square: decryptions exact, and the
+    limb-wise ops equal the oracle's arithmetic on the same ciphertexts."""
+    import kunpbfv_b200 as kb
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    rng = np.random.default_rng(8)
+    v1 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+    v2 = rng.integers(0, T, size=ctx.N, dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=31)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=32)
+    dec = lambda c: host(ctx.decode(sch.decryptMsg(sk, c).mx_device)).reshape(-1)
+    vo = lambda x: x.astype(object)
+    d = sch.sub(c1, c2)
+    assert np.array_equal(dec(d), ((vo(v1) - vo(v2)) % T).astype(np.uint64))
+    h1 = host(c1.cipher_device).reshape(2, ctx.q_count, ctx.N)
+    h2 = host(c2.cipher_device).reshape(2, ctx.q_count, ctx.N)
+    qs = np.array(ctx.q, dtype=object).reshape(1, -1, 1)
+    assert np.array_equal(host(d.cipher_device).reshape(h1.shape), ((vo(h1) - vo(h2)) % qs).astype(np.uint64))
+    n = kb.Ciphertext(ctx, c1.cipher_device.clone())
+    sch.negateAndEqual(n)
+    assert np.array_equal(dec(n), ((-vo(v1)) % T).astype(np.uint64))
+    s = kb.Ciphertext(ctx, c1.cipher_device.clone())
+    sch.multScalarAndEqual(s, 12345)
+    assert np.array_equal(dec(s), (vo(v1) * 12345 % T).astype(np.uint64))
+    assert np.array_equal(host(s.cipher_device).reshape(h1.shape), (vo(h1) * 12345 % qs).astype(np.uint64))
+    a = kb.Ciphertext(ctx, c1.cipher_device.clone())
+    sch.multConstAndAddCipherEqual(a, c2, 7)
+    assert np.array_equal(dec(a), ((vo(v1) + 7 * vo(v2)) % T).astype(np.uint64))
+    q = kb.Ciphertext(ctx, c1.cipher_device.clone())
+    sch.squareAndEqual(q)
+    assert np.array_equal(dec(q), (vo(v1) * vo(v1) % T).astype(np.uint64))
+    assert np.array_equal(host(q.cipher_device), host(sch.mult_relin(c1, c1).cipher_device))
