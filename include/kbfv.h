@@ -186,6 +186,16 @@ int kbfv_encrypt(kbfv_context* ctx, const uint8_t seed[32], uint64_t enc_id, con
                  const uint64_t* d_m, uint64_t* d_ct, uint32_t count, kbfv_stream stream);
 int kbfv_decrypt(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, uint64_t* d_m,
                  uint32_t count, kbfv_stream stream);
+/* encryption, decryption and addition of `count` objects at arbitrary addresses
+ * (HOST arrays of device pointers, as kbfv_mul_relin_batch): item i of
+ * kbfv_encrypt_batch uses encryption id enc_ids[i] (HOST array) and equals
+ * kbfv_encrypt(ctx, seed, enc_ids[i], ...) of that item alone. */
+int kbfv_encrypt_batch(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* enc_ids, const uint64_t* d_pk,
+                       const uint64_t* const* d_m, uint64_t* const* d_ct, uint32_t count, kbfv_stream stream);
+int kbfv_decrypt_batch(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* const* d_ct, uint64_t* const* d_m,
+                       uint32_t count, kbfv_stream stream);
+int kbfv_add_batch(kbfv_context* ctx, const uint64_t* const* d_x, const uint64_t* const* d_y, uint64_t* const* d_out,
+                   uint32_t count, kbfv_stream stream);
 /* BFVScheme::add / addAndEqual (include/BFVScheme.cuh:169-190); polys per item = 2 */
 int kbfv_add(kbfv_context* ctx, const uint64_t* d_x, const uint64_t* d_y, uint64_t* d_out,
              uint32_t count, kbfv_stream stream);
@@ -366,6 +376,16 @@ int kbfv_noise_budget(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d
  * (zero constants, 32-bit nonce from nonce[0..3], no HSalsa20). */
 int kbfv_salsa20_stream(const uint8_t key[32], const uint8_t nonce[24], uint64_t block0, uint8_t* d_out,
                         size_t nbytes, int compat, kbfv_stream stream);
+/* The reference's sampler conversions (include/Sampler_impl.cuh:13-108) applied
+ * to caller-supplied random words, restated bit for bit (so the same words give
+ * the reference's samples): kind 0 uniform (limbs x N 64-bit words; double
+ * scaling, biased like the reference's), 1 Gaussian sigma 3.2 (N 32-bit words;
+ * normcdfinvf, clamp +-19.2, truncation), 2 ternary (N bytes; `probability` of 0),
+ * 3 Hamming weight h (h 32-bit positions then h sign bytes; collisions keep the
+ * last writer, as in the reference). Output: limbs x N residues for primes
+ * prime0 .. prime0+limbs-1 of the context's table. */
+int kbfv_sample_compat(kbfv_context* ctx, int kind, const void* d_rand, uint64_t* d_out, uint32_t prime0,
+                       uint32_t limbs, uint32_t h, double probability, kbfv_stream stream);
 
 #ifdef __cplusplus
 }

@@ -135,6 +135,10 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_probe_arith": (I, [I, u32, C.POINTER(C.c_double)]),
         "kbfv_galois_element": (u64, [VP, C.c_int64]),
         "kbfv_sub": (I, [VP, VP, VP, VP, u32, VP]),
+        "kbfv_sample_compat": (I, [VP, I, VP, VP, u32, u32, u32, C.c_double, VP]),
+        "kbfv_encrypt_batch": (I, [VP, U8P, U64P, VP, C.POINTER(VP), C.POINTER(VP), u32, VP]),
+        "kbfv_decrypt_batch": (I, [VP, VP, C.POINTER(VP), C.POINTER(VP), u32, VP]),
+        "kbfv_add_batch": (I, [VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
         "kbfv_wire_bytes": (C.c_size_t, [VP, I, u64, u32]),
         "kbfv_wire_save": (I, [VP, I, u64, VP, u32, VP, C.c_size_t, VP]),
         "kbfv_wire_load": (I, [VP, I, VP, C.c_size_t, VP, u32, C.POINTER(u32), C.POINTER(u64), VP]),
@@ -346,6 +350,14 @@ class BFVContext:
         finally:
             lib().kbfv_params_destroy(out)
         return cls(_handle=h)
+
+    def sample_compat(self, kind: int, rand, prime0: int, limbs: int, h: int = 64, probability: float = 0.5,
+                      stream=None):
+        """the reference's sampler conversions on random words (kbfv_sample_compat)"""
+        out = self.zeros(limbs, self.N)
+        _check(lib().kbfv_sample_compat(self._h, kind, _ptr(rand), _ptr(out), prime0, limbs, h, probability,
+                                        _stream_ptr(stream)))
+        return out
 
     def set_seed(self, seed: bytes):
         _check(lib().kbfv_set_seed(self._h, _u8(seed)))

@@ -1064,6 +1064,71 @@ struct GaloisASrc {
     }
 };
 
+// ---- pointer-table variants of encryption, decryption and addition ----------
+// delta * m of item i (plaintext pb.a[i]) into its work slot
+__global__ void delta_m_ptr_kernel(DevConsts c, PtrBatch pb, uint64_t* __restrict__ work, size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const size_t lq = (size_t)c.nq << c.logn;
+    const size_t item = i / lq, w = i % lq;
+    const int l = (int)(w >> c.logn);
+    const uint64_t mv = pb.a[item][w & (((size_t)1 << c.logn) - 1)];
+    const uint64_t mq = shoup(mv, c.negq_mod_t, c.negq_mod_t_s, c.t);
+    work[item * 4 * lq + 3 * lq + w] = shoup(mq, c.tinv_q[l], c.tinv_qs[l], c.mods[l]);
+}
+__global__ void enc_combine_ptr_kernel(DevConsts c, const uint64_t* __restrict__ pk, const uint64_t* __restrict__ work,
+                                       PtrBatch pb, size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const size_t lq = (size_t)c.nq << c.logn;
+    const size_t item = i / lq, w = i % lq;
+    const int l = (int)(w >> c.logn);
+    const uint64_t q = c.mods[l], mh = c.mu_hi[l], ml = c.mu_lo[l];
+    const uint64_t* wk = work + item * 4 * lq;
+    const uint64_t v = wk[w], e0 = wk[lq + w], e1 = wk[2 * lq + w], dm = wk[3 * lq + w];
+    uint64_t* ct = pb.o[item];
+    ct[w] = add_mod(mul_mod(v, pk[w], q, mh, ml), e0, q);
+    ct[lq + w] = add_mod(add_mod(mul_mod(v, pk[lq + w], q, mh, ml), e1, q), dm, q);
+}
+// x = pb.a[item], y = pb.b[item], out = pb.o[item]: 2 x nq limbs each; grid.y = item
+__global__ void add_ptr_kernel(DevConsts c, PtrBatch pb, size_t per_item) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= per_item) return;
+    const int item = blockIdx.y;
+    const int l = (int)((i >> c.logn) % c.nq);
+    pb.o[item][i] = add_mod(pb.a[item][i], pb.b[item][i], c.mods[l]);
+}
+// decryption source with ciphertexts at pb.a[item]
+struct DecSrcP {
+    PtrBatch pb;
+    const uint64_t* sk;
+    DevConsts dc;
+    struct Row {
+        const uint64_t *a, *b, *s;
+        uint64_t q, mp;
+        __device__ __forceinline__ uint64_t load(int j) const { return add_mod(mul_mod_prod(a[j], s[j], q, mp), b[j], q); }
+        __device__ __forceinline__ void store(int, uint64_t) const {}
+    };
+    __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
+    __device__ __forceinline__ Row bind(int row) const {
+        const int item = row / dc.nq, l = row % dc.nq;
+        Row r;
+        r.a = pb.a[item] + ((size_t)l << dc.logn);
+        r.b = r.a + ((size_t)dc.nq << dc.logn);
+        r.s = sk + ((size_t)l << dc.logn);
+        r.q = dc.mods[l];
+        r.mp = dc.mu_prod[l];
+        return r;
+    }
+};
+template <int MAXQ>
+__global__ void decrypt_round_ptr_kernel(DevConsts c, const uint64_t* __restrict__ in, PtrBatch pb) {
+    // the rounding of decrypt_round_kernel, written to pb.o[item]
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t* src = in + ((size_t)blockIdx.y * c.nq << c.logn);
+    pb.o[blockIdx.y][k] = decrypt_round_coeff<MAXQ>(c, src, k);
+}
+
 static void require_klss(const Context& c) {
     KB_REQUIRE(c.klss_ok, KBFV_ERR_INVALID,
                "context has no T-base key switch (needs T primes, q_count divisible by p_count, dnum = q_count / p_count)");
@@ -2481,6 +2546,112 @@ int kbfv_wire_load(kbfv_context* ctx, int kind, const void* h_buf, size_t h_byte
         KB_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
         if (count) *count = hd.count;
         if (aux) *aux = hd.aux;
+    });
+}
+
+
+int kbfv_sample_compat(kbfv_context* ctx, int kind, const void* d_rand, uint64_t* d_out, uint32_t prime0,
+                       uint32_t limbs, uint32_t h, double probability, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(d_rand && d_out, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE(limbs >= 1 && prime0 + limbs <= c.mods.size(), KBFV_ERR_INVALID, "prime range out of table");
+        cudaStream_t st = S(stream);
+        const size_t n = c.n;
+        switch (kind) {
+            case 0:
+                compat_uniform_kernel<<<blocks_for(limbs * n, 256), 256, 0, st>>>(
+                    c.dc, (const uint64_t*)d_rand, d_out, (int)prime0, limbs * n);
+                break;
+            case 1:
+                compat_gauss_kernel<<<blocks_for(n, 256), 256, 0, st>>>(c.dc, (const uint32_t*)d_rand, d_out,
+                                                                       (int)prime0, (int)limbs);
+                break;
+            case 2:
+                compat_zo_kernel<<<blocks_for(n, 256), 256, 0, st>>>(c.dc, (const uint8_t*)d_rand, d_out, (int)prime0,
+                                                                    (int)limbs, probability);
+                break;
+            case 3:
+                KB_REQUIRE(h >= 1 && h <= 1024 && h <= n, KBFV_ERR_INVALID, "Hamming weight out of range");
+                KB_CHECK_CUDA(cudaMemsetAsync(d_out, 0, limbs * n * 8, st));
+                compat_hwt_kernel<<<limbs, h, 0, st>>>(c.dc, (const uint8_t*)d_rand, d_out, (int)prime0, (int)h);
+                break;
+            default:
+                throw KbfvError(KBFV_ERR_INVALID, "unknown sampler kind");
+        }
+        check_launch("sample_compat");
+    });
+}
+
+
+// ---- batches at arbitrary addresses (HOST arrays of device pointers) ---------
+int kbfv_encrypt_batch(kbfv_context* ctx, const uint8_t seed[32], const uint64_t* enc_ids, const uint64_t* d_pk,
+                       const uint64_t* const* d_m, uint64_t* const* d_ct, uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_top(c);
+        if (!seed) seed = c.seed;
+        KB_REQUIRE(enc_ids && d_pk && d_m && d_ct, KBFV_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            PtrBatch pb = make_batch(d_m + off, d_m + off, d_ct + off, cnt);
+            IdTable ids{};
+            for (int i = 0; i < cnt; i++) ids.v[i] = enc_ids[off + i];
+            uint64_t* work = (uint64_t*)ensure_scratch(c, (size_t)cnt * 4 * lq * 8);
+            const size_t per = c.n / 16, per8 = c.n / 8;
+            const SalsaKey kv = subkey_for(seed, DOM_ENC_V, 0), k0 = subkey_for(seed, DOM_ENC_E0, 0),
+                           k1 = subkey_for(seed, DOM_ENC_E1, 0);
+            sample_small_ids_kernel<0><<<blocks_for(per * cnt, 128), 128, 0, st>>>(c.dc, kv, ids, 0, c.nq, work, 4 * lq, cnt);
+            sample_small_ids_kernel<1><<<blocks_for(per8 * cnt, 128), 128, 0, st>>>(c.dc, k0, ids, 0, c.nq, work + lq, 4 * lq, cnt);
+            sample_small_ids_kernel<1><<<blocks_for(per8 * cnt, 128), 128, 0, st>>>(c.dc, k1, ids, 0, c.nq, work + 2 * lq, 4 * lq, cnt);
+            check_launch("sample_small");
+            const size_t total = (size_t)cnt * lq;
+            delta_m_ptr_kernel<<<blocks_for(total, 256), 256, 0, st>>>(c.dc, pb, work, total);
+            check_launch("delta_m");
+            RowsIO io = rows_io(c.dc, work, 0, c.nq);
+            ntt_fwd(c.dc, io, io, cnt * 4 * c.nq, st);
+            enc_combine_ptr_kernel<<<blocks_for(total, 256), 256, 0, st>>>(c.dc, d_pk, work, pb, total);
+            check_launch("enc_combine");
+        }
+    });
+}
+
+int kbfv_decrypt_batch(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* const* d_ct, uint64_t* const* d_m,
+                       uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_sk && d_ct && d_m, KBFV_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        const size_t lq = (size_t)c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            PtrBatch pb = make_batch(d_ct + off, d_ct + off, d_m + off, cnt);
+            uint64_t* work = (uint64_t*)ensure_scratch(c, (size_t)cnt * lq * 8);
+            ntt_inv(c.dc, DecSrcP{pb, d_sk, c.dc}, rows_io(c.dc, work, 0, c.nq), cnt * c.nq, st);
+            dim3 grid((unsigned)(c.n / 128), (unsigned)cnt);
+#define L_DR(M) decrypt_round_ptr_kernel<M><<<grid, 128, 0, st>>>(c.dc, work, pb)
+            DISPATCH_MAXQ(c.nq, L_DR);
+#undef L_DR
+            check_launch("decrypt_round");
+        }
+    });
+}
+
+int kbfv_add_batch(kbfv_context* ctx, const uint64_t* const* d_x, const uint64_t* const* d_y, uint64_t* const* d_out,
+                   uint32_t count, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(d_x && d_y && d_out, KBFV_ERR_INVALID, "null argument");
+        const size_t per = (size_t)2 * c.nq * c.n;
+        for (uint32_t off = 0; off < count; off += kMaxBatch) {
+            const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
+            PtrBatch pb = make_batch(d_x + off, d_y + off, d_out + off, cnt);
+            add_ptr_kernel<<<dim3(blocks_for(per, 256), (unsigned)cnt), 256, 0, S(stream)>>>(c.dc, pb, per);
+            check_launch("add_batch");
+        }
     });
 }
 

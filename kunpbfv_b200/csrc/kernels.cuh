@@ -220,9 +220,8 @@ __global__ void moddown_kernel(DevConsts c, const uint64_t* __restrict__ in, uin
 // decrypt rounding (hps_decrypt_scale_and_round_kernel_*, include/poly_arithmetic.cuh:930-1075)
 // ===========================================================================
 template <int MAXQ>
-__global__ void decrypt_round_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
-    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t* src = in + ((size_t)blockIdx.y * c.nq << c.logn);
+__device__ __forceinline__ uint64_t decrypt_round_coeff(const DevConsts& c, const uint64_t* __restrict__ src,
+                                                       size_t k) {
     const uint64_t t = c.t;
     const int hf = c.qmsbhf;
     const uint64_t mask = ((uint64_t)1 << hf) - 1;
@@ -263,7 +262,14 @@ __global__ void decrypt_round_kernel(DevConsts c, const uint64_t* __restrict__ i
     ds = __dadd_rn(ds, __ull2double_rn(is));
     const uint64_t quot = __double2ull_rz(__dmul_rn(ds, tinv));
     ds = __dsub_rn(ds, __ull2double_rn(t * quot));
-    out[((size_t)blockIdx.y << c.logn) + k] = (uint64_t)llround(ds);
+    return (uint64_t)llround(ds);
+}
+
+template <int MAXQ>
+__global__ void decrypt_round_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t* src = in + ((size_t)blockIdx.y * c.nq << c.logn);
+    out[((size_t)blockIdx.y << c.logn) + k] = decrypt_round_coeff<MAXQ>(c, src, k);
 }
 
 // ===========================================================================
@@ -430,16 +436,10 @@ __global__ void sample_uniform_kernel(DevConsts c, SalsaKey key, uint64_t id0, i
 
 // small polynomials (ternary: 4 bytes/coef, Gaussian: 8 bytes/coef), written
 // as residues over `limbs` consecutive primes from prime0.
-template <int KIND>  // 0 ternary, 1 gaussian
-__global__ void sample_small_kernel(DevConsts c, SalsaKey key, uint64_t id0, int prime0, int limbs,
-                                    uint64_t* __restrict__ out, size_t item_stride, int items) {
+template <int KIND>
+__device__ __forceinline__ void sample_small_block(const DevConsts& c, const SalsaKey& key, uint64_t id, size_t b,
+                                                   int prime0, int limbs, uint64_t* __restrict__ out) {
     constexpr int PER = KIND == 0 ? 16 : 8;
-    const size_t n = (size_t)1 << c.logn;
-    const size_t per_item = n / PER;
-    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= per_item * items) return;
-    const size_t item = gid / per_item, b = gid % per_item;
-    const uint64_t id = id0 + item;
     uint32_t w[16];
     salsa_block(key, (uint32_t)id, (uint32_t)(id >> 32), b, w);
 #pragma unroll
@@ -456,9 +456,35 @@ __global__ void sample_small_kernel(DevConsts c, SalsaKey key, uint64_t id0, int
         const size_t k = b * PER + s;
         for (int l = 0; l < limbs; l++) {
             const uint64_t q = c.mods[prime0 + l];
-            out[item * item_stride + ((size_t)l << c.logn) + k] = v < 0 ? q - (uint64_t)(-v) : (uint64_t)v;
+            out[((size_t)l << c.logn) + k] = v < 0 ? q - (uint64_t)(-v) : (uint64_t)v;
         }
     }
+}
+
+template <int KIND>
+__global__ void sample_small_kernel(DevConsts c, SalsaKey key, uint64_t id0, int prime0, int limbs,
+                                    uint64_t* __restrict__ out, size_t item_stride, int items) {
+    constexpr int PER = KIND == 0 ? 16 : 8;
+    const size_t per_item = ((size_t)1 << c.logn) / PER;
+    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= per_item * items) return;
+    const size_t item = gid / per_item, b = gid % per_item;
+    sample_small_block<KIND>(c, key, id0 + item, b, prime0, limbs, out + item * item_stride);
+}
+
+// the same with one stream id per item (ids passed by value)
+struct IdTable {
+    uint64_t v[128];
+};
+template <int KIND>
+__global__ void sample_small_ids_kernel(DevConsts c, SalsaKey key, IdTable ids, int prime0, int limbs,
+                                        uint64_t* __restrict__ out, size_t item_stride, int items) {
+    constexpr int PER = KIND == 0 ? 16 : 8;
+    const size_t per_item = ((size_t)1 << c.logn) / PER;
+    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= per_item * items) return;
+    const size_t item = gid / per_item, b = gid % per_item;
+    sample_small_block<KIND>(c, key, ids.v[item], b, prime0, limbs, out + item * item_stride);
 }
 
 // Hamming-weight-h ternary secret (convert_HWT, include/Sampler_impl.cuh:68-87):
@@ -532,6 +558,66 @@ __global__ void gk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, c
     uint64_t v = sub_mod(eb[i], mul_mod(a[i], s[i], q, mh, ml), q);
     if (l == prime) v = add_mod(v, mul_mod(mul_mod(s[i], s[i], q, mh, ml), g, q, mh, ml), q);
     eb[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// The reference's conversions of random words into samples
+// (include/Sampler_impl.cuh:13-108), restated operation for operation so that
+// the same random words give the same samples: double arithmetic for the
+// uniform one, float arithmetic and CUDA's normcdfinvf for the Gaussian one.
+// ---------------------------------------------------------------------------
+__global__ void compat_uniform_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                      int prime0, size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const uint64_t q = c.mods[prime0 + (int)(i >> c.logn)];
+    double d = __ull2double_rn(in[i]);
+    d = __ddiv_rn(d, 18446744073709551615.0);  // UINT64_MAX as a double (2^64)
+    d = __dmul_rn(d, __ull2double_rn(q - 1));
+    out[i] = __double2ull_rz(d);
+}
+__global__ void compat_gauss_kernel(DevConsts c, const uint32_t* __restrict__ in, uint64_t* __restrict__ out,
+                                    int prime0, int limbs) {
+    const size_t n = (size_t)1 << c.logn;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float d = __uint2float_rn(in[i]);
+    d = __fdiv_rn(d, 4294967296.0f);  // 4294967295 rounds to 2^32 as a float
+    if (d == 0.f) d = __fadd_rn(d, 1.192092896e-07F);
+    else if (d == 1.f) d = __fsub_rn(d, 1.192092896e-07F);
+    d = normcdfinvf(d);
+    d = __fmaf_rn(d, 3.2f, 0.0f);  // d * stdev + mean, contracted as nvcc does
+    if ((double)d > 19.2) d = 19.2f;
+    else if ((double)d < -19.2) d = -19.2f;
+    const int dd = __float2int_rz(d);
+    for (int t = 0; t < limbs; t++) {
+        const uint64_t q = c.mods[prime0 + t];
+        out[t * n + i] = dd < 0 ? q + (int64_t)dd : (uint64_t)dd;
+    }
+}
+__global__ void compat_zo_kernel(DevConsts c, const uint8_t* __restrict__ in, uint64_t* __restrict__ out,
+                                 int prime0, int limbs, double probability) {
+    const size_t n = (size_t)1 << c.logn;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = (double)(float)in[i];
+    for (int t = 0; t < limbs; t++) {
+        const uint64_t q = c.mods[prime0 + t];
+        uint64_t v;
+        if (d < 256.0 * probability) v = 0;
+        else if (d < 256.0 * (1 + probability) / 2) v = 1;
+        else v = q - 1;
+        out[t * n + i] = v;
+    }
+}
+// one block per limb, h threads: position word, then sign byte (out pre-zeroed)
+__global__ void compat_hwt_kernel(DevConsts c, const uint8_t* __restrict__ in, uint64_t* __restrict__ out,
+                                  int prime0, int h) {
+    const int t = blockIdx.x, j = threadIdx.x;
+    if (j >= h) return;
+    const uint32_t pos = ((const uint32_t*)in)[j] & (((uint32_t)1 << c.logn) - 1);
+    const float d = __fdiv_rn((float)in[(size_t)h * 4 + j], 128.0f);
+    out[((size_t)t << c.logn) + pos] = d >= 1.f ? 1 : c.mods[prime0 + t] - 1;
 }
 
 // Galois automorphism X -> X^g in NTT form: index i holds A(psi^(2 brv(i) + 1)),

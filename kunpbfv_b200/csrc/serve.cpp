@@ -83,6 +83,7 @@ struct Request {
     uint64_t *d_pt = nullptr, *d_ct = nullptr, *d_res = nullptr;
     uint64_t *h_in = nullptr, *h_out = nullptr;
     uint32_t step = 0;  // operations issued
+    bool encrypted = false;
     Clock::time_point t_submit, t_done;
     bool done = false;
     int status = KBFV_OK;
@@ -100,7 +101,7 @@ struct Ring {
     uint8_t seed[32];
     const uint64_t *pk = nullptr, *rlk = nullptr, *sk = nullptr;
     uint64_t n = 0, t = 0;
-    uint32_t nq = 0;
+    uint32_t nq = 0, pt_prime = 0;  // pt_prime: index of the plain modulus in the prime table
     cudaStream_t st = nullptr;
     std::deque<Request*> pending;
     std::vector<Request*> active;
@@ -192,9 +193,7 @@ bool kbfv_server::admit(Ring& r, Request* q) {
     std::vector<uint64_t>().swap(q->input);
     if (cudaMemcpyAsync(q->d_pt, q->h_in, k1 * n * 8, cudaMemcpyHostToDevice, r.st) != cudaSuccess)
         throw ServeError(KBFV_ERR_CUDA, "input copy failed");
-    SRV_CALL(kbfv_encode(r.ctx, q->d_pt, q->d_pt, (uint32_t)k1, r.st));
-    SRV_CALL(kbfv_encrypt(r.ctx, r.seed, q->enc_id, r.pk, q->d_pt, q->d_ct, (uint32_t)k1, r.st));
-    return true;
+    return true;  // encoding and encryption are batched over the iteration's admissions
 }
 
 // One iteration of a ring: admit, advance every admitted request by one
@@ -222,6 +221,26 @@ void kbfv_server::issue(Ring& r) {
     }
     if (r.active.empty()) return;
     const size_t lq = (size_t)r.nq * r.n;
+    // encode + encrypt everything admitted in this iteration in batched calls
+    {
+        std::vector<uint64_t*> pts, cts;
+        std::vector<uint64_t> ids;
+        for (Request* q : r.active) {
+            if (q->step != 0 || q->encrypted) continue;
+            for (uint32_t j = 0; j <= q->nops; j++) {
+                pts.push_back(q->d_pt + (size_t)j * r.n);
+                cts.push_back(q->d_ct + (size_t)j * 2 * lq);
+                ids.push_back(q->enc_id + j);
+            }
+            q->encrypted = true;
+        }
+        if (!pts.empty()) {
+            SRV_CALL(kbfv_ntt_inv_batch(r.ctx, pts.data(), (uint32_t)pts.size(), 1, r.pt_prime, r.st));
+            std::vector<const uint64_t*> cpts(pts.begin(), pts.end());
+            SRV_CALL(kbfv_encrypt_batch(r.ctx, r.seed, ids.data(), r.pk, cpts.data(), cts.data(), (uint32_t)cts.size(),
+                                        r.st));
+        }
+    }
     std::vector<const uint64_t*> A, B;
     std::vector<uint64_t*> O;
     std::vector<Request*> adds;
@@ -241,23 +260,39 @@ void kbfv_server::issue(Ring& r) {
         SRV_CALL(kbfv_mul_relin_batch(r.ctx, r.rlk, A.data() + off, B.data() + off, O.data() + off, cnt, r.st));
         mul_launches++;
     }
-    for (Request* q : adds)
-        SRV_CALL(kbfv_add(r.ctx, q->d_ct, q->d_ct + (size_t)(q->step + 1) * 2 * lq, q->d_ct, 1, r.st));
+    if (!adds.empty()) {
+        std::vector<const uint64_t*> X, Y;
+        std::vector<uint64_t*> Z;
+        for (Request* q : adds) {
+            X.push_back(q->d_ct);
+            Y.push_back(q->d_ct + (size_t)(q->step + 1) * 2 * lq);
+            Z.push_back(q->d_ct);
+        }
+        SRV_CALL(kbfv_add_batch(r.ctx, X.data(), Y.data(), Z.data(), (uint32_t)adds.size(), r.st));
+    }
     std::vector<Request*> still;
+    std::vector<const uint64_t*> dct;
+    std::vector<uint64_t*> dres;
     for (Request* q : r.active) {
         q->step++;
         if (q->step < q->nops) {
             still.push_back(q);
             continue;
         }
-        SRV_CALL(kbfv_decrypt(r.ctx, r.sk, q->d_ct, q->d_res, 1, r.st));
-        SRV_CALL(kbfv_decode(r.ctx, q->d_res, q->d_res, 1, r.st));
-        if (cudaMemcpyAsync(q->h_out, q->d_res, r.n * 8, cudaMemcpyDeviceToHost, r.st) != cudaSuccess)
-            throw ServeError(KBFV_ERR_CUDA, "result copy failed");
-        if ((q->flags & KBFV_REQ_RETURN_CT) &&
-            cudaMemcpyAsync(q->h_out + r.n, q->d_ct, 2 * lq * 8, cudaMemcpyDeviceToHost, r.st) != cudaSuccess)
-            throw ServeError(KBFV_ERR_CUDA, "ciphertext copy failed");
+        dct.push_back(q->d_ct);
+        dres.push_back(q->d_res);
         it.finishing.push_back(q);
+    }
+    if (!dct.empty()) {  // decrypt + decode the finished chains together, then read them back
+        SRV_CALL(kbfv_decrypt_batch(r.ctx, r.sk, dct.data(), dres.data(), (uint32_t)dct.size(), r.st));
+        SRV_CALL(kbfv_ntt_fwd_batch(r.ctx, dres.data(), (uint32_t)dres.size(), 1, r.pt_prime, r.st));
+        for (Request* q : it.finishing) {
+            if (cudaMemcpyAsync(q->h_out, q->d_res, r.n * 8, cudaMemcpyDeviceToHost, r.st) != cudaSuccess)
+                throw ServeError(KBFV_ERR_CUDA, "result copy failed");
+            if ((q->flags & KBFV_REQ_RETURN_CT) &&
+                cudaMemcpyAsync(q->h_out + r.n, q->d_ct, 2 * lq * 8, cudaMemcpyDeviceToHost, r.st) != cudaSuccess)
+                throw ServeError(KBFV_ERR_CUDA, "ciphertext copy failed");
+        }
     }
     if (r.spare_events.empty()) {
         cudaEvent_t e;
@@ -403,8 +438,12 @@ int kbfv_server_add_ring(kbfv_server* s, kbfv_context* ctx, const uint8_t seed[3
     if (rc != KBFV_OK) return rc;
     r->nq = nq;
     r->t = kbfv_context_plain_modulus(ctx);
-    // scratch for a full batch, and at least enough for one request's encryption
-    rc = kbfv_reserve(ctx, std::max<uint32_t>(s->cfg.max_batch, 4));
+    uint32_t nprimes = 0;
+    rc = kbfv_context_primes(ctx, nullptr, &nprimes);
+    if (rc != KBFV_OK) return rc;
+    r->pt_prime = nprimes - 1;
+    // scratch for a full multiply batch and for encrypting 128 plaintexts at once
+    rc = kbfv_reserve(ctx, std::max<uint32_t>(s->cfg.max_batch, 40));
     if (rc != KBFV_OK) return rc;
     if (cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking) != cudaSuccess) return KBFV_ERR_CUDA;
     if (ring_id) *ring_id = (uint32_t)s->rings.size();

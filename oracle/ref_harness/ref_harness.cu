@@ -311,6 +311,32 @@ int main(int argc, char** argv) {
                                                                                               nonce, 1);
         dump_dev("rng_out", (uint64_tt*)d, nbytes / 8);
     }
+    // ---- sampler conversions (Sampler.cuh:16-45, Sampler_impl.cuh:13-108) on
+    // seeded random words, over the P|Q primes (pqt_cons order)
+    {
+        const int npq = K + L + 1;
+        const std::vector<uint64_tt> raw = {~0ULL};
+        auto ru = gen(26, rep(raw, npq), N);  // one 64-bit word per output
+        dump_host("samp_uniform_in", ru.data(), ru.size());
+        uint64_tt* du = up(ru);
+        uint64_tt* ou;
+        ck(cudaMalloc(&ou, (size_t)npq * N * 8), "m");
+        Sampler::uniformSampler_xq((uint8_tt*)du, ou, N, 0, 0, npq);
+        dump_dev("samp_uniform_out", ou, (size_t)npq * N);
+        auto rg = gen(27, raw, N / 2);  // N 32-bit words
+        uint64_tt* dg = up(rg);
+        Sampler::gaussianSampler_xq((uint8_tt*)dg, ou, N, 0, 0, npq);
+        dump_dev("samp_gauss_out", ou, (size_t)npq * N);
+        auto rz = gen(28, raw, N / 8);  // N bytes
+        uint64_tt* dz = up(rz);
+        Sampler::ZOSampler((uint8_tt*)dz, ou, N, 0.5, 0, 0, npq);
+        dump_dev("samp_zo_out", ou, (size_t)npq * N);
+        auto rh = gen(29, raw, 40);  // 64 positions (32-bit) then 64 sign bytes
+        uint64_tt* dh = up(rh);
+        ck(cudaMemset(ou, 0, (size_t)npq * N * 8), "z");
+        Sampler::HWTSampler((uint8_tt*)dh, ou, logN, 64, 0, 0, npq);
+        dump_dev("samp_hwt_out", ou, (size_t)npq * N);
+    }
     // ---- the multiply path without the secret-key shortcut: HPS tensor then
     // the KLSS key switch, as multAndEqual_23 (KeySwitch_23.cuh:244-305) runs
     // them, omitting only its final copy of mult_scale_buffer into cipher1.

@@ -2,7 +2,7 @@
 
     make -C oracle ref                                  # builds oracle/_ref/ref_harness
     oracle/_ref/ref_harness 14 <dir>                    # on a B200
-    python tests/golden/make_ref_fixtures.py <dir> tests/golden/ref_logn14.json
+    python tests/golden/make_ref_fixtures.py <dir> tests/golden/ref_logn14.json [--merge]
 
 The harness writes manifest.txt: per array its name, length, 64-bit digest
 (tests/golden/refgen.py:digest) and first values, and raw copies of small
@@ -16,12 +16,17 @@ import sys
 import numpy as np
 
 
-def main(src, dst):
+def main(src, dst, merge=False):
     out = {"source": "kunpBFV kernels compiled for sm_100a, run on a B200 by oracle/ref_harness", "arrays": {}}
+    if merge and os.path.exists(dst):  # keep the committed arrays; a repeated array must agree
+        with open(dst) as f:
+            out = json.load(f)
     with open(os.path.join(src, "manifest.txt")) as f:
         for line in f:
             parts = line.split()
             name, count, dig = parts[0], int(parts[1]), int(parts[2])
+            if name in out["arrays"]:
+                assert out["arrays"][name]["digest"] == dig, f"{name}: this run disagrees with the committed fixture"
             out["arrays"][name] = {"count": count, "digest": dig, "head": [int(x) for x in parts[3:]]}
             raw = os.path.join(src, name + ".bin")
             if os.path.exists(raw) and count <= 64:
@@ -32,4 +37,4 @@ def main(src, dst):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1], sys.argv[2])
+    main(sys.argv[1], sys.argv[2], "--merge" in sys.argv[3:])

@@ -97,3 +97,27 @@ def test_multiply_vs_reference(ref):
     sch.rlk = dev(rlk)
     out = sch.relinearize(t3)
     check(fx, "mult_out", host(out.cipher_device))
+
+
+def test_sampler_conversions_vs_reference(ref):
+    """The reference's sampler conversions restated on the GPU reproduce its
+    outputs on the same random words (uniform, Gaussian, ternary, HWT)."""
+    ctx, fx = ref
+    n, K, nq = ctx.N, ctx.p_count, ctx.q_count
+    M = 2**64 - 1
+
+    def both(kind, words, **kw):  # reference order P|Q
+        d = dev(words)
+        p = host(ctx.sample_compat(kind, d, ctx.idx_p, K, **kw)).reshape(K, n)
+        q = host(ctx.sample_compat(kind, d, 0, nq, **kw)).reshape(nq, n)
+        return np.concatenate([p, q])
+
+    ru = gen(26, [M] * (K + nq), n)
+    check(fx, "samp_uniform_in", ru)
+    d = dev(ru)
+    p = host(ctx.sample_compat(0, d[:K], ctx.idx_p, K)).reshape(K, n)
+    q = host(ctx.sample_compat(0, d[K:], 0, nq)).reshape(nq, n)
+    check(fx, "samp_uniform_out", np.concatenate([p, q]))
+    check(fx, "samp_gauss_out", both(1, gen(27, [M], n // 2)))
+    check(fx, "samp_zo_out", both(2, gen(28, [M], n // 8), probability=0.5))
+    check(fx, "samp_hwt_out", both(3, gen(29, [M], 40), h=64))

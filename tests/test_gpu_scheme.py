@@ -244,3 +244,39 @@ def test_linear_ops_and_square():
     sch.squareAndEqual(q)
     assert np.array_equal(dec(q), (vo(v1) * vo(v1) % T).astype(np.uint64))
     assert np.array_equal(host(q.cipher_device), host(sch.mult_relin(c1, c1).cipher_device))
+
+
+def test_pointer_batches_equal_contiguous_calls():
+    """kbfv_encrypt_batch / decrypt_batch / add_batch over scattered buffers equal
+    the contiguous calls item by item."""
+    import ctypes as C
+
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200.api import _ptr, _u8, lib
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    rng = np.random.default_rng(12)
+    v = rng.integers(0, T, size=(3, ctx.N), dtype=np.uint64)
+    m = [ctx.encode(dev(v[i])) for i in range(3)]
+    ids = [77, 5, 1234]
+    outs = [kb.Ciphertext(ctx) for _ in range(3)]
+    VP = C.c_void_p
+    rc = lib().kbfv_encrypt_batch(ctx.handle, _u8(SEED), (C.c_uint64 * 3)(*ids), _ptr(sch.publicKey),
+                                  (VP * 3)(*[_ptr(x) for x in m]), (VP * 3)(*[_ptr(o.cipher_device) for o in outs]),
+                                  3, None)
+    assert rc == 0
+    for i in range(3):
+        alone = sch.encryptMsg(kb.Plaintext(ctx, m[i]), enc_id=ids[i])
+        assert np.array_equal(host(outs[i].cipher_device), host(alone.cipher_device)), i
+    sums = [kb.Ciphertext(ctx) for _ in range(2)]
+    rc = lib().kbfv_add_batch(ctx.handle, (VP * 2)(_ptr(outs[0].cipher_device), _ptr(outs[1].cipher_device)),
+                              (VP * 2)(_ptr(outs[2].cipher_device), _ptr(outs[0].cipher_device)),
+                              (VP * 2)(*[_ptr(s.cipher_device) for s in sums]), 2, None)
+    assert rc == 0
+    assert np.array_equal(host(sums[0].cipher_device), host(sch.add(outs[0], outs[2]).cipher_device))
+    res = [ctx.zeros(ctx.N) for _ in range(2)]
+    rc = lib().kbfv_decrypt_batch(ctx.handle, _ptr(sk.sx_device), (VP * 2)(*[_ptr(s.cipher_device) for s in sums]),
+                                  (VP * 2)(*[_ptr(r) for r in res]), 2, None)
+    assert rc == 0
+    assert np.array_equal(host(ctx.decode(res[0])).reshape(-1), (v[0] + v[2]) % T)
+    assert np.array_equal(host(ctx.decode(res[1])).reshape(-1), (v[1] + v[0]) % T)
