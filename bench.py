@@ -49,7 +49,7 @@ def parse():
                     help="run one kernel on a profiling-sized case and exit (for ncu)")
     ap.add_argument("--rows", type=int, default=1024, help="rows for the ntt16k profiling cases")
     ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
-    ap.add_argument("--serve-rates", default="250,500,1000,2000",
+    ap.add_argument("--serve-rates", default="500,1000,2000,3000,4000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=2.5, help="arrival window per rate")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving sweep and print it")
@@ -510,7 +510,7 @@ def serving(args):
              for i, (ln, qb, pb, d, _) in enumerate(SERVE_RINGS)]
     w = make_workload(rings, 64, [m for *_, m in SERVE_RINGS], seed=11)
     points = []
-    with Server(rings, hbm_budget_bytes=8 << 30, max_batch=32, pinned_bytes=1 << 30) as srv:
+    with Server(rings, hbm_budget_bytes=24 << 30, max_batch=64, pinned_bytes=2 << 30) as srv:
         run_open_loop(srv, w, rate=200.0, duration_s=0.5, seed=99)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
             pt = run_open_loop(srv, w, rate=rate, duration_s=args.serve_seconds, seed=100 + i,
