@@ -426,6 +426,25 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     ms_op = time_cuda(per_op, stream, 3)
     res["per_op"] = {"value": round(BATCH / (ms_op / 1e3), 2), "unit": "ct/s",
                      "form": "one pair per call, 8 eager launches each, no graph"}
+    # the operation-by-operation form: tensor (kbfv_mul) then relinearisation
+    # (kbfv_relinearize) as separate calls, one pair each (13 launches per pair)
+    t3 = kb.Tensor3(ctx, count=1)
+    one = kb.Ciphertext(ctx, count=1)
+    ca = [kb.Ciphertext(ctx, a1[i]) for i in range(BATCH)]
+    cb = [kb.Ciphertext(ctx, b1[i]) for i in range(BATCH)]
+
+    def per_op_split():
+        with torch.cuda.stream(stream):
+            for i in range(BATCH):
+                from kunpbfv_b200.api import _ptr, lib
+                lib().kbfv_mul(ctx.handle, _ptr(ca[i].cipher_device), _ptr(cb[i].cipher_device), _ptr(t3.data), 1,
+                               stream.cuda_stream)
+                lib().kbfv_relinearize(ctx.handle, _ptr(sch.rlk), _ptr(t3.data), _ptr(one.cipher_device), 1,
+                                       stream.cuda_stream)
+
+    ms_split = time_cuda(per_op_split, stream, 3)
+    res["per_op_split"] = {"value": round(BATCH / (ms_split / 1e3), 2), "unit": "ct/s",
+                           "form": "one pair per call, multiply then relinearise as separate calls, no graph"}
 
     # e2e through the C ABI with pinned host buffers
     h_a = torch.empty(c1.cipher_device.shape, dtype=torch.int64, pin_memory=True)
