@@ -164,34 +164,18 @@ class ClockSampler:
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    from kunpbfv_b200.replicas import init
+    return init("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from kunpbfv_b200.replicas import barrier as b
+    b(world)
 
 
 def max_over_ranks(world, v):
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from kunpbfv_b200.replicas import max_over_ranks as m
+    return m(world, v)
 
 
 # ---------------------------------------------------------------------------
@@ -308,8 +292,9 @@ def run_ours(args, world, rank, local):
     rng = np.random.default_rng(rank)
     v1 = rng.integers(0, T, size=(BATCH, ctx.N), dtype=np.uint64)
     v2 = rng.integers(0, T, size=(BATCH, ctx.N), dtype=np.uint64)
-    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v1))), enc_id=rank * 1000000)
-    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v2))), enc_id=rank * 1000000 + BATCH)
+    from kunpbfv_b200.replicas import enc_id_base, job_rate
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v1))), enc_id=enc_id_base(rank))
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v2))), enc_id=enc_id_base(rank) + BATCH)
     out = kb.Ciphertext(ctx, count=BATCH)
     torch.cuda.synchronize()
 
@@ -359,7 +344,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(world, ms)
-    value = world * BATCH / (ms / 1e3)
+    value = job_rate(world, BATCH, ms)
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "ct/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -566,10 +551,8 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-            dist.destroy_process_group()
+        from kunpbfv_b200.replicas import finish
+        finish(world)
 
 
 if __name__ == "__main__":
