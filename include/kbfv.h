@@ -349,9 +349,11 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
 /* ---- multiply without allocating -------------------------------------
  * No counterpart in the reference. Same result as kbfv_mul_relin, for callers
  * that must not allocate device memory during a call: services that fix their
- * device-memory budget at start-up, code running where cudaMalloc is not
- * allowed (inside a stream being captured into a CUDA graph, a host callback,
- * an allocator hook), or pools that must not fragment. Its scratch is a
+ * device-memory budget at start-up and cannot risk an out-of-memory failure in
+ * the middle of a request, code running inside another framework's allocator
+ * or memory-pool hook (where calling cudaMalloc again is forbidden), and
+ * latency-bound paths that cannot afford the implicit device synchronisation of
+ * cudaMalloc / cudaFree. Its scratch is a
  * statically sized device array inside libkbfv.so of KBFV_NOALLOC_SCRATCH_BYTES
  * (40 MiB, held by every GPU that loads the library until exit): enough for 2
  * pairs at N=16384 with 7 ciphertext primes and 1 special prime

@@ -2,8 +2,9 @@
 allocating entry point (kbfv_mul_relin).
 
 Some callers cannot allocate device memory while they run (a service that
-fixed its memory budget at start-up, code inside a stream capture or a host
-callback); kbfv_mul_relin_noalloc serves them from a static device array in
+fixed its memory budget at start-up and must not fail with out-of-memory in the
+middle of a request, code inside another framework's allocator hook);
+kbfv_mul_relin_noalloc serves them from a static device array in
 libkbfv.so. This file runs last so that a failure here leaves every other
 result in place; it also passes alone in a fresh process.
 """
