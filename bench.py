@@ -353,7 +353,8 @@ def run_ours(args, world, rank, local):
                    "batch_pairs_per_gpu": BATCH, "cuda_graph": graph is not None,
                    "l2": "inputs 235 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
         "decrypt_exact": ok, "noise_budget_bits": round(budget, 2),
-        "gpu_launches": 8 * args.steps,
+        # 8 kernels per sub-batch; batches of 16+ pairs run as 2 sub-batches on forked streams
+        "gpu_launches": 8 * max(1, min(2, BATCH // 8)) * args.steps,
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.skip_extras:

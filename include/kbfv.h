@@ -231,6 +231,12 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
 int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* const* ct_a,
                          const uint64_t* const* ct_b, uint64_t* const* out, uint32_t count,
                          kbfv_stream stream);
+/* Batches of 16 or more pairs run as sub-batches on the caller's stream and on
+ * auxiliary streams of the context, forked from and joined back into the
+ * caller's stream with events (the call stays ordered on `stream`); the partial
+ * last wave of one sub-batch's kernels then overlaps the others'. branches: 1..4
+ * sub-batches (default 2; 1 disables). No counterpart in the reference. */
+int kbfv_set_branches(kbfv_context* ctx, uint32_t branches);
 /* same for consecutive ciphertexts (stride 2*q_count*N words) */
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);

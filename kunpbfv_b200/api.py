@@ -121,6 +121,7 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_mul": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_relinearize": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_batch": (I, [VP, VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
+        "kbfv_set_branches": (I, [VP, u32]),
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_context_klss": (I, [VP, C.POINTER(u32), C.POINTER(u32), U64P]),
@@ -324,6 +325,10 @@ class BFVContext:
     @property
     def handle(self):
         return self._h
+
+    def set_branches(self, branches: int):
+        """sub-batches (and streams) a batched multiply of 16+ pairs uses, 1..4"""
+        _check(lib().kbfv_set_branches(self._h, branches))
 
     def reserve(self, pairs: int):
         _check(lib().kbfv_reserve(self._h, pairs))

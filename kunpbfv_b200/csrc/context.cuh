@@ -111,6 +111,12 @@ struct Context {
     // levels: contexts for fewer live primes, owned by the top level (index = live primes)
     const Context* parent = nullptr;
     std::vector<void*> levels;
+    // batched multiplies run as `branches` sub-batches on the caller's stream and
+    // auxiliary streams (forked and joined with events), so one sub-batch's
+    // partial last wave overlaps the others' kernels
+    int branches = 2;
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
 };
 
 }  // namespace kbfv

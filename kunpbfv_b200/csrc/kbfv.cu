@@ -1129,6 +1129,28 @@ __global__ void decrypt_round_ptr_kernel(DevConsts c, const uint64_t* __restrict
     pb.o[blockIdx.y][k] = decrypt_round_coeff<MAXQ>(c, src, k);
 }
 
+// sub-batches of a batched multiply: one per `branches`, at least 8 pairs each
+constexpr int kMinBranchPairs = 8;
+static int branch_count(const Context& c, int cnt) {
+    return std::max(1, std::min(c.branches, cnt / kMinBranchPairs));
+}
+static size_t branch_region_bytes(const Context& c, int per) {
+    return (mul_scratch_layout(c, per, nullptr).bytes + 255) & ~(size_t)255;
+}
+static size_t mul_scratch_need(const Context& c, int cnt) {
+    const int nb = branch_count(c, cnt);
+    const size_t whole = mul_scratch_layout(c, cnt, nullptr).bytes;
+    return nb == 1 ? whole : std::max(whole, branch_region_bytes(c, (cnt + nb - 1) / nb) * nb);
+}
+static void ensure_branch_streams(Context& c) {
+    if (c.fork_ev) return;
+    for (int i = 0; i < 3; i++) {
+        KB_CHECK_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
+        KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.join_ev[i], cudaEventDisableTiming));
+    }
+    KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
+}
+
 static void require_klss(const Context& c) {
     KB_REQUIRE(c.klss_ok, KBFV_ERR_INVALID,
                "context has no T-base key switch (needs T primes, q_count divisible by p_count, dnum = q_count / p_count)");
@@ -1245,6 +1267,11 @@ int kbfv_context_destroy(kbfv_context* ctx) {
         if (c.pool) cudaFree(c.pool);
         if (c.scratch) cudaFree(c.scratch);
         if (c.ptrs_event) cudaEventDestroy(c.ptrs_event);
+        for (int i = 0; i < 3; i++) {
+            if (c.aux[i]) cudaStreamDestroy(c.aux[i]);
+            if (c.join_ev[i]) cudaEventDestroy(c.join_ev[i]);
+        }
+        if (c.fork_ev) cudaEventDestroy(c.fork_ev);
         delete ctx;
     });
 }
@@ -1277,7 +1304,7 @@ int kbfv_context_decrypt_variant(const kbfv_context* ctx) { return ctx ? ctx->c.
 
 size_t kbfv_mul_relin_scratch_bytes(const kbfv_context* ctx, uint32_t count) {
     if (!ctx) return 0;
-    return mul_scratch_layout(ctx->c, (int)std::min<uint32_t>(count, kMaxBatch), nullptr).bytes;
+    return mul_scratch_need(ctx->c, (int)std::min<uint32_t>(count, kMaxBatch));
 }
 
 int kbfv_reserve(kbfv_context* ctx, uint32_t pairs) {
@@ -1285,7 +1312,7 @@ int kbfv_reserve(kbfv_context* ctx, uint32_t pairs) {
         Context& c = CX(ctx);
         std::lock_guard<std::mutex> lk(c.mu);
         const int chunk = (int)std::min<uint32_t>(std::max<uint32_t>(pairs, 1), kMaxBatch);
-        size_t need = mul_scratch_layout(c, chunk, nullptr).bytes;
+        size_t need = mul_scratch_need(c, chunk);
         // encryption work area: 4 polys x nq per item; secret/relin keygen: 2*(nq+np)
         need = std::max(need, (size_t)chunk * 4 * c.nq * c.n * 8);
         ensure_scratch(c, need);
@@ -1798,13 +1825,44 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
         cudaStream_t st = S(stream);
         for (uint32_t off = 0; off < count; off += kMaxBatch) {
             const int cnt = (int)std::min<uint32_t>(kMaxBatch, count - off);
-            PtrBatch pb = make_batch(ct_a + off, ct_b + off, out + off, cnt);
             for (int i = 0; i < cnt; i++)
-                KB_REQUIRE(pb.a[i] && pb.b[i] && pb.o[i], KBFV_ERR_INVALID, "null ciphertext pointer");
-            uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
-            MulScratch m = mul_scratch_layout(c, cnt, base);
-            mul_relin_chunk(c, d_rlk, pb, cnt, m, st);
+                KB_REQUIRE(ct_a[off + i] && ct_b[off + i] && out[off + i], KBFV_ERR_INVALID, "null ciphertext pointer");
+            const int nb = branch_count(c, cnt);
+            if (nb == 1) {
+                PtrBatch pb = make_batch(ct_a + off, ct_b + off, out + off, cnt);
+                uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
+                MulScratch m = mul_scratch_layout(c, cnt, base);
+                mul_relin_chunk(c, d_rlk, pb, cnt, m, st);
+                continue;
+            }
+            // sub-batches on the caller's stream and auxiliary streams, each with its
+            // own scratch region, forked from and joined back into the caller's stream
+            const int per = (cnt + nb - 1) / nb;
+            const size_t each = branch_region_bytes(c, per);
+            uint8_t* base = ensure_scratch(c, each * nb);
+            ensure_branch_streams(c);
+            KB_CHECK_CUDA(cudaEventRecord(c.fork_ev, st));
+            for (int b = 1; b < nb; b++) KB_CHECK_CUDA(cudaStreamWaitEvent(c.aux[b - 1], c.fork_ev, 0));
+            for (int b = 0; b < nb; b++) {
+                const int lo = b * per, n = std::min(per, cnt - lo);
+                if (n <= 0) break;
+                PtrBatch pb = make_batch(ct_a + off + lo, ct_b + off + lo, out + off + lo, n);
+                MulScratch m = mul_scratch_layout(c, n, base + b * each);
+                mul_relin_chunk(c, d_rlk, pb, n, m, b == 0 ? st : c.aux[b - 1]);
+            }
+            for (int b = 1; b < nb; b++) {
+                KB_CHECK_CUDA(cudaEventRecord(c.join_ev[b - 1], c.aux[b - 1]));
+                KB_CHECK_CUDA(cudaStreamWaitEvent(st, c.join_ev[b - 1], 0));
+            }
         }
+    });
+}
+
+int kbfv_set_branches(kbfv_context* ctx, uint32_t branches) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        KB_REQUIRE(branches >= 1 && branches <= 4, KBFV_ERR_INVALID, "branches must be 1..4");
+        c.branches = (int)branches;
     });
 }
 

@@ -70,3 +70,22 @@ def test_params_create_without_gpu(oracle_mod):
     bad = (ctypes.c_uint32 * 1)(61)
     out2 = ctypes.POINTER(_Params)()
     assert L.kbfv_params_create(12, bad, 1, pb, 1, 65537, 1, ctypes.byref(out2)) == -1
+
+
+def test_compat_header_compiles_and_links(tmp_path):
+    """include/kbfv_compat.hpp (the reference's class API over the C ABI) and the
+    reference-style driver compile and link against libkbfv.so without a GPU."""
+    import shutil
+    import subprocess
+    from kunpbfv_b200 import build
+    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else shutil.which("nvcc")
+    if not nvcc:
+        pytest.skip("nvcc not available")
+    lib = build.build()
+    out = tmp_path / "compat_mult"
+    r = subprocess.run([nvcc, "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "compat_mult.cpp"), "-L", os.path.dirname(lib), "-lkbfv",
+                        "-Xlinker", "-rpath", "-Xlinker", os.path.dirname(lib), "-o", str(out)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert out.exists()

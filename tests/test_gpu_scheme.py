@@ -280,3 +280,45 @@ def test_pointer_batches_equal_contiguous_calls():
     assert rc == 0
     assert np.array_equal(host(ctx.decode(res[0])).reshape(-1), (v[0] + v[2]) % T)
     assert np.array_equal(host(ctx.decode(res[1])).reshape(-1), (v[1] + v[0]) % T)
+
+
+def test_sub_batches_on_streams_identical():
+    """A 40-pair batch run as 1, 2, 3 or 4 sub-batches on forked streams gives
+    identical ciphertexts, also when captured into a CUDA graph."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    ctx, orc = c3_pair()
+    sk, sch, osk = setup(ctx, orc)
+    rng = np.random.default_rng(21)
+    B = 40
+    v1 = rng.integers(0, T, size=(B, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, T, size=(B, ctx.N), dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=3000)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=4000)
+    outs = []
+    try:
+        for nb in (1, 2, 3, 4):
+            ctx.set_branches(nb)
+            outs.append(host(sch.mult_relin(c1, c2).cipher_device))
+        for o in outs[1:]:
+            assert np.array_equal(o, outs[0])
+        ctx.set_branches(2)
+        st = torch.cuda.Stream()
+        out = kb.Ciphertext(ctx, count=B)
+        with torch.cuda.stream(st):
+            sch.mult_relin(c1, c2, out=out, stream=st)  # warm-up outside the capture
+        torch.cuda.synchronize()
+        out.cipher_device.zero_()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            sch.mult_relin(c1, c2, out=out, stream=st)
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(host(out.cipher_device), outs[0])
+        dec = host(ctx.decode(sch.decryptMsg(sk, out).mx_device)).reshape(B, ctx.N)
+        assert np.array_equal(dec, (v1 * v2) % T)
+    finally:
+        ctx.set_branches(2)
+    with pytest.raises(kb.KbfvError):
+        ctx.set_branches(5)
