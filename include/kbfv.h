@@ -240,6 +240,18 @@ int kbfv_set_branches(kbfv_context* ctx, uint32_t branches);
 /* same for consecutive ciphertexts (stride 2*q_count*N words) */
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);
+/* kbfv_mul_relin on ciphertexts in HOST memory (same layout): the pairs move
+ * through device staging slots in chunks of at most `chunk_pairs` (0: about
+ * 32 MiB of inputs; at most 128; the first and last chunks are smaller), the
+ * copy-in of one chunk overlapping the multiply of the previous and the
+ * copy-out of the one before that. The copies
+ * overlap only when the host buffers are page-locked (cudaHostAlloc /
+ * cudaHostRegister). Ordered on `stream` like every call: the copies start after
+ * the work queued on it, and h_out holds the products once `stream` has passed
+ * the call. The reference multiplies device ciphertexts only (its callers copy
+ * them in and out); no counterpart in the reference. */
+int kbfv_mul_relin_host(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* h_ct_a, const uint64_t* h_ct_b,
+                        uint64_t* h_out, uint32_t count, uint32_t chunk_pairs, kbfv_stream stream);
 
 /* ---- key switching over a gadget decomposition of base 2^w --------------
  * No counterpart in the reference. a1*a2 = sum_i [a1*a2]_{q_i} * g_i (mod Q),

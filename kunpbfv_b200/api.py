@@ -124,6 +124,7 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_set_branches": (I, [VP, u32]),
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
+        "kbfv_mul_relin_host": (I, [VP, VP, VP, VP, VP, u32, u32, VP]),
         "kbfv_context_klss": (I, [VP, C.POINTER(u32), C.POINTER(u32), U64P]),
         "kbfv_params_create": (I, [u32, C.POINTER(u32), u32, C.POINTER(u32), u32, u64, u32,
                                    C.POINTER(C.POINTER(_Params))]),
@@ -696,6 +697,50 @@ class BFVScheme:
             _check(lib().kbfv_mul_relin(c1.ctx.handle, _ptr(self.rlk), _ptr(c1.cipher_device),
                                         _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count,
                                         _stream_ptr(stream)))
+        return out
+
+    def mult_relin_host(self, h_a, h_b, out=None, chunk_pairs: int = 0, stream=None, synchronize: bool = True):
+        """Hybrid mult+relin of ciphertext pairs held in host memory (torch CPU
+        int64 tensors, page-locked for overlapped copies, or numpy uint64 arrays)
+        of the context's top level: [count, 2, q_count, N] each. Copies in,
+        multiplies and copies out chunk by chunk on the context's streams; the
+        products land in `out` (allocated page-locked when not given). With
+        synchronize=False the call only queues the work on `stream`."""
+        torch = _torch()
+        if self.rlk is None:
+            raise KbfvError(-5, "rotKey_23 not exists")
+        if self.relin != "hybrid":
+            raise KbfvInvalidArgument(-1, "host-memory multiply runs the hybrid key switch only")
+        ctx = self.context
+
+        def as_host(x):
+            if isinstance(x, np.ndarray):
+                return torch.from_numpy(np.ascontiguousarray(x, dtype=np.uint64).view(np.int64))
+            if x.device.type != "cpu" or x.dtype != torch.int64 or not x.is_contiguous():
+                raise KbfvInvalidArgument(-1, "host ciphertexts must be contiguous CPU int64 tensors")
+            return x
+
+        a, b = as_host(h_a), as_host(h_b)
+        words = 2 * ctx.q_count * ctx.N
+        if a.numel() != b.numel() or a.numel() % words:
+            raise KbfvInvalidArgument(-1, "host ciphertexts must hold whole ciphertexts, as many in each")
+        count = a.numel() // words
+        if out is None:
+            out = torch.empty(count, 2, ctx.q_count, ctx.N, dtype=torch.int64, pin_memory=True)
+        elif isinstance(out, np.ndarray):
+            raise KbfvInvalidArgument(-1, "out must be a CPU int64 tensor")
+        if out.numel() != a.numel() or out.device.type != "cpu" or out.dtype != torch.int64:
+            raise KbfvInvalidArgument(-1, "out must be a CPU int64 tensor as large as the inputs")
+        sp = _stream_ptr(stream)
+        _check(lib().kbfv_mul_relin_host(ctx.handle, _ptr(self.rlk), a.data_ptr(), b.data_ptr(), out.data_ptr(),
+                                         count, chunk_pairs, sp))
+        if synchronize:
+            if stream is None:
+                torch.cuda.current_stream().synchronize()
+            elif hasattr(stream, "synchronize"):
+                stream.synchronize()
+            else:
+                torch.cuda.synchronize()
         return out
 
     def mult_relin_ptrs(self, a_ptrs, b_ptrs, out_ptrs, stream=None):

@@ -117,6 +117,14 @@ struct Context {
     int branches = 2;
     cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
+    // multiplies of ciphertexts in host memory: copy-in, two compute and
+    // copy-out streams (hs[0..3]); per staging slot the events that mark its
+    // inputs copied in, its product computed and its product copied out
+    cudaStream_t hs[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t hfork = nullptr, hjoin[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t hin[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t hcomp[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t hout[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 }  // namespace kbfv

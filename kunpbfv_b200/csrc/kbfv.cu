@@ -1272,6 +1272,12 @@ int kbfv_context_destroy(kbfv_context* ctx) {
             if (c.join_ev[i]) cudaEventDestroy(c.join_ev[i]);
         }
         if (c.fork_ev) cudaEventDestroy(c.fork_ev);
+        for (int i = 0; i < 4; i++) {
+            if (c.hs[i]) cudaStreamDestroy(c.hs[i]);
+            for (cudaEvent_t e : {c.hjoin[i], c.hin[i], c.hcomp[i], c.hout[i]})
+                if (e) cudaEventDestroy(e);
+        }
+        if (c.hfork) cudaEventDestroy(c.hfork);
         delete ctx;
     });
 }
@@ -1880,6 +1886,122 @@ int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_c
         }
         int rc = kbfv_mul_relin_batch(ctx, d_rlk, A.data(), B.data(), O.data(), count, stream);
         if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+    });
+}
+
+// ---- multiply of ciphertexts held in host memory ----------------------------
+// The pairs stream through kHostSlots device staging slots in chunks: chunk j's
+// inputs are copied in on hs[0] while chunk j-1 is multiplied on hs[1 + (j-1)%2]
+// and chunk j-2's products are copied out on hs[3]. Host-to-device and
+// device-to-host copies use separate copy engines, so the step costs about the
+// larger of the two copy times plus one chunk's multiply and copy-out.
+constexpr int kHostSlots = 4;
+static void ensure_host_streams(Context& c) {
+    if (c.hfork) return;
+    for (int i = 0; i < 4; i++) {
+        KB_CHECK_CUDA(cudaStreamCreateWithFlags(&c.hs[i], cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&c.hjoin[i], &c.hin[i], &c.hcomp[i], &c.hout[i]})
+            KB_CHECK_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.hfork, cudaEventDisableTiming));
+}
+// default chunk: about 32 MiB of input ciphertexts (8 pairs at N=16384 with 7
+// primes, the fastest of 6-24 pairs on a B200 with PCIe 5 at ~55 GB/s each way)
+static int host_chunk_default(const Context& c) {
+    const size_t pair_bytes = (size_t)4 * c.nq * c.n * 8;
+    return (int)std::max<size_t>(1, std::min<size_t>(kMaxBatch, ((size_t)32 << 20) / pair_bytes));
+}
+// chunk sizes for `count` pairs, none above `chunk`: the first two and the last
+// three taper (chunk/4, chunk/2, ..., chunk/2, chunk/4, 1) so the first multiply
+// waits for a short copy-in and the step ends with a short multiply and copy-out
+static std::vector<int> host_chunks(uint32_t count, int chunk) {
+    std::vector<int> head, tail, sizes;
+    if (chunk >= 4) {
+        head = {chunk / 4, chunk / 2};
+        tail = {chunk / 2, chunk / 4, 1};
+    }
+    size_t ends = 0;
+    for (int x : head) ends += x;
+    for (int x : tail) ends += x;
+    if (head.empty() || count < ends + (size_t)chunk) {
+        head.clear();
+        tail.clear();
+        ends = 0;
+    }
+    sizes = head;
+    for (size_t r = count - ends; r > 0;) {
+        const int x = (int)std::min<size_t>(r, chunk);
+        sizes.push_back(x);
+        r -= x;
+    }
+    sizes.insert(sizes.end(), tail.begin(), tail.end());
+    return sizes;
+}
+
+int kbfv_mul_relin_host(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* h_ct_a, const uint64_t* h_ct_b,
+                        uint64_t* h_out, uint32_t count, uint32_t chunk_pairs, kbfv_stream stream) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(d_rlk, KBFV_ERR_NO_KEY, "relinearisation key missing");
+        KB_REQUIRE(h_ct_a && h_ct_b && h_out, KBFV_ERR_INVALID, "null host buffer");
+        KB_REQUIRE(chunk_pairs <= (uint32_t)kMaxBatch, KBFV_ERR_INVALID, "chunk_pairs must be 0..128");
+        if (count == 0) return;
+        const int chunk = (int)std::min<uint32_t>(count, chunk_pairs ? chunk_pairs : host_chunk_default(c));
+        const size_t ctw = (size_t)2 * c.nq * c.n;  // words of one ciphertext
+        const size_t region = branch_region_bytes(c, chunk);
+        const size_t slot_bytes = ((size_t)3 * chunk * ctw * 8 + 255) & ~(size_t)255;
+        uint8_t* base = ensure_scratch(c, 2 * region + kHostSlots * slot_bytes);
+        ensure_host_streams(c);
+        cudaStream_t st = S(stream), h2d = c.hs[0], d2h = c.hs[3];
+        KB_CHECK_CUDA(cudaEventRecord(c.hfork, st));
+        for (int i = 0; i < 4; i++) KB_CHECK_CUDA(cudaStreamWaitEvent(c.hs[i], c.hfork, 0));
+        // slot s: [a x chunk | b x chunk | out x chunk]
+        auto slot = [&](int s) { return (uint64_t*)(base + 2 * region + (size_t)s * slot_bytes); };
+        const std::vector<int> sizes = host_chunks(count, chunk);
+        std::vector<size_t> first(sizes.size());  // first pair of each chunk
+        for (size_t j = 1; j < sizes.size(); j++) first[j] = first[j - 1] + sizes[j - 1];
+        auto copy_out = [&](size_t j) {
+            const int s = (int)(j % kHostSlots);
+            KB_CHECK_CUDA(cudaStreamWaitEvent(d2h, c.hcomp[s], 0));
+            KB_CHECK_CUDA(cudaMemcpyAsync(h_out + first[j] * ctw, slot(s) + 2 * chunk * ctw,
+                                          (size_t)sizes[j] * ctw * 8, cudaMemcpyDeviceToHost, d2h));
+            KB_CHECK_CUDA(cudaEventRecord(c.hout[s], d2h));
+        };
+        const size_t chunks = sizes.size();
+        std::vector<const uint64_t*> A(chunk), B(chunk);
+        std::vector<uint64_t*> O(chunk);
+        for (size_t j = 0; j < chunks; j++) {
+            const int s = (int)(j % kHostSlots), k = (int)(j & 1), n = sizes[j];
+            cudaStream_t comp = c.hs[1 + k];
+            uint64_t* da = slot(s);
+            uint64_t* db = da + chunk * ctw;
+            uint64_t* dout = db + chunk * ctw;
+            // the slot's inputs are free once the multiply of chunk j - kHostSlots read them
+            if (j >= kHostSlots) KB_CHECK_CUDA(cudaStreamWaitEvent(h2d, c.hcomp[s], 0));
+            const size_t off = first[j] * ctw, bytes = (size_t)n * ctw * 8;
+            KB_CHECK_CUDA(cudaMemcpyAsync(da, h_ct_a + off, bytes, cudaMemcpyHostToDevice, h2d));
+            KB_CHECK_CUDA(cudaMemcpyAsync(db, h_ct_b + off, bytes, cudaMemcpyHostToDevice, h2d));
+            KB_CHECK_CUDA(cudaEventRecord(c.hin[s], h2d));
+            KB_CHECK_CUDA(cudaStreamWaitEvent(comp, c.hin[s], 0));
+            // ... and its products once chunk j - kHostSlots was copied out
+            if (j >= kHostSlots) KB_CHECK_CUDA(cudaStreamWaitEvent(comp, c.hout[s], 0));
+            for (int i = 0; i < n; i++) {
+                A[i] = da + i * ctw;
+                B[i] = db + i * ctw;
+                O[i] = dout + i * ctw;
+            }
+            PtrBatch pb = make_batch(A.data(), B.data(), O.data(), n);
+            MulScratch m = mul_scratch_layout(c, n, base + k * region);
+            mul_relin_chunk(c, d_rlk, pb, n, m, comp);
+            KB_CHECK_CUDA(cudaEventRecord(c.hcomp[s], comp));
+            if (j >= 1) copy_out(j - 1);
+        }
+        copy_out(chunks - 1);
+        for (int i = 0; i < 4; i++) {
+            KB_CHECK_CUDA(cudaEventRecord(c.hjoin[i], c.hs[i]));
+            KB_CHECK_CUDA(cudaStreamWaitEvent(st, c.hjoin[i], 0));
+        }
     });
 }
 
