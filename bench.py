@@ -7,8 +7,12 @@ Inputs are resident in HBM (235 MB, larger than the 126 MB L2, so no flush
 is needed between steps).
 
 Also reported on the same box: the one-pair-per-call ("per-op") form, the
-end-to-end rate through the C ABI with host buffers, the standalone NTT at
-N=65536 x 2048 rows (32 primes x 64 polynomials), and the CPU baseline.
+end-to-end rate through the C ABI with page-locked host buffers
+(kbfv_mul_relin_host: copies inside the timed region, overlapped with the
+multiply), the standalone NTT at N=65536 x 2048 rows (32 primes x 64
+polynomials), and the CPU baseline. The default 300 timed steps take about a
+second, so the SM clock is sampled (every 100 ms) several times inside the
+timed region; only those samples are reported.
 
 `--impl reference` times the reference path on the host cores instead: the
 reference (kunpBFV) has no CPU implementation, so this is the CPU oracle's
@@ -22,7 +26,6 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
 import threading
 import time
 
@@ -40,7 +43,7 @@ SEED = bytes(range(32))
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-graph", action="store_true")
@@ -108,27 +111,37 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples (every 100 ms) kept only while the timed region runs:
+    mark() at its start and end."""
 
     def __init__(self, index=0):
         self.index = index
         self.proc = None
-        self.path = None
+        self.rows = []  # (arrival time, fields)
+        self.window = [None, None]
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
         except Exception:
             self.proc = None
         time.sleep(0.3)
         return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.rows.append((time.monotonic(), line.strip().split(",")))
+
+    def mark(self):
+        self.window[0 if self.window[0] is None else 1] = time.monotonic()
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -137,13 +150,12 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+            self.reader.join(timeout=5)
 
     def summary(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
-        try:
-            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
-        except Exception:
-            return out
+        t0, t1 = self.window
+        rows = [r for t, r in self.rows if t0 is None or t1 is None or t0 <= t <= t1]
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -336,11 +348,13 @@ def run_ours(args, world, rank, local):
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         barrier(world)
+        clk.mark()
         ev0.record(stream)
         for _ in range(args.steps):
             run_step()
         ev1.record(stream)
         torch.cuda.synchronize()
+        clk.mark()
     barrier(world)
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(world, ms)

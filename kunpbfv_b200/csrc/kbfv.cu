@@ -509,10 +509,17 @@ static void launch_inv_block(const DevConsts& dc, Src s, Dst d, int rows, int lo
         s, d, dc.tw_inv, dc.mods, logn);
 }
 
+// The view of a store target that the column pass of rings above 2^14 writes
+// and the block kernel reads back: the target itself, unless its store adds an
+// epilogue (an overload for that target returns its plain rows).
+template <class Dst>
+static inline Dst plain_of(const Dst& d) { return d; }
+
 // Forward NTT of `rows` rows read through `s` and written through `d`.
-// For logn <= 14 one block kernel; for 15/16 a column pass (s -> d) then the
-// block kernel in place on d (d must also be readable). FULL = false leaves
-// outputs in [0, 8q) for consumers that reduce anyway (pipeline stages only).
+// For logn <= 14 one block kernel; for 15/16 a column pass (s -> plain_of(d))
+// then the block kernel from plain_of(d) to d in place (d must also be
+// readable). FULL = false leaves outputs in [0, 8q) for consumers that reduce
+// anyway (pipeline stages only).
 template <class Src, class Dst, bool FULL = true>
 static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st) {
     if (rows <= 0) return;
@@ -524,14 +531,18 @@ static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 14: launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st); break;
         case 15: {
             const int total = rows << 14;
-            ntt_fwd_col_kernel<1, Src, Dst><<<blocks_for(total, 256), 256, 0, st>>>(s, d, dc.tw_fwd, dc.mods, 15, total);
-            launch_fwd_block<14, Dst, Dst, FULL>(dc, d, d, rows, 15, st);
+            using DP = decltype(plain_of(d));
+            const DP dp = plain_of(d);
+            ntt_fwd_col_kernel<1, Src, DP><<<blocks_for(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 15, total);
+            launch_fwd_block<14, DP, Dst, FULL>(dc, dp, d, rows, 15, st);
             break;
         }
         case 16: {
             const int total = rows << 14;
-            ntt_fwd_col_kernel<2, Src, Dst><<<blocks_for(total, 256), 256, 0, st>>>(s, d, dc.tw_fwd, dc.mods, 16, total);
-            launch_fwd_block<14, Dst, Dst, FULL>(dc, d, d, rows, 16, st);
+            using DP = decltype(plain_of(d));
+            const DP dp = plain_of(d);
+            ntt_fwd_col_kernel<2, Src, DP><<<blocks_for(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
+            launch_fwd_block<14, DP, Dst, FULL>(dc, dp, d, rows, 16, st);
             break;
         }
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
@@ -737,10 +748,11 @@ struct KeyIPSrc {
     const uint64_t* rlk;  // [ndig][2][npq]
     DevConsts dc;
     int ndig;             // digits: dnum (hybrid) or q_count * pieces (gadget)
-    __device__ __forceinline__ int prime(int row) const { return row % dc.npq; }
+    int m0 = 0, nm = 0;   // rows cover limbs m0 .. m0+nm-1 of Q|P (nm = 0: all of Q|P)
+    __device__ __forceinline__ int prime(int row) const { return m0 + row % (nm ? nm : dc.npq); }
     __device__ __forceinline__ KeyIPRow bind(int row) const {
-        const int npq = dc.npq, logn = dc.logn;
-        const int item = row / (2 * npq), w = row % (2 * npq), h = w / npq, m = w % npq;
+        const int npq = dc.npq, logn = dc.logn, per = nm ? nm : npq;
+        const int item = row / (2 * per), w = row % (2 * per), h = w / per, m = m0 + w % per;
         KeyIPRow r;
         r.dig = sd2 + (((size_t)item * ndig * npq + m) << logn);
         // key limbs: [digit][a|b][Q|P] of the top level; a level reads its live Q limbs and P
@@ -782,7 +794,7 @@ struct GadgetDigitSrc {
 
 // K7 source: mod down P|Q -> q_l and add the tensor term (coefficient form)
 struct ModDownAddRow {
-    const uint64_t* x;    // limb l of the Q|P polynomial
+    const uint64_t* x;    // limb l of the Q|P polynomial, or null (Q part added in the NTT domain)
     const uint64_t* xp;   // limb 0 of its P part
     const uint64_t* add;  // limb l of the term to add, or null
     const uint64_t* pmods;
@@ -804,7 +816,7 @@ struct ModDownAddRow {
             }
             conv = barrett128(acc, q, mh, ml);
         }
-        uint64_t v = shoup(q - conv + x[j], pinv, pinvs, q);
+        uint64_t v = shoup(q - conv + (x ? x[j] : 0), pinv, pinvs, q);
         if (add) v = add_mod(v, add[j], q);
         return v;
     }
@@ -814,13 +826,14 @@ struct ModDownAddSrc {
     const uint64_t* se;   // [item][2][npq]
     const uint64_t* sd;   // [item][2][nq] or null
     DevConsts dc;
+    bool p_only = false;  // se holds only the P limbs (OutCtKeyDst adds the Q part)
     __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
     __device__ __forceinline__ ModDownAddRow bind(int row) const {
         const int nq = dc.nq, npq = dc.npq, logn = dc.logn;
         const int item = row / (2 * nq), w = row % (2 * nq), h = w / nq, l = w % nq;
         ModDownAddRow r;
         const uint64_t* poly = se + (((size_t)item * 2 + h) * npq << logn);
-        r.x = poly + ((size_t)l << logn);
+        r.x = p_only ? nullptr : poly + ((size_t)l << logn);
         r.xp = poly + ((size_t)nq << logn);
         r.add = sd ? sd + (((size_t)(item * 2 + h) * nq + l) << logn) : nullptr;
         r.pmods = dc.mods + dc.idx_p;
@@ -844,6 +857,65 @@ struct OutCtDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
         return PtrRow{pb.o[item] + ((size_t)w << logn)};
     }
 };
+
+// rows (item, h, k) -> limb nq + k (P part) of se ([item][2][npq])
+struct SeRowsP {
+    uint64_t* se;
+    int logn, nq, np, npq;
+    __device__ __forceinline__ int prime(int row) const { return nq + row % np; }
+    __device__ __forceinline__ PtrRow bind(int row) const {
+        const int item = row / (2 * np), w = row % (2 * np), h = w / np, k = w % np;
+        return PtrRow{se + (((size_t)(item * 2 + h) * npq + nq + k) << logn)};
+    }
+};
+
+// Output store of the key-switch tail: adds P^-1 * sum_d digit_d * key_d[h] at
+// limb l of Q (all NTT form, fully reduced) to the transformed value.
+struct OutKeyRow {
+    uint64_t* p;
+    const uint64_t* dig;  // limb l of digit 0, digit stride ds
+    const uint64_t* key;  // limb l of half h of digit 0, digit stride ks
+    size_t ds, ks;
+    int ndig;
+    uint64_t q, mh, ml, mp, pinv, pinvs;
+    __device__ __forceinline__ uint64_t load(int j) const { return p[j]; }
+    __device__ __forceinline__ void store(int j, uint64_t v) const {
+        uint64_t ip;
+        if (ndig == 1) {
+            ip = mul_mod_prod(dig[j], key[j], q, mp);
+        } else {
+            u128 acc{0, 0};
+            for (int d = 0; d < ndig; d++) mac(acc, dig[d * ds + j], key[d * ks + j]);
+            ip = barrett128(acc, q, mh, ml);
+        }
+        p[j] = add_mod(v, shoup(ip, pinv, pinvs, q), q);
+    }
+};
+struct OutCtKeyDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
+    PtrBatch pb;
+    const uint64_t* sd2;  // NTT-form digits [item][ndig][npq]
+    const uint64_t* rlk;  // [ndig][2][Q|P] of the top level
+    DevConsts dc;
+    int ndig;
+    __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
+    __device__ __forceinline__ OutKeyRow bind(int row) const {
+        const int nq = dc.nq, logn = dc.logn;
+        const int item = row / (2 * nq), w = row % (2 * nq), h = w / nq, l = w % nq;
+        OutKeyRow r;
+        r.p = pb.o[item] + ((size_t)w << logn);
+        r.dig = sd2 + (((size_t)item * ndig * dc.npq + l) << logn);
+        r.key = rlk + (((size_t)h * dc.key_npq + l) << logn);
+        r.ds = (size_t)dc.npq << logn;
+        r.ks = (size_t)2 * dc.key_npq << logn;
+        r.ndig = ndig;
+        r.q = dc.mods[l]; r.mh = dc.mu_hi[l]; r.ml = dc.mu_lo[l]; r.mp = dc.mu_prod[l];
+        r.pinv = dc.pinv_q[l]; r.pinvs = dc.pinv_qs[l];
+        return r;
+    }
+};
+// the column pass of rings above 2^14 writes plain values; only the block
+// kernel's final store runs the epilogue
+static inline OutCtDst plain_of(const OutCtKeyDst& d) { return OutCtDst{d.pb, d.dc.logn, d.dc.nq}; }
 
 // K5: scale-and-round to R, R -> Q, and (mode 1) the key-switch lift of a1*a2.
 // mode 0: all three outputs over Q to out0 ([item][3][nq]).
@@ -893,6 +965,20 @@ __global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__ sc, ui
     }
 }
 
+// Key-switch tail over NTT-form digits (sd2, [item][ndig][npq]) and a key
+// ([ndig][2][Q|P] of the top level), written to the outputs of pb:
+//   out_h = add_h + P^-1 (x_h,Q - [x_h,P]_Q),  x_h = sum_d digit_d * key_d[h].
+// Only the P limbs of x are brought back to coefficient form (inverse NTT over
+// P, the key product fused into its loads) for the conversion to Q. The Q limbs
+// stay in the NTT domain, where the forward NTT's store adds them:
+//   NTT(add - P^-1 [x_P]_Q) + P^-1 x_Q,  with x_Q computed at the store.
+static void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* key, int ndig, uint64_t* se,
+                    const uint64_t* add, const PtrBatch& pb, int count, cudaStream_t st) {
+    ntt_inv(dc, KeyIPSrc{sd2, key, dc, ndig, dc.nq, dc.np}, SeRowsP{se, dc.logn, dc.nq, dc.np, dc.npq},
+            count * 2 * dc.np, st);
+    ntt_fwd(dc, ModDownAddSrc{se, add, dc, true}, OutCtKeyDst{pb, sd2, key, dc, ndig}, count * 2 * dc.nq, st);
+}
+
 // INTT over Q of the four input polynomials, Q -> R, NTT over R, fused tensor +
 // INTT over Q|R: steps shared by kbfv_mul and the fused multiply-relinearise.
 static void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st) {
@@ -927,10 +1013,9 @@ static void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb,
     // K6a: NTT over Q|P of the lifted digits, in place, fully reduced (key product uses barrett_prod)
     ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                    count * dc.dnum * dc.npq, st);
-    // K6b: inner product with the key fused into INTT over Q|P
-    ntt_inv(dc, KeyIPSrc{m.sd2, rlk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
-    // K7: mod down + add (cross | b1b2) fused into NTT over Q, written to the outputs
-    ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
+    // K6b: key product over P fused into INTT over P; K7: mod down + add (cross |
+    // b1b2) fused into NTT over Q, the key product over Q added at its store
+    ks_tail(dc, m.sd2, rlk, dc.dnum, m.se, m.sd, pb, count, st);
 }
 
 // rows (item, limb) of the first polynomial of consecutive 3-polynomial tensors
@@ -1804,12 +1889,11 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
             check_launch("modup");
             ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                            cnt * dc.dnum * dc.npq, st);
-            ntt_inv(dc, KeyIPSrc{m.sd2, d_rlk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
             std::vector<uint64_t*> O(cnt);
             std::vector<const uint64_t*> Z(cnt);
             for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
             PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
-            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            ks_tail(dc, m.sd2, d_rlk, dc.dnum, m.se, nullptr, pb, cnt, st);
             // add [cross | b1b2] (NTT form)
             for (int i = 0; i < cnt; i++) {
                 const size_t tot = 2 * lq;
@@ -2375,8 +2459,7 @@ int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32
 
 // ---- key switching over a gadget decomposition ------------------------------
 // G1: pieces of a1*a2 (coefficient form, sd2) fused into the forward NTT over Q|P;
-// G2: inner product with the gadget key fused into the inverse NTT; G3: mod down
-// + add fused into the forward NTT over Q, written to the outputs.
+// G2/G3: the key-switch tail (ks_tail) with the gadget key, written to the outputs.
 static size_t gadget_sg_bytes(const Context& c, int count, int w) {
     return (size_t)count * c.nq * gadget_pieces(w) * (c.nq + c.np) * c.n * 8;
 }
@@ -2386,13 +2469,13 @@ static int gadget_chunk(const Context& c, int w) {
 }
 
 static void gadget_keyswitch(Context& c, const uint64_t* gk, int w, int count, const MulScratch& m, uint64_t* sg,
-                             cudaStream_t st) {
+                             const uint64_t* add, const PtrBatch& pb, cudaStream_t st) {
     const DevConsts& dc = c.dc;
     const int J = gadget_pieces(w), ndig = c.nq * J;
     // fully reduced NTT outputs: the key product sums ndig terms below q^2
     ntt_fwd<GadgetDigitSrc, RowsIO, true>(dc, GadgetDigitSrc{m.sd2, dc, J, w}, rows_io(dc, sg, 0, dc.npq),
                                          count * ndig * dc.npq, st);
-    ntt_inv(dc, KeyIPSrc{sg, gk, dc, ndig}, rows_io(dc, m.se, 0, dc.npq), count * 2 * dc.npq, st);
+    ks_tail(dc, sg, gk, ndig, m.se, add, pb, count, st);
 }
 
 int kbfv_relinearize_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_base, const uint64_t* d_tensor,
@@ -2417,12 +2500,11 @@ int kbfv_relinearize_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t lo
             const uint64_t* tz = d_tensor + (size_t)off * 3 * lq;
             uint64_t* out = d_ct + (size_t)off * 2 * lq;
             ntt_inv(dc, TensorA2{tz, dc.logn, dc.nq}, rows_io(dc, m.sd2, 0, dc.nq), cnt * dc.nq, st);
-            gadget_keyswitch(c, d_gk, w, cnt, m, sg, st);
             std::vector<uint64_t*> O(cnt);
             std::vector<const uint64_t*> Z(cnt);
             for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
             PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
-            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            gadget_keyswitch(c, d_gk, w, cnt, m, sg, nullptr, pb, st);
             for (int i = 0; i < cnt; i++) {
                 const size_t tot = 2 * lq;
                 add_kernel<<<blocks_for(tot, 256), 256, 0, st>>>(dc, out + (size_t)i * 2 * lq, tz + (size_t)i * 3 * lq + lq,
@@ -2461,8 +2543,7 @@ int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_
             uint64_t* sg = (uint64_t*)(base + mb);
             mul_front(c, pb, cnt, m, st);
             k5_launch(c, cnt, m, nullptr, 2, st);
-            gadget_keyswitch(c, d_gk, w, cnt, m, sg, st);
-            ntt_fwd(c.dc, ModDownAddSrc{m.se, m.sd, c.dc}, OutCtDst{pb, c.dc.logn, c.dc.nq}, cnt * 2 * c.dc.nq, st);
+            gadget_keyswitch(c, d_gk, w, cnt, m, sg, m.sd, pb, st);
         }
     });
 }
@@ -2576,12 +2657,11 @@ int kbfv_apply_galois(kbfv_context* ctx, const uint64_t* d_gk, uint64_t galois_e
             check_launch("modup");
             ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                           cnt * dc.dnum * dc.npq, st);
-            ntt_inv(dc, KeyIPSrc{m.sd2, d_gk, dc, dc.dnum}, rows_io(dc, m.se, 0, dc.npq), cnt * 2 * dc.npq, st);
             std::vector<uint64_t*> O(cnt);
             std::vector<const uint64_t*> Z(cnt);
             for (int i = 0; i < cnt; i++) { O[i] = out + (size_t)i * 2 * lq; Z[i] = nullptr; }
             PtrBatch pb = make_batch(Z.data(), Z.data(), O.data(), cnt);
-            ntt_fwd(dc, ModDownAddSrc{m.se, nullptr, dc}, OutCtDst{pb, dc.logn, dc.nq}, cnt * 2 * dc.nq, st);
+            ks_tail(dc, m.sd2, d_gk, dc.dnum, m.se, nullptr, pb, cnt, st);
             for (int i = 0; i < cnt; i++)
                 add_kernel<<<blocks_for(lq, 256), 256, 0, st>>>(dc, out + (size_t)i * 2 * lq + lq, m.sb + (size_t)i * lq,
                                                                 out + (size_t)i * 2 * lq + lq, lq, dc.nq);
