@@ -848,6 +848,41 @@ struct ModDownAddSrc {
     }
 };
 
+// ModDownAddSrc for one special prime: [x_P]_q is x_P mod q, so the row needs
+// no conversion tables (fewer live registers in the transform's first pass)
+struct ModDownAdd1Row {
+    const uint64_t* x;    // limb l of the Q|P polynomial, or null
+    const uint64_t* xp;   // its P limb
+    const uint64_t* add;  // limb l of the term to add, or null
+    uint64_t q, mh, pinv, pinvs;
+    __device__ __forceinline__ uint64_t load(int j) const {
+        const uint64_t conv = barrett64(xp[j], q, mh);
+        uint64_t v = shoup(q - conv + (x ? x[j] : 0), pinv, pinvs, q);
+        if (add) v = add_mod(v, add[j], q);
+        return v;
+    }
+    __device__ __forceinline__ void store(int, uint64_t) const {}
+};
+struct ModDownAdd1Src {
+    const uint64_t* se;   // [item][2][npq]
+    const uint64_t* sd;   // [item][2][nq] or null
+    DevConsts dc;
+    bool p_only = false;
+    __device__ __forceinline__ int prime(int row) const { return row % dc.nq; }
+    __device__ __forceinline__ ModDownAdd1Row bind(int row) const {
+        const int nq = dc.nq, npq = dc.npq, logn = dc.logn;
+        const int item = row / (2 * nq), w = row % (2 * nq), h = w / nq, l = w % nq;
+        const uint64_t* poly = se + (((size_t)item * 2 + h) * npq << logn);
+        ModDownAdd1Row r;
+        r.x = p_only ? nullptr : poly + ((size_t)l << logn);
+        r.xp = poly + ((size_t)nq << logn);
+        r.add = sd ? sd + (((size_t)(item * 2 + h) * nq + l) << logn) : nullptr;
+        r.q = dc.mods[l]; r.mh = dc.mu_hi[l];
+        r.pinv = dc.pinv_q[l]; r.pinvs = dc.pinv_qs[l];
+        return r;
+    }
+};
+
 struct OutCtDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
     PtrBatch pb;
     int logn, nq;
@@ -976,7 +1011,11 @@ static void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* ke
                     const uint64_t* add, const PtrBatch& pb, int count, cudaStream_t st) {
     ntt_inv(dc, KeyIPSrc{sd2, key, dc, ndig, dc.nq, dc.np}, SeRowsP{se, dc.logn, dc.nq, dc.np, dc.npq},
             count * 2 * dc.np, st);
-    ntt_fwd(dc, ModDownAddSrc{se, add, dc, true}, OutCtKeyDst{pb, sd2, key, dc, ndig}, count * 2 * dc.nq, st);
+    const OutCtKeyDst dst{pb, sd2, key, dc, ndig};
+    if (dc.np == 1)
+        ntt_fwd(dc, ModDownAdd1Src{se, add, dc, true}, dst, count * 2 * dc.nq, st);
+    else
+        ntt_fwd(dc, ModDownAddSrc{se, add, dc, true}, dst, count * 2 * dc.nq, st);
 }
 
 // INTT over Q of the four input polynomials, Q -> R, NTT over R, fused tensor +

@@ -244,7 +244,6 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const int t = threadIdx.x;
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
-    const auto d = dst.bind(row);
     const uint64_t q = mods[pidx], q4 = q << 2;
     PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
 
@@ -263,7 +262,9 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     }
     __syncthreads();
     fwd_passes<LOGB, RAD, R0>(c);
-    // coalesced write-out
+    // coalesced write-out; the store target is bound here, so a fused store's
+    // operands hold no registers during the transform
+    const auto d = dst.bind(row);
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         const int j = t + k * T;
@@ -286,7 +287,6 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const int t = threadIdx.x;
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
-    const auto d = dst.bind(row);
     const uint64_t q = mods[pidx], q4 = q << 2;
     PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
 
@@ -298,6 +298,7 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     __syncthreads();
     inv_passes<LOGB, RAD, R0>(c);
     // pass 0 (local stages 0..R0-1), coalesced stores
+    const auto d = dst.bind(row);
 #pragma unroll 1
     for (int g = 0; g < 16 / G0; g++) {
         const int gi = g * T + t;
