@@ -490,6 +490,10 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     mods = torch.tensor(ctx2.q, dtype=torch.int64, device=dev)
     y = torch.randint(0, 1 << 62, (64, 32, 1 << 16), dtype=torch.int64, device=dev)
     y = torch.remainder(y, mods.view(1, 32, 1))
+    # the autotuner's radix split for this ring (column pass + 2^v-point blocks)
+    from kunpbfv_b200 import tune
+    split = tune.tune_ntt(ctx2, rows=2048)
+    ctx2.tune_set("ntt_block_log", split["ntt_block_log"])
     ms_f = time_cuda(lambda: ctx2.ntt_fwd(y, 0, 32, stream=stream), stream, 5)
     ms_i = time_cuda(lambda: ctx2.ntt_inv(y, 0, 32, stream=stream), stream, 5)
     alg2 = 16 * 65536 * 2048 + 16 * 65536 * 32
@@ -497,7 +501,8 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
                          "inv_gbs": round(alg2 / (ms_i / 1e3) / 1e9, 1),
                          "fwd_ms": round(ms_f, 4), "inv_ms": round(ms_i, 4),
                          "frac_of_peak_fwd": round(alg2 / (ms_f / 1e3) / 1e9 / peak, 4),
-                         "rows": 2048, "algorithmic_bytes": alg2}
+                         "rows": 2048, "algorithmic_bytes": alg2,
+                         "split": {"block_log": split["ntt_block_log"], "tuner_ms_fwd_inv": split["ms"]}}
     del y
     ctx2.close()
     return res

@@ -237,12 +237,28 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
  * last wave of one sub-batch's kernels then overlaps the others'. branches: 1..4
  * sub-batches (default 2; 1 disables). No counterpart in the reference. */
 int kbfv_set_branches(kbfv_context* ctx, uint32_t branches);
+/* ---- tuning ---------------------------------------------------------------
+ * Per-context knobs that change speed only, never results. The Python module
+ * kunpbfv_b200.tune picks them by timing the candidates on the device and
+ * caches the choice per device and parameter set. No counterpart in the
+ * reference (its shapes are fixed at compile time). */
+typedef enum {
+    KBFV_TUNE_NTT_BLOCK_LOG = 0, /* 12..14 (default 14): kbfv_ntt_fwd/inv on rings above 2^v
+                                    points run as a column pass of log_n - v stages and blocks of
+                                    2^v points (14: one block per ring up to 2^14) */
+    KBFV_TUNE_BRANCHES = 1,      /* 1..4 (default 2): sub-batches of a batched multiply */
+    KBFV_TUNE_HOST_CHUNK = 2     /* 0..128 (default 0 = ~32 MiB of inputs): pairs per chunk of
+                                    kbfv_mul_relin_host when its chunk_pairs is 0 */
+} kbfv_tune_knob;
+int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value);
+int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value);
 /* same for consecutive ciphertexts (stride 2*q_count*N words) */
 int kbfv_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                    uint64_t* d_out, uint32_t count, kbfv_stream stream);
 /* kbfv_mul_relin on ciphertexts in HOST memory (same layout): the pairs move
- * through device staging slots in chunks of at most `chunk_pairs` (0: about
- * 32 MiB of inputs; at most 128; the first and last chunks are smaller), the
+ * through device staging slots in chunks of at most `chunk_pairs` (0: the
+ * context's KBFV_TUNE_HOST_CHUNK, else about 32 MiB of inputs; at most 128;
+ * the first and last chunks are smaller), the
  * copy-in of one chunk overlapping the multiply of the previous and the
  * copy-out of the one before that. The copies
  * overlap only when the host buffers are page-locked (cudaHostAlloc /

@@ -36,6 +36,10 @@ _ERR_NAMES = {
 }
 
 
+# kbfv_tune_knob (include/kbfv.h)
+TUNE_KNOBS = {"ntt_block_log": 0, "branches": 1, "host_chunk": 2}
+
+
 class KbfvError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"kbfv error {code} ({_ERR_NAMES.get(code, '?')}): {msg}")
@@ -122,6 +126,8 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_relinearize": (I, [VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_batch": (I, [VP, VP, C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32, VP]),
         "kbfv_set_branches": (I, [VP, u32]),
+        "kbfv_tune_set": (I, [VP, I, C.c_int64]),
+        "kbfv_tune_get": (I, [VP, I, C.POINTER(C.c_int64)]),
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_host": (I, [VP, VP, VP, VP, VP, u32, u32, VP]),
@@ -330,6 +336,15 @@ class BFVContext:
     def set_branches(self, branches: int):
         """sub-batches (and streams) a batched multiply of 16+ pairs uses, 1..4"""
         _check(lib().kbfv_set_branches(self._h, branches))
+
+    def tune_set(self, knob: str, value: int):
+        """set a speed-only knob: ntt_block_log (12..14), branches (1..4), host_chunk (0..128)"""
+        _check(lib().kbfv_tune_set(self._h, TUNE_KNOBS[knob], int(value)))
+
+    def tune_get(self, knob: str) -> int:
+        v = C.c_int64()
+        _check(lib().kbfv_tune_get(self._h, TUNE_KNOBS[knob], C.byref(v)))
+        return int(v.value)
 
     def reserve(self, pairs: int):
         _check(lib().kbfv_reserve(self._h, pairs))

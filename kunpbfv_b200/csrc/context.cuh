@@ -115,6 +115,11 @@ struct Context {
     // auxiliary streams (forked and joined with events), so one sub-batch's
     // partial last wave overlaps the others' kernels
     int branches = 2;
+    // tuning knobs (kbfv_tune_set): block size 2^ntt_block_log of the standalone
+    // NTT on rings above it (the rest runs as a column pass of logn - ntt_block_log
+    // stages); pairs per chunk of the host-memory multiply (0: by bytes)
+    int ntt_block_log = 14;
+    int host_chunk = 0;
     cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
     // multiplies of ciphertexts in host memory: copy-in, two compute and

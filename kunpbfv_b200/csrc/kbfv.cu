@@ -480,6 +480,10 @@ static void build_context(Context& c, const kbfv_params& prm) {
 // ===========================================================================
 static inline cudaStream_t S(kbfv_stream s) { return (cudaStream_t)s; }
 static inline unsigned blocks_for(size_t total, unsigned threads) { return (unsigned)((total + threads - 1) / threads); }
+// grid of a grid-stride kernel: enough blocks to cover `total`, at most 2^20
+static inline unsigned stride_blocks(size_t total, unsigned threads) {
+    return (unsigned)std::min<size_t>((total + threads - 1) / threads, (size_t)1 << 20);
+}
 
 template <int LOGB, class Src, class Dst, bool FULL = true>
 static void launch_fwd_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
@@ -530,18 +534,18 @@ static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 13: launch_fwd_block<13, Src, Dst, FULL>(dc, s, d, rows, 13, st); break;
         case 14: launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st); break;
         case 15: {
-            const int total = rows << 14;
+            const size_t total = (size_t)rows << 14;
             using DP = decltype(plain_of(d));
             const DP dp = plain_of(d);
-            ntt_fwd_col_kernel<1, Src, DP><<<blocks_for(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 15, total);
+            ntt_fwd_col_kernel<1, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 15, total);
             launch_fwd_block<14, DP, Dst, FULL>(dc, dp, d, rows, 15, st);
             break;
         }
         case 16: {
-            const int total = rows << 14;
+            const size_t total = (size_t)rows << 14;
             using DP = decltype(plain_of(d));
             const DP dp = plain_of(d);
-            ntt_fwd_col_kernel<2, Src, DP><<<blocks_for(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
+            ntt_fwd_col_kernel<2, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
             launch_fwd_block<14, DP, Dst, FULL>(dc, dp, d, rows, 16, st);
             break;
         }
@@ -561,14 +565,14 @@ static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 14: launch_inv_block<14, Src, Dst, true>(dc, s, d, rows, 14, st); break;
         case 15: {
             launch_inv_block<14, Src, Dst, false>(dc, s, d, rows, 15, st);
-            const int total = rows << 14;
-            ntt_inv_col_kernel<1, Dst, Dst><<<blocks_for(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 15, total);
+            const size_t total = (size_t)rows << 14;
+            ntt_inv_col_kernel<1, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 15, total);
             break;
         }
         case 16: {
             launch_inv_block<14, Src, Dst, false>(dc, s, d, rows, 16, st);
-            const int total = rows << 14;
-            ntt_inv_col_kernel<2, Dst, Dst><<<blocks_for(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
+            const size_t total = (size_t)rows << 14;
+            ntt_inv_col_kernel<2, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
             break;
         }
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
@@ -578,6 +582,44 @@ static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
 
 static inline RowsIO rows_io(const DevConsts& dc, uint64_t* base, int p0, int period) {
     return RowsIO{base, dc.logn, p0, period};
+}
+
+// Standalone NTT of plain rows with a chosen radix split for rings above 2^lb:
+// a column pass of logn - lb stages (forward: first; inverse: last) and block
+// kernels of 2^lb points, lb in 12..14 (14: the default shapes).
+template <int RC, int LB>
+static void ntt_rows_split(const DevConsts& dc, RowsIO io, int rows, bool fwd, cudaStream_t st) {
+    const size_t total = (size_t)rows << LB;
+    if (fwd) {
+        ntt_fwd_col_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_fwd, dc.mods,
+                                                                                      dc.logn, total);
+        launch_fwd_block<LB, RowsIO, RowsIO, true>(dc, io, io, rows, dc.logn, st);
+    } else {
+        launch_inv_block<LB, RowsIO, RowsIO, false>(dc, io, io, rows, dc.logn, st);
+        ntt_inv_col_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_inv, dc.mods,
+                                                                                      dc.logn, total);
+    }
+    check_launch(fwd ? "ntt_fwd" : "ntt_inv");
+}
+static void ntt_rows(const Context& c, RowsIO io, int rows, bool fwd, cudaStream_t st) {
+    const DevConsts& dc = c.dc;
+    if (rows <= 0) return;
+    const int lb = c.ntt_block_log;
+    if (lb >= dc.logn || lb == 14) {
+        if (fwd) ntt_fwd(dc, io, io, rows, st);
+        else ntt_inv(dc, io, io, rows, st);
+        return;
+    }
+    switch (dc.logn * 100 + lb) {
+        case 1312: ntt_rows_split<1, 12>(dc, io, rows, fwd, st); break;
+        case 1412: ntt_rows_split<2, 12>(dc, io, rows, fwd, st); break;
+        case 1413: ntt_rows_split<1, 13>(dc, io, rows, fwd, st); break;
+        case 1513: ntt_rows_split<2, 13>(dc, io, rows, fwd, st); break;
+        case 1512: ntt_rows_split<3, 12>(dc, io, rows, fwd, st); break;
+        case 1613: ntt_rows_split<3, 13>(dc, io, rows, fwd, st); break;
+        case 1612: ntt_rows_split<4, 12>(dc, io, rows, fwd, st); break;
+        default: throw KbfvError(KBFV_ERR_INVALID, "unsupported NTT split");
+    }
 }
 
 // bucketed MAX template dispatch for per-coefficient kernels
@@ -1454,8 +1496,9 @@ int kbfv_ntt_fwd(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t pr
     return guarded([&] {
         Context& c = CX(ctx);
         KB_REQUIRE(d_rows && period >= 1 && prime0 + period <= c.mods.size(), KBFV_ERR_INVALID, "bad NTT rows");
+        KB_REQUIRE(rows <= (1u << 27), KBFV_ERR_INVALID, "at most 2^27 rows per call");
         RowsIO io = rows_io(c.dc, d_rows, (int)prime0, (int)period);
-        ntt_fwd(c.dc, io, io, (int)rows, S(stream));
+        ntt_rows(c, io, (int)rows, true, S(stream));
     });
 }
 
@@ -1464,8 +1507,9 @@ int kbfv_ntt_inv(kbfv_context* ctx, uint64_t* d_rows, uint32_t rows, uint32_t pr
     return guarded([&] {
         Context& c = CX(ctx);
         KB_REQUIRE(d_rows && period >= 1 && prime0 + period <= c.mods.size(), KBFV_ERR_INVALID, "bad NTT rows");
+        KB_REQUIRE(rows <= (1u << 27), KBFV_ERR_INVALID, "at most 2^27 rows per call");
         RowsIO io = rows_io(c.dc, d_rows, (int)prime0, (int)period);
-        ntt_inv(c.dc, io, io, (int)rows, S(stream));
+        ntt_rows(c, io, (int)rows, false, S(stream));
     });
 }
 
@@ -1793,7 +1837,7 @@ int kbfv_encrypt(kbfv_context* ctx, const uint8_t seed[32], uint64_t enc_id, con
             RowsIO io = rows_io(c.dc, work, 0, c.nq);
             ntt_fwd(c.dc, io, io, cnt * 4 * c.nq, st);
             const size_t total = (size_t)cnt * lq;
-            enc_combine_kernel<<<blocks_for(total, 256), 256, 0, st>>>(c.dc, d_pk, work, d_ct + (size_t)off * 2 * lq, total);
+            enc_combine_kernel<<<stride_blocks(total, 256), 256, 0, st>>>(c.dc, d_pk, work, d_ct + (size_t)off * 2 * lq, total);
             check_launch("enc_combine");
         }
     });
@@ -1987,6 +2031,40 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
     });
 }
 
+int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        switch (knob) {
+            case KBFV_TUNE_NTT_BLOCK_LOG:
+                KB_REQUIRE(value >= 12 && value <= 14, KBFV_ERR_INVALID, "NTT block log must be 12..14");
+                c.ntt_block_log = (int)value;
+                break;
+            case KBFV_TUNE_BRANCHES:
+                KB_REQUIRE(value >= 1 && value <= 4, KBFV_ERR_INVALID, "branches must be 1..4");
+                c.branches = (int)value;
+                break;
+            case KBFV_TUNE_HOST_CHUNK:
+                KB_REQUIRE(value >= 0 && value <= kMaxBatch, KBFV_ERR_INVALID, "host chunk must be 0..128");
+                c.host_chunk = (int)value;
+                break;
+            default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
+        }
+    });
+}
+
+int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value) {
+    return guarded([&] {
+        const Context& c = CX(const_cast<kbfv_context*>(ctx));
+        KB_REQUIRE(value, KBFV_ERR_INVALID, "null argument");
+        switch (knob) {
+            case KBFV_TUNE_NTT_BLOCK_LOG: *value = c.ntt_block_log; break;
+            case KBFV_TUNE_BRANCHES: *value = c.branches; break;
+            case KBFV_TUNE_HOST_CHUNK: *value = c.host_chunk; break;
+            default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
+        }
+    });
+}
+
 int kbfv_set_branches(kbfv_context* ctx, uint32_t branches) {
     return guarded([&] {
         Context& c = CX(ctx);
@@ -2070,7 +2148,8 @@ int kbfv_mul_relin_host(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t
         KB_REQUIRE(h_ct_a && h_ct_b && h_out, KBFV_ERR_INVALID, "null host buffer");
         KB_REQUIRE(chunk_pairs <= (uint32_t)kMaxBatch, KBFV_ERR_INVALID, "chunk_pairs must be 0..128");
         if (count == 0) return;
-        const int chunk = (int)std::min<uint32_t>(count, chunk_pairs ? chunk_pairs : host_chunk_default(c));
+        const int want = chunk_pairs ? (int)chunk_pairs : c.host_chunk ? c.host_chunk : host_chunk_default(c);
+        const int chunk = (int)std::min<uint32_t>(count, (uint32_t)want);
         const size_t ctw = (size_t)2 * c.nq * c.n;  // words of one ciphertext
         const size_t region = branch_region_bytes(c, chunk);
         const size_t slot_bytes = ((size_t)3 * chunk * ctw * 8 + 255) & ~(size_t)255;
@@ -2460,7 +2539,7 @@ int kbfv_mod_switch(kbfv_context* ctx, const uint64_t* d_ct, uint64_t* d_out, ui
             ntt_inv(dc, LastLimbSrc{in, c.logn, c.nq}, rows_io(dc, last, c.nq - 1, 1), polys, st);
             ntt_fwd(dc, ModSwitchSrc{last, dc}, rows_io(dc, corr, 0, nout), polys * nout, st);
             const size_t total = (size_t)polys * nout * c.n;
-            mod_switch_combine_kernel<<<blocks_for(total, 256), 256, 0, st>>>(dc, in, corr, o, total);
+            mod_switch_combine_kernel<<<stride_blocks(total, 256), 256, 0, st>>>(dc, in, corr, o, total);
             check_launch("mod_switch");
         }
     });
@@ -2907,11 +2986,11 @@ int kbfv_encrypt_batch(kbfv_context* ctx, const uint8_t seed[32], const uint64_t
             sample_small_ids_kernel<1><<<blocks_for(per8 * cnt, 128), 128, 0, st>>>(c.dc, k1, ids, 0, c.nq, work + 2 * lq, 4 * lq, cnt);
             check_launch("sample_small");
             const size_t total = (size_t)cnt * lq;
-            delta_m_ptr_kernel<<<blocks_for(total, 256), 256, 0, st>>>(c.dc, pb, work, total);
+            delta_m_ptr_kernel<<<stride_blocks(total, 256), 256, 0, st>>>(c.dc, pb, work, total);
             check_launch("delta_m");
             RowsIO io = rows_io(c.dc, work, 0, c.nq);
             ntt_fwd(c.dc, io, io, cnt * 4 * c.nq, st);
-            enc_combine_ptr_kernel<<<blocks_for(total, 256), 256, 0, st>>>(c.dc, d_pk, work, pb, total);
+            enc_combine_ptr_kernel<<<stride_blocks(total, 256), 256, 0, st>>>(c.dc, d_pk, work, pb, total);
             check_launch("enc_combine");
         }
     });

@@ -318,12 +318,10 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
 // Forward outputs are in [0, 8q); inverse inputs may be in [0, 4q).
 // ---------------------------------------------------------------------------
 template <int RC, class Src, class Dst>
-__global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
-                                   const uint64_t* __restrict__ mods, int logn, int ncol_total) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= ncol_total) return;
+__device__ __forceinline__ void ntt_fwd_col(const Src& src, const Dst& dst, const tw_t* __restrict__ tw_all,
+                                            const uint64_t* __restrict__ mods, int logn, size_t gid) {
     const int cols = 1 << (logn - RC);
-    const int row = gid / cols, c = gid % cols;
+    const int row = (int)(gid >> (logn - RC)), c = (int)(gid & (cols - 1));
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
@@ -338,12 +336,10 @@ __global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw
 }
 
 template <int RC, class Src, class Dst>
-__global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
-                                   const uint64_t* __restrict__ mods, int logn, int ncol_total) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= ncol_total) return;
+__device__ __forceinline__ void ntt_inv_col(const Src& src, const Dst& dst, const tw_t* __restrict__ tw_all,
+                                            const uint64_t* __restrict__ mods, int logn, size_t gid) {
     const int cols = 1 << (logn - RC);
-    const int row = gid / cols, c = gid % cols;
+    const int row = (int)(gid >> (logn - RC)), c = (int)(gid & (cols - 1));
     const int pidx = src.prime(row);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
@@ -355,6 +351,23 @@ __global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw
     inv_group<RC>(x, tw, 0, 0, q, q4, true);
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) d.store(c + k * cols, x[k]);
+}
+
+// grid-stride over all columns of all rows (more than 2^31 columns allowed)
+template <int RC, class Src, class Dst>
+__global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
+                                   const uint64_t* __restrict__ mods, int logn, size_t ncol_total) {
+    for (size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gid < ncol_total;
+         gid += (size_t)gridDim.x * blockDim.x)
+        ntt_fwd_col<RC>(src, dst, tw_all, mods, logn, gid);
+}
+
+template <int RC, class Src, class Dst>
+__global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
+                                   const uint64_t* __restrict__ mods, int logn, size_t ncol_total) {
+    for (size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gid < ncol_total;
+         gid += (size_t)gridDim.x * blockDim.x)
+        ntt_inv_col<RC>(src, dst, tw_all, mods, logn, gid);
 }
 
 // ---------------------------------------------------------------------------

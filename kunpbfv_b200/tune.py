@@ -1,0 +1,221 @@
+"""Autotuner for the speed-only knobs of a context (``kbfv_tune_set``).
+
+Knobs (include/kbfv.h, ``kbfv_tune_knob``):
+
+* ``ntt_block_log`` - the radix split of the standalone NTT on rings above
+  2^v points: a column pass of ``log_n - v`` stages and block kernels of 2^v
+  points, v in 12..14;
+* ``branches`` - sub-batches (one stream each) of a batched multiply, 1..4;
+* ``host_chunk`` - pairs per chunk of the host-memory multiply, 0..128.
+
+Each candidate is timed on the device with CUDA events (two warm-up calls,
+then the median of three timed trials of ``reps`` calls). Knobs never change
+results: every candidate's output is compared with the default's, and a
+mismatch raises. The winners are applied to the context and stored in a JSON
+cache keyed by device and parameter set, so a later process applies them with
+``apply_cached`` instead of timing again. The reference has no tuner (its
+kernel shapes are fixed at compile time).
+"""
+from __future__ import annotations
+
+import json
+import os
+import statistics
+from typing import Callable, Dict, Optional
+
+DEFAULT_CACHE = os.environ.get("KBFV_TUNE_CACHE",
+                               os.path.join(os.path.expanduser("~"), ".cache", "kunpbfv_b200", "tune.json"))
+
+NTT_BLOCK_LOGS = (12, 13, 14)
+BRANCHES = (1, 2, 3, 4)
+HOST_CHUNKS = (4, 8, 12, 16, 24)
+
+
+def cache_key(device: str, log_n: int, q_count: int, p_count: int, dnum: int, pairs: int) -> str:
+    return f"{device}|logn={log_n}|q={q_count}|p={p_count}|dnum={dnum}|pairs={pairs}"
+
+
+def context_key(ctx, pairs: int) -> str:
+    import torch
+    dev = torch.cuda.get_device_name()
+    return cache_key(dev, ctx.log_n, ctx.q_count, ctx.p_count, ctx.dnum, pairs)
+
+
+def load_cache(path: str = DEFAULT_CACHE) -> Dict[str, dict]:
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return data if isinstance(data, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def save_cache(entries: Dict[str, dict], path: str = DEFAULT_CACHE) -> None:
+    """Merge `entries` into the cache file (written atomically)."""
+    data = load_cache(path)
+    data.update(entries)
+    d = os.path.dirname(path)
+    if d:
+        os.makedirs(d, exist_ok=True)
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def time_ms(fn: Callable[[], None], reps: int = 5, trials: int = 3) -> float:
+    """Median over `trials` of the CUDA-event time of `reps` calls, per call."""
+    import torch
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(trials):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b) / reps)
+    return statistics.median(out)
+
+
+def _random_rows(ctx, rows: int, prime0: int, period: int, seed: int = 1):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.randint(0, 1 << 62, (rows, ctx.N), dtype=torch.int64, device="cuda", generator=g)
+    mods = torch.tensor([ctx.primes[prime0 + r % period] for r in range(rows)], dtype=torch.int64, device="cuda")
+    return torch.remainder(x, mods[:, None])
+
+
+def tune_ntt(ctx, rows: int = 512, reps: int = 5) -> Dict[str, object]:
+    """Radix split of the standalone forward + inverse NTT over `rows` rows."""
+    import torch
+    if ctx.log_n <= 12:
+        return {"ntt_block_log": 14, "ms": {}}
+    keep = ctx.tune_get("ntt_block_log")
+    x0 = _random_rows(ctx, rows, 0, ctx.q_count)
+    ms, want = {}, None
+    try:
+        for v in [v for v in NTT_BLOCK_LOGS if v < ctx.log_n or v == 14]:
+            ctx.tune_set("ntt_block_log", v)
+            y = x0.clone()
+            ctx.ntt_fwd(y, 0, ctx.q_count)
+            torch.cuda.synchronize()
+            if want is None:
+                want = y.clone()
+            elif not torch.equal(y, want):
+                raise RuntimeError(f"NTT split {v} changed the transform")
+            ctx.ntt_inv(y, 0, ctx.q_count)
+            torch.cuda.synchronize()
+            if not torch.equal(y, x0):
+                raise RuntimeError(f"NTT split {v} broke the round trip")
+
+            def step():
+                ctx.ntt_fwd(y, 0, ctx.q_count)
+                ctx.ntt_inv(y, 0, ctx.q_count)
+            ms[v] = round(time_ms(step, reps), 4)
+    finally:
+        ctx.tune_set("ntt_block_log", keep)
+    best = min(ms, key=ms.get)
+    return {"ntt_block_log": best, "ms": {str(k): v for k, v in ms.items()}}
+
+
+def _random_pairs(ctx, pairs: int, seed: int):
+    import torch
+    rows = pairs * 2 * ctx.q_count
+    return _random_rows(ctx, rows, 0, ctx.q_count, seed).view(pairs, 2, ctx.q_count, ctx.N)
+
+
+def tune_branches(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
+    """Sub-batches of the batched multiply (hybrid key switch)."""
+    import torch
+
+    from .api import Ciphertext
+    ctx = scheme.context
+    keep = ctx.tune_get("branches")
+    c1 = Ciphertext(ctx, _random_pairs(ctx, pairs, 2))
+    c2 = Ciphertext(ctx, _random_pairs(ctx, pairs, 3))
+    out = Ciphertext(ctx, count=pairs)
+    ms, want = {}, None
+    try:
+        for b in BRANCHES:
+            ctx.tune_set("branches", b)
+            scheme.mult_relin(c1, c2, out=out)
+            torch.cuda.synchronize()
+            if want is None:
+                want = out.cipher_device.clone()
+            elif not torch.equal(out.cipher_device, want):
+                raise RuntimeError(f"{b} sub-batches changed the product")
+            ms[b] = round(time_ms(lambda: scheme.mult_relin(c1, c2, out=out), reps), 4)
+    finally:
+        ctx.tune_set("branches", keep)
+    best = min(ms, key=ms.get)
+    return {"branches": best, "ms": {str(k): v for k, v in ms.items()}}
+
+
+def tune_host_chunk(scheme, pairs: int = 64, reps: int = 3) -> Dict[str, object]:
+    """Pairs per chunk of the host-memory multiply (page-locked buffers)."""
+    import torch
+    ctx = scheme.context
+    h_a = _random_pairs(ctx, pairs, 4).cpu().pin_memory()
+    h_b = _random_pairs(ctx, pairs, 5).cpu().pin_memory()
+    h_o = torch.empty_like(h_a).pin_memory()
+    ms, want = {}, None
+    for ch in HOST_CHUNKS:
+        if ch > pairs:
+            continue
+        scheme.mult_relin_host(h_a, h_b, out=h_o, chunk_pairs=ch)
+        if want is None:
+            want = h_o.clone()
+        elif not torch.equal(h_o, want):
+            raise RuntimeError(f"host chunk {ch} changed the product")
+        ms[ch] = round(time_ms(lambda: scheme.mult_relin_host(h_a, h_b, out=h_o, chunk_pairs=ch,
+                                                              synchronize=False), reps), 4)
+    if not ms:
+        return {"host_chunk": 0, "ms": {}}
+    best = min(ms, key=ms.get)
+    return {"host_chunk": best, "ms": {str(k): v for k, v in ms.items()}}
+
+
+def apply_choice(ctx, choice: dict) -> None:
+    for knob in ("ntt_block_log", "branches", "host_chunk"):
+        if knob in choice:
+            ctx.tune_set(knob, int(choice[knob]))
+
+
+def autotune(ctx, scheme=None, pairs: int = 64, cache_path: Optional[str] = DEFAULT_CACHE, force: bool = False,
+             ntt_rows: int = 512, host: bool = True) -> dict:
+    """Pick every knob for `ctx` (the multiply knobs need `scheme` with a
+    relinearisation key), apply the choice and store it in the cache. A cached
+    choice for the same device and parameter set is applied without timing
+    unless `force`."""
+    key = context_key(ctx, pairs)
+    if cache_path and not force:
+        hit = load_cache(cache_path).get(key)
+        if hit is not None:
+            apply_choice(ctx, hit)
+            return dict(hit, cached=True)
+    choice: Dict[str, object] = {}
+    r = tune_ntt(ctx, ntt_rows)
+    choice["ntt_block_log"], choice["ntt_ms"] = r["ntt_block_log"], r["ms"]
+    if scheme is not None and scheme.rlk is not None and scheme.relin == "hybrid":
+        r = tune_branches(scheme, pairs)
+        choice["branches"], choice["branches_ms"] = r["branches"], r["ms"]
+        if host:
+            r = tune_host_chunk(scheme, pairs)
+            choice["host_chunk"], choice["host_chunk_ms"] = r["host_chunk"], r["ms"]
+    apply_choice(ctx, choice)
+    if cache_path:
+        save_cache({key: choice}, cache_path)
+    return dict(choice, cached=False)
+
+
+def apply_cached(ctx, pairs: int = 64, cache_path: str = DEFAULT_CACHE) -> Optional[dict]:
+    """Apply a stored choice for this device and parameter set, if any."""
+    hit = load_cache(cache_path).get(context_key(ctx, pairs))
+    if hit is not None:
+        apply_choice(ctx, hit)
+    return hit

@@ -1,0 +1,71 @@
+"""The tuning knobs and the autotuner (kunpbfv_b200.tune): every radix split of
+the standalone NTT on rings of 2^13-2^16 points gives the oracle's transform, every
+sub-batch count and host chunk gives the same product, and the tuner applies
+and caches its choice."""
+import numpy as np
+import pytest
+
+from tests.gpu_util import dev, host, rand_rows, small_pair
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("log_n", [13, 14, 15, 16])
+def test_ntt_splits_match_oracle(log_n):
+    ctx, orc = small_pair(log_n=log_n, nq=2, np_=1, bits=60)
+    rows = 6
+    x = np.concatenate([rand_rows(orc, [0, 1], ctx.N, seed=s) for s in range(rows // 2)])
+    want = np.concatenate([orc.ntt_fwd(r % 2, x[r:r + 1]) for r in range(rows)])
+    try:
+        for v in (12, 13, 14):
+            ctx.tune_set("ntt_block_log", v)
+            assert ctx.tune_get("ntt_block_log") == v
+            y = dev(x)
+            ctx.ntt_fwd(y, 0, 2)
+            assert np.array_equal(host(y), want), v
+            ctx.ntt_inv(y, 0, 2)
+            assert np.array_equal(host(y), x), v
+    finally:
+        ctx.tune_set("ntt_block_log", 14)
+
+
+def test_knob_bounds():
+    import kunpbfv_b200 as kb
+    ctx, _ = small_pair()
+    for knob, bad in (("ntt_block_log", 11), ("ntt_block_log", 15), ("branches", 0), ("branches", 5),
+                      ("host_chunk", -1), ("host_chunk", 129)):
+        with pytest.raises(kb.KbfvError):
+            ctx.tune_set(knob, bad)
+    assert ctx.tune_get("branches") == 2 and ctx.tune_get("host_chunk") == 0
+
+
+def test_autotune_applies_and_caches(tmp_path):
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200 import tune
+    ctx = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
+    sk = kb.SecretKey(ctx, b"\x21" * 32)
+    sch = kb.BFVScheme(ctx, b"\x22" * 32)
+    sch.addMultKey_23(sk)
+    cache = str(tmp_path / "tune.json")
+    got = tune.autotune(ctx, sch, pairs=32, cache_path=cache)
+    assert not got["cached"]
+    assert got["branches"] in tune.BRANCHES and got["host_chunk"] in tune.HOST_CHUNKS
+    assert ctx.tune_get("branches") == got["branches"]
+    assert ctx.tune_get("host_chunk") == got["host_chunk"]
+    assert set(got["branches_ms"]) == {str(b) for b in tune.BRANCHES}
+    # a fresh context of the same parameters takes the cached choice without timing
+    ctx2 = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
+    hit = tune.autotune(ctx2, None, pairs=32, cache_path=cache)
+    assert hit["cached"] and ctx2.tune_get("branches") == got["branches"]
+    assert tune.apply_cached(ctx2, pairs=32, cache_path=cache)["host_chunk"] == got["host_chunk"]
+
+
+def test_autotune_ntt_split_large_ring(tmp_path):
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200 import tune
+    ctx, _ = small_pair(log_n=16, nq=2, np_=1, bits=60)
+    got = tune.autotune(ctx, None, cache_path=str(tmp_path / "t.json"), ntt_rows=64)
+    assert got["ntt_block_log"] in tune.NTT_BLOCK_LOGS
+    assert ctx.tune_get("ntt_block_log") == got["ntt_block_log"]
+    assert set(got["ntt_ms"]) == {"12", "13", "14"}
+    ctx.tune_set("ntt_block_log", 14)
