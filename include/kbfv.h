@@ -243,9 +243,9 @@ int kbfv_set_branches(kbfv_context* ctx, uint32_t branches);
  * caches the choice per device and parameter set. No counterpart in the
  * reference (its shapes are fixed at compile time). */
 typedef enum {
-    KBFV_TUNE_NTT_BLOCK_LOG = 0, /* 12..14 (default 14): kbfv_ntt_fwd/inv on rings above 2^v
-                                    points run as a column pass of log_n - v stages and blocks of
-                                    2^v points (14: one block per ring up to 2^14) */
+    KBFV_TUNE_NTT_BLOCK_LOG = 0, /* 0 (default: built-in shapes) or 12..14: kbfv_ntt_fwd/inv on
+                                    rings above 2^v points run as a column pass of log_n - v
+                                    stages and blocks of 2^v points */
     KBFV_TUNE_BRANCHES = 1,      /* 1..4 (default 2): sub-batches of a batched multiply */
     KBFV_TUNE_HOST_CHUNK = 2     /* 0..128 (default 0 = ~32 MiB of inputs): pairs per chunk of
                                     kbfv_mul_relin_host when its chunk_pairs is 0 */

@@ -118,7 +118,7 @@ struct Context {
     // tuning knobs (kbfv_tune_set): block size 2^ntt_block_log of the standalone
     // NTT on rings above it (the rest runs as a column pass of logn - ntt_block_log
     // stages); pairs per chunk of the host-memory multiply (0: by bytes)
-    int ntt_block_log = 14;
+    int ntt_block_log = 0;  // 0: built-in shapes
     int host_chunk = 0;
     cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};

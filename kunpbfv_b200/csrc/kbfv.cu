@@ -520,9 +520,10 @@ template <class Dst>
 static inline Dst plain_of(const Dst& d) { return d; }
 
 // Forward NTT of `rows` rows read through `s` and written through `d`.
-// For logn <= 14 one block kernel; for 15/16 a column pass (s -> plain_of(d))
-// then the block kernel from plain_of(d) to d in place (d must also be
-// readable). FULL = false leaves outputs in [0, 8q) for consumers that reduce
+// For logn <= 14 one block kernel; for 15/16 a radix-8/16 column pass
+// (s -> plain_of(d)) then 2^12-point block kernels from plain_of(d) to d in
+// place (d must also be readable): several 256-thread CTAs per SM run faster
+// than one 1024-thread CTA per 2^14-point block. FULL = false leaves outputs in [0, 8q) for consumers that reduce
 // anyway (pipeline stages only).
 template <class Src, class Dst, bool FULL = true>
 static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st) {
@@ -534,19 +535,19 @@ static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 13: launch_fwd_block<13, Src, Dst, FULL>(dc, s, d, rows, 13, st); break;
         case 14: launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st); break;
         case 15: {
-            const size_t total = (size_t)rows << 14;
+            const size_t total = (size_t)rows << 12;
             using DP = decltype(plain_of(d));
             const DP dp = plain_of(d);
-            ntt_fwd_col_kernel<1, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 15, total);
-            launch_fwd_block<14, DP, Dst, FULL>(dc, dp, d, rows, 15, st);
+            ntt_fwd_col_kernel<3, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 15, total);
+            launch_fwd_block<12, DP, Dst, FULL>(dc, dp, d, rows, 15, st);
             break;
         }
         case 16: {
-            const size_t total = (size_t)rows << 14;
+            const size_t total = (size_t)rows << 12;
             using DP = decltype(plain_of(d));
             const DP dp = plain_of(d);
-            ntt_fwd_col_kernel<2, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
-            launch_fwd_block<14, DP, Dst, FULL>(dc, dp, d, rows, 16, st);
+            ntt_fwd_col_kernel<4, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
+            launch_fwd_block<12, DP, Dst, FULL>(dc, dp, d, rows, 16, st);
             break;
         }
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
@@ -564,15 +565,15 @@ static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 13: launch_inv_block<13, Src, Dst, true>(dc, s, d, rows, 13, st); break;
         case 14: launch_inv_block<14, Src, Dst, true>(dc, s, d, rows, 14, st); break;
         case 15: {
-            launch_inv_block<14, Src, Dst, false>(dc, s, d, rows, 15, st);
-            const size_t total = (size_t)rows << 14;
-            ntt_inv_col_kernel<1, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 15, total);
+            launch_inv_block<12, Src, Dst, false>(dc, s, d, rows, 15, st);
+            const size_t total = (size_t)rows << 12;
+            ntt_inv_col_kernel<3, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 15, total);
             break;
         }
         case 16: {
-            launch_inv_block<14, Src, Dst, false>(dc, s, d, rows, 16, st);
-            const size_t total = (size_t)rows << 14;
-            ntt_inv_col_kernel<2, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
+            launch_inv_block<12, Src, Dst, false>(dc, s, d, rows, 16, st);
+            const size_t total = (size_t)rows << 12;
+            ntt_inv_col_kernel<4, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
             break;
         }
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");
@@ -586,7 +587,7 @@ static inline RowsIO rows_io(const DevConsts& dc, uint64_t* base, int p0, int pe
 
 // Standalone NTT of plain rows with a chosen radix split for rings above 2^lb:
 // a column pass of logn - lb stages (forward: first; inverse: last) and block
-// kernels of 2^lb points, lb in 12..14 (14: the default shapes).
+// kernels of 2^lb points, lb in 12..14 (0: the built-in shapes of ntt_fwd/inv).
 template <int RC, int LB>
 static void ntt_rows_split(const DevConsts& dc, RowsIO io, int rows, bool fwd, cudaStream_t st) {
     const size_t total = (size_t)rows << LB;
@@ -605,7 +606,7 @@ static void ntt_rows(const Context& c, RowsIO io, int rows, bool fwd, cudaStream
     const DevConsts& dc = c.dc;
     if (rows <= 0) return;
     const int lb = c.ntt_block_log;
-    if (lb >= dc.logn || lb == 14) {
+    if (lb == 0 || lb >= dc.logn) {  // built-in shapes
         if (fwd) ntt_fwd(dc, io, io, rows, st);
         else ntt_inv(dc, io, io, rows, st);
         return;
@@ -614,10 +615,12 @@ static void ntt_rows(const Context& c, RowsIO io, int rows, bool fwd, cudaStream
         case 1312: ntt_rows_split<1, 12>(dc, io, rows, fwd, st); break;
         case 1412: ntt_rows_split<2, 12>(dc, io, rows, fwd, st); break;
         case 1413: ntt_rows_split<1, 13>(dc, io, rows, fwd, st); break;
-        case 1513: ntt_rows_split<2, 13>(dc, io, rows, fwd, st); break;
         case 1512: ntt_rows_split<3, 12>(dc, io, rows, fwd, st); break;
-        case 1613: ntt_rows_split<3, 13>(dc, io, rows, fwd, st); break;
+        case 1513: ntt_rows_split<2, 13>(dc, io, rows, fwd, st); break;
+        case 1514: ntt_rows_split<1, 14>(dc, io, rows, fwd, st); break;
         case 1612: ntt_rows_split<4, 12>(dc, io, rows, fwd, st); break;
+        case 1613: ntt_rows_split<3, 13>(dc, io, rows, fwd, st); break;
+        case 1614: ntt_rows_split<2, 14>(dc, io, rows, fwd, st); break;
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported NTT split");
     }
 }
@@ -2036,7 +2039,8 @@ int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
         Context& c = CX(ctx);
         switch (knob) {
             case KBFV_TUNE_NTT_BLOCK_LOG:
-                KB_REQUIRE(value >= 12 && value <= 14, KBFV_ERR_INVALID, "NTT block log must be 12..14");
+                KB_REQUIRE(value == 0 || (value >= 12 && value <= 14), KBFV_ERR_INVALID,
+                           "NTT block log must be 0 (built-in) or 12..14");
                 c.ntt_block_log = (int)value;
                 break;
             case KBFV_TUNE_BRANCHES:

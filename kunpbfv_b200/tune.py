@@ -4,7 +4,7 @@ Knobs (include/kbfv.h, ``kbfv_tune_knob``):
 
 * ``ntt_block_log`` - the radix split of the standalone NTT on rings above
   2^v points: a column pass of ``log_n - v`` stages and block kernels of 2^v
-  points, v in 12..14;
+  points, v in 12..14, or 0 for the built-in shapes;
 * ``branches`` - sub-batches (one stream each) of a batched multiply, 1..4;
 * ``host_chunk`` - pairs per chunk of the host-memory multiply, 0..128.
 
@@ -26,7 +26,7 @@ from typing import Callable, Dict, Optional
 DEFAULT_CACHE = os.environ.get("KBFV_TUNE_CACHE",
                                os.path.join(os.path.expanduser("~"), ".cache", "kunpbfv_b200", "tune.json"))
 
-NTT_BLOCK_LOGS = (12, 13, 14)
+NTT_BLOCK_LOGS = (0, 12, 13, 14)  # 0: built-in shapes
 BRANCHES = (1, 2, 3, 4)
 HOST_CHUNKS = (4, 8, 12, 16, 24)
 
@@ -94,12 +94,12 @@ def tune_ntt(ctx, rows: int = 512, reps: int = 5) -> Dict[str, object]:
     """Radix split of the standalone forward + inverse NTT over `rows` rows."""
     import torch
     if ctx.log_n <= 12:
-        return {"ntt_block_log": 14, "ms": {}}
+        return {"ntt_block_log": 0, "ms": {}}
     keep = ctx.tune_get("ntt_block_log")
     x0 = _random_rows(ctx, rows, 0, ctx.q_count)
     ms, want = {}, None
     try:
-        for v in [v for v in NTT_BLOCK_LOGS if v < ctx.log_n or v == 14]:
+        for v in [v for v in NTT_BLOCK_LOGS if v < ctx.log_n]:
             ctx.tune_set("ntt_block_log", v)
             y = x0.clone()
             ctx.ntt_fwd(y, 0, ctx.q_count)

@@ -17,7 +17,7 @@ def test_ntt_splits_match_oracle(log_n):
     x = np.concatenate([rand_rows(orc, [0, 1], ctx.N, seed=s) for s in range(rows // 2)])
     want = np.concatenate([orc.ntt_fwd(r % 2, x[r:r + 1]) for r in range(rows)])
     try:
-        for v in (12, 13, 14):
+        for v in (0, 12, 13, 14):
             ctx.tune_set("ntt_block_log", v)
             assert ctx.tune_get("ntt_block_log") == v
             y = dev(x)
@@ -26,17 +26,18 @@ def test_ntt_splits_match_oracle(log_n):
             ctx.ntt_inv(y, 0, 2)
             assert np.array_equal(host(y), x), v
     finally:
-        ctx.tune_set("ntt_block_log", 14)
+        ctx.tune_set("ntt_block_log", 0)
 
 
 def test_knob_bounds():
     import kunpbfv_b200 as kb
     ctx, _ = small_pair()
-    for knob, bad in (("ntt_block_log", 11), ("ntt_block_log", 15), ("branches", 0), ("branches", 5),
-                      ("host_chunk", -1), ("host_chunk", 129)):
+    for knob, bad in (("ntt_block_log", 11), ("ntt_block_log", 15), ("ntt_block_log", 1), ("branches", 0),
+                      ("branches", 5), ("host_chunk", -1), ("host_chunk", 129)):
         with pytest.raises(kb.KbfvError):
             ctx.tune_set(knob, bad)
     assert ctx.tune_get("branches") == 2 and ctx.tune_get("host_chunk") == 0
+    assert ctx.tune_get("ntt_block_log") == 0
 
 
 def test_autotune_applies_and_caches(tmp_path):
@@ -67,5 +68,5 @@ def test_autotune_ntt_split_large_ring(tmp_path):
     got = tune.autotune(ctx, None, cache_path=str(tmp_path / "t.json"), ntt_rows=64)
     assert got["ntt_block_log"] in tune.NTT_BLOCK_LOGS
     assert ctx.tune_get("ntt_block_log") == got["ntt_block_log"]
-    assert set(got["ntt_ms"]) == {"12", "13", "14"}
-    ctx.tune_set("ntt_block_log", 14)
+    assert set(got["ntt_ms"]) == {"0", "12", "13", "14"}
+    ctx.tune_set("ntt_block_log", 0)
