@@ -519,8 +519,17 @@ static void launch_inv_block(const DevConsts& dc, Src s, Dst d, int rows, int lo
 template <class Dst>
 static inline Dst plain_of(const Dst& d) { return d; }
 
+// At N = 2^14, launches of at most this many rows (fewer 1024-thread CTAs
+// than SMs, e.g. one ciphertext pair per call: 2-45 rows) run as a radix-4
+// column pass and 2^12-point blocks: four times the CTAs cover the SMs, 15-23 us
+// instead of 29-31 us per launch of 8-45 rows on the B200. At 64 rows the
+// split alone is still faster, but beside a concurrent sub-batch it cost the
+// batched multiply ~1%, so 64-row launches keep the whole-ring blocks.
+constexpr int kSplitRows14 = 48;
+
 // Forward NTT of `rows` rows read through `s` and written through `d`.
-// For logn <= 14 one block kernel; for 15/16 a radix-8/16 column pass
+// For logn <= 14 one block kernel (N = 2^14 with at most kSplitRows14 rows:
+// as for 15/16 with a radix-4 column pass); for 15/16 a radix-8/16 column pass
 // (s -> plain_of(d)) then 2^12-point block kernels from plain_of(d) to d in
 // place (d must also be readable): several 256-thread CTAs per SM run faster
 // than one 1024-thread CTA per 2^14-point block. FULL = false leaves outputs in [0, 8q) for consumers that reduce
@@ -533,7 +542,18 @@ static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 11: launch_fwd_block<11, Src, Dst, FULL>(dc, s, d, rows, 11, st); break;
         case 12: launch_fwd_block<12, Src, Dst, FULL>(dc, s, d, rows, 12, st); break;
         case 13: launch_fwd_block<13, Src, Dst, FULL>(dc, s, d, rows, 13, st); break;
-        case 14: launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st); break;
+        case 14: {
+            if (rows > kSplitRows14) {
+                launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st);
+                break;
+            }
+            const size_t total = (size_t)rows << 12;
+            using DP = decltype(plain_of(d));
+            const DP dp = plain_of(d);
+            ntt_fwd_col_kernel<2, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 14, total);
+            launch_fwd_block<12, DP, Dst, FULL>(dc, dp, d, rows, 14, st);
+            break;
+        }
         case 15: {
             const size_t total = (size_t)rows << 12;
             using DP = decltype(plain_of(d));
@@ -563,7 +583,16 @@ static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 11: launch_inv_block<11, Src, Dst, true>(dc, s, d, rows, 11, st); break;
         case 12: launch_inv_block<12, Src, Dst, true>(dc, s, d, rows, 12, st); break;
         case 13: launch_inv_block<13, Src, Dst, true>(dc, s, d, rows, 13, st); break;
-        case 14: launch_inv_block<14, Src, Dst, true>(dc, s, d, rows, 14, st); break;
+        case 14: {
+            if (rows > kSplitRows14) {
+                launch_inv_block<14, Src, Dst, true>(dc, s, d, rows, 14, st);
+                break;
+            }
+            launch_inv_block<12, Src, Dst, false>(dc, s, d, rows, 14, st);
+            const size_t total = (size_t)rows << 12;
+            ntt_inv_col_kernel<2, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 14, total);
+            break;
+        }
         case 15: {
             launch_inv_block<12, Src, Dst, false>(dc, s, d, rows, 15, st);
             const size_t total = (size_t)rows << 12;
