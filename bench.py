@@ -446,6 +446,56 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     res["per_op_split"] = {"value": round(BATCH / (ms_split / 1e3), 2), "unit": "ct/s",
                            "form": "one pair per call, multiply then relinearise as separate calls, no graph"}
 
+    # the plain one-op-per-launch form: the HPS tensor composed from the
+    # building-block entry points (INTT, base conversion, NTT, tensor, INTT,
+    # scale-and-round, base conversion, NTT; one kernel each, about 20 launches
+    # and 6 device copies per pair), then kbfv_relinearize; one pair per call
+    from kunpbfv_b200.api import _ptr, lib
+    NR, NQR = ctx.r_count, NQ + ctx.r_count
+    L = lib()
+    sp = stream.cuda_stream
+    x4 = torch.empty(4, NQ, N, dtype=torch.int64, device=dev)
+    r4 = torch.empty(4, NR, N, dtype=torch.int64, device=dev)
+    qr = torch.empty(2, 2, NQR, N, dtype=torch.int64, device=dev)
+    tz = torch.empty(3, NQR, N, dtype=torch.int64, device=dev)
+    sr = torch.empty(3, NR, N, dtype=torch.int64, device=dev)
+    d3 = torch.empty(3, NQ, N, dtype=torch.int64, device=dev)
+    po = torch.empty(2, NQ, N, dtype=torch.int64, device=dev)
+
+    def plain_pair(i):
+        A, B = a1[i].view(2, NQ, N), b1[i].view(2, NQ, N)
+        x4[:2].copy_(A)
+        x4[2:].copy_(B)
+        L.kbfv_ntt_inv(ctx.handle, _ptr(x4), 4 * NQ, 0, NQ, sp)
+        L.kbfv_bconv_q_to_r(ctx.handle, _ptr(x4), _ptr(r4), 4, sp)
+        L.kbfv_ntt_fwd(ctx.handle, _ptr(r4), 4 * NR, ctx.idx_r, NR, sp)
+        qr[0, :, :NQ].copy_(A)
+        qr[1, :, :NQ].copy_(B)
+        qr[:, :, NQ:].copy_(r4.view(2, 2, NR, N))
+        L.kbfv_tensor_qr(ctx.handle, _ptr(qr[0]), _ptr(qr[1]), _ptr(tz), 1, sp)
+        for k in range(3):
+            L.kbfv_ntt_inv(ctx.handle, _ptr(tz[k]), NQ, 0, NQ, sp)
+            L.kbfv_ntt_inv(ctx.handle, _ptr(tz[k, NQ:]), NR, ctx.idx_r, NR, sp)
+        L.kbfv_scale_round_qr_r(ctx.handle, _ptr(tz), _ptr(sr), 3, sp)
+        L.kbfv_bconv_r_to_q(ctx.handle, _ptr(sr), _ptr(d3), 3, sp)
+        L.kbfv_ntt_fwd(ctx.handle, _ptr(d3), 3 * NQ, 0, NQ, sp)
+        L.kbfv_relinearize(ctx.handle, _ptr(sch.rlk), _ptr(d3), _ptr(po), 1, sp)
+
+    def per_op_plain():
+        with torch.cuda.stream(stream):
+            for i in range(BATCH):
+                plain_pair(i)
+
+    with torch.cuda.stream(stream):
+        plain_pair(0)
+    torch.cuda.synchronize()
+    if not torch.equal(po.view(-1), o1[0]):
+        raise RuntimeError("the building-block multiply differs from the fused one")
+    ms_plain = time_cuda(per_op_plain, stream, 3)
+    res["per_op_plain"] = {"value": round(BATCH / (ms_plain / 1e3), 2), "unit": "ct/s",
+                           "form": "one pair per call, one kernel per building block (about 25 launches and "
+                                   "6 device copies per pair), no graph"}
+
     # e2e through the C ABI with page-locked host buffers: kbfv_mul_relin_host
     # copies each chunk in, multiplies it and copies its products out, the
     # copies of one chunk overlapping the multiply of its neighbours
