@@ -79,7 +79,9 @@ const char* kbfv_version(void);
  * independent register chains, no memory traffic. kind 0: 64x64->128
  * multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64, 3: forward NTT butterfly,
  * 4: Shoup product, 5: 128-bit Barrett, 6: one-high-product Barrett,
- * 7: 32x32->64 multiply-add. The roofline of the IMAD-bound kernels. */
+ * 7: 32x32->64 multiply-add, 8: 32x32 high product, 9: 32-bit multiply-add,
+ * 10: 64x64->128 multiply-accumulate from 32-bit partial products with carry
+ * chains. The roofline of the IMAD-bound kernels. */
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops);
 
 /* ---- context ---------------------------------------------------------

@@ -1357,7 +1357,9 @@ static void require_klss(const Context& c) {
 // ---- arithmetic-rate probe: independent register chains of one primitive -------
 // kind 0: 64x64->128 multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64,
 // 3: forward butterfly (approximate-quotient Shoup), 4: fully reduced Shoup,
-// 5: 128-bit Barrett, 6: one-high-product Barrett, 7: 32x32->64 multiply-add.
+// 5: 128-bit Barrett, 6: one-high-product Barrett, 7: 32x32->64 multiply-add,
+// 8: 32x32 high product, 9: 32-bit multiply-add, 10: mac32 (64x64->128
+// multiply-accumulate from 32-bit partial products).
 constexpr int kProbeChains = 8;
 template <int KIND>
 __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_t mh, uint64_t ml, uint64_t mp) {
@@ -1373,7 +1375,7 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
     for (int it = 0; it < iters; it++) {
 #pragma unroll
         for (int c = 0; c < kProbeChains; c++) {
-            if (KIND == 0) mac(acc[c], a[c], b[c]);
+            if (KIND == 0) mac64(acc[c], a[c], b[c]);
             if (KIND == 1) acc[c].lo += a[c] * b[c];
             if (KIND == 2) acc[c].lo += __umul64hi(a[c], b[c]);
             if (KIND == 3) {
@@ -1385,6 +1387,9 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
             if (KIND == 5) acc[c].lo += barrett128(u128{a[c], b[c] >> 4}, q, mh, ml);
             if (KIND == 6) acc[c].lo += barrett_prod(mul_wide(a[c], b[c]), q, mp);
             if (KIND == 7) acc[c].lo += (uint64_t)(uint32_t)a[c] * (uint32_t)b[c];
+            if (KIND == 8) acc[c].lo += __umulhi((uint32_t)a[c], (uint32_t)b[c]);
+            if (KIND == 9) acc[c].lo = (uint32_t)a[c] * (uint32_t)b[c] + (uint32_t)acc[c].lo;
+            if (KIND == 10) mac32(acc[c], a[c], b[c]);
             a[c] = (a[c] + (acc[c].lo & 15)) & 0x0fffffffffffffffULL;
         }
     }
@@ -2702,7 +2707,7 @@ int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_
 
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
     return guarded([&] {
-        KB_REQUIRE(kind >= 0 && kind <= 7 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
+        KB_REQUIRE(kind >= 0 && kind <= 10 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
         int dev = 0, sms = 0;
         KB_CHECK_CUDA(cudaGetDevice(&dev));
         KB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -2721,7 +2726,7 @@ int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
             KB_CHECK_CUDA(cudaEventRecord(e0));
             switch (kind) {
 #define P_K(K) case K: probe_arith_kernel<K><<<blocks, threads>>>(out, (int)iters, q, mh, ml, mp); break;
-                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7)
+                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7) P_K(8) P_K(9) P_K(10)
 #undef P_K
             }
             KB_CHECK_CUDA(cudaEventRecord(e1));
