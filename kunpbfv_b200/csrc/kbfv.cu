@@ -513,7 +513,7 @@ static void launch_inv_block(const DevConsts& dc, Src s, Dst d, int rows, int lo
         s, d, dc.tw_inv, dc.mods, logn);
 }
 
-// The view of a store target that the column pass of rings above 2^14 writes
+// The view of a store target that the column pass of a split transform writes
 // and the block kernel reads back: the target itself, unless its store adds an
 // epilogue (an overload for that target returns its plain rows).
 template <class Dst>
@@ -1022,7 +1022,7 @@ struct OutCtKeyDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
         return r;
     }
 };
-// the column pass of rings above 2^14 writes plain values; only the block
+// the column pass of a split transform writes plain values; only the block
 // kernel's final store runs the epilogue
 static inline OutCtDst plain_of(const OutCtKeyDst& d) { return OutCtDst{d.pb, d.dc.logn, d.dc.nq}; }
 
@@ -1142,9 +1142,10 @@ struct TensorA2 {
     }
 };
 
-// Fused stages run as one block kernel for N <= 2^14; for N = 2^15, 2^16 the
-// fused loader feeds the column pass and the fused store target is read back
-// by the block kernel, which every functor here supports.
+// Fused stages run as one block kernel for N <= 2^14; for split transforms
+// (N = 2^15, 2^16, and launches of few rows at 2^14) the fused loader feeds
+// the column pass and the store target is read back by the block kernel, which
+// every functor here supports.
 static void require_batchable(const Context& c) {
     KB_REQUIRE(c.logn >= 10 && c.logn <= 16, KBFV_ERR_UNSUPPORTED, "ring degree outside 2^10..2^16");
 }

@@ -8,9 +8,10 @@
 // Shape: one CTA transforms one block of 2^LOGB points held in shared memory
 // (N = 2^14 -> 1024 threads x 16 points, 136 KiB of padded smem). Each thread
 // runs register groups of 16 points through 4 butterfly stages between
-// shared-memory exchanges (N = 2^14: stages 4 + 4 + 4 + 2, three exchanges). Larger rings (2^15, 2^16)
-// add one elementwise radix-2/4 column pass in front of (forward) or behind
-// (inverse) the block kernels. Moduli must be below 2^60 (lazy range 8q < 2^63).
+// shared-memory exchanges (N = 2^14: stages 4 + 4 + 4 + 2, three exchanges). Larger rings (2^15, 2^16),
+// and launches of few rows at 2^14, add one elementwise radix-2^RC column pass in
+// front of (forward) or behind (inverse) 2^12-point block kernels (the launch
+// code picks the split). Moduli must be below 2^60 (lazy range 8q < 2^63).
 //
 // Rows are described by Src/Dst functors: src.prime(row) and
 // src.bind(row) -> {load(j), store(j, v)}. This lets pipeline stages fuse their per-element
