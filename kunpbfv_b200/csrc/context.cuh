@@ -130,6 +130,9 @@ struct Context {
     cudaEvent_t hin[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t hcomp[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t hout[4] = {nullptr, nullptr, nullptr, nullptr};
+    // batches of pairs at several levels: one lane (stream) per level group
+    cudaStream_t lane[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t lane_fork = nullptr, lane_join[3] = {nullptr, nullptr, nullptr};
 };
 
 }  // namespace kbfv

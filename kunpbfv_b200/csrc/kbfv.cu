@@ -1482,6 +1482,11 @@ int kbfv_context_destroy(kbfv_context* ctx) {
                 if (e) cudaEventDestroy(e);
         }
         if (c.hfork) cudaEventDestroy(c.hfork);
+        for (int i = 0; i < 3; i++) {
+            if (c.lane[i]) cudaStreamDestroy(c.lane[i]);
+            if (c.lane_join[i]) cudaEventDestroy(c.lane_join[i]);
+        }
+        if (c.lane_fork) cudaEventDestroy(c.lane_fork);
         delete ctx;
     });
 }
@@ -2596,7 +2601,25 @@ int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32
             KB_REQUIRE(live_q[i] >= 1 && live_q[i] <= (uint32_t)c.nq, KBFV_ERR_LEVEL, "live prime count out of range");
             groups[live_q[i]].push_back(i);
         }
-        for (auto it = groups.rbegin(); it != groups.rend(); ++it) {  // highest level first
+        // the level groups run concurrently: the first on the caller's stream, the
+        // next ones on the context's lane streams (forked from and joined back into
+        // the caller's stream); each level context has its own scratch arena
+        cudaStream_t st = S(stream);
+        const int ng = (int)groups.size();
+        const int lanes = std::min(ng, 4);
+        if (lanes > 1) {
+            if (!c.lane_fork) {
+                for (int k = 0; k < 3; k++) {
+                    KB_CHECK_CUDA(cudaStreamCreateWithFlags(&c.lane[k], cudaStreamNonBlocking));
+                    KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.lane_join[k], cudaEventDisableTiming));
+                }
+                KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.lane_fork, cudaEventDisableTiming));
+            }
+            KB_CHECK_CUDA(cudaEventRecord(c.lane_fork, st));
+            for (int k = 1; k < lanes; k++) KB_CHECK_CUDA(cudaStreamWaitEvent(c.lane[k - 1], c.lane_fork, 0));
+        }
+        int g = 0;
+        for (auto it = groups.rbegin(); it != groups.rend(); ++it, ++g) {  // highest level first
             kbfv_context* lv = nullptr;
             int rc = kbfv_context_at_level(ctx, it->first, &lv);
             if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
@@ -2607,8 +2630,14 @@ int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32
                 B.push_back(ct_b[i]);
                 O.push_back(out[i]);
             }
-            rc = kbfv_mul_relin_batch(lv, d_rlk, A.data(), B.data(), O.data(), (uint32_t)A.size(), stream);
+            const int lane = g % lanes;
+            cudaStream_t ls = lane == 0 ? st : c.lane[lane - 1];
+            rc = kbfv_mul_relin_batch(lv, d_rlk, A.data(), B.data(), O.data(), (uint32_t)A.size(), (kbfv_stream)ls);
             if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+        }
+        for (int k = 1; k < lanes; k++) {
+            KB_CHECK_CUDA(cudaEventRecord(c.lane_join[k - 1], c.lane[k - 1]));
+            KB_CHECK_CUDA(cudaStreamWaitEvent(st, c.lane_join[k - 1], 0));
         }
     });
 }
