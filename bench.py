@@ -54,7 +54,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
     ap.add_argument("--serve-rates", default="500,1000,2000,3000,4000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
-    ap.add_argument("--serve-seconds", type=float, default=2.5, help="arrival window per rate")
+    ap.add_argument("--serve-seconds", type=float, default=2.5,
+                    help="shortest arrival window per rate (longer where needed for --serve-requests)")
+    ap.add_argument("--serve-requests", type=int, default=10000,
+                    help="requests offered per rate point at least (window = max(seconds, requests / rate))")
     ap.add_argument("--serving-only", action="store_true", help="run only the serving sweep and print it")
     return ap.parse_args()
 
@@ -594,7 +597,8 @@ def serving(args):
     with Server(rings, hbm_budget_bytes=24 << 30, max_batch=64, pinned_bytes=2 << 30) as srv:
         run_open_loop(srv, w, rate=200.0, duration_s=0.5, seed=99)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
-            pt = run_open_loop(srv, w, rate=rate, duration_s=args.serve_seconds, seed=100 + i,
+            window = max(args.serve_seconds, args.serve_requests / rate)
+            pt = run_open_loop(srv, w, rate=rate, duration_s=window, seed=100 + i,
                                enc_base=(i + 1) << 36)
             points.append(pt)
         st = srv.stats()
