@@ -398,8 +398,10 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
  * cudaFree or any allocating routine. All calls share the one array: calls
  * that overlap on the GPU (several streams or contexts) race and must be
  * serialised by the caller. The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress); make that first call outside any
- * stream capture. The context's device must be current. */
+ * device address (cudaGetSymbolAddress); make that first call on each device
+ * before any stream capture begins. The context's device must be current.
+ * Every scratch word is written before it is read, so nothing needs clearing
+ * between calls. */
 #define KBFV_NOALLOC_SCRATCH_BYTES ((size_t)40 << 20)
 int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                            uint64_t* d_out, uint32_t count, kbfv_stream stream);
