@@ -81,7 +81,8 @@ const char* kbfv_version(void);
  * 4: Shoup product, 5: 128-bit Barrett, 6: one-high-product Barrett,
  * 7: 32x32->64 multiply-add, 8: 32x32 high product, 9: 32-bit multiply-add,
  * 10: 64x64->128 multiply-accumulate from 32-bit partial products with carry
- * chains. The roofline of the IMAD-bound kernels. */
+ * chains, 11: forward NTT butterfly from 32-bit partial products. The roofline
+ * of the IMAD-bound kernels. */
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops);
 
 /* ---- context ---------------------------------------------------------

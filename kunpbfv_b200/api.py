@@ -862,7 +862,8 @@ def wire_load(ctx: BFVContext, kind: str, data: bytes, out, max_count: int = 1):
 
 PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64", "forward NTT butterfly",
                "Shoup product", "128-bit Barrett", "one-high-product Barrett", "32x32->64 multiply-add",
-               "32x32 high product", "32-bit multiply-add", "64x64->128 multiply-accumulate from 32-bit parts"]
+               "32x32 high product", "32-bit multiply-add", "64x64->128 multiply-accumulate from 32-bit parts",
+               "forward NTT butterfly from 32-bit parts"]
 
 
 def probe_arith(kind: int, iters: int = 4096) -> float:

@@ -1360,7 +1360,8 @@ static void require_klss(const Context& c) {
 // 3: forward butterfly (approximate-quotient Shoup), 4: fully reduced Shoup,
 // 5: 128-bit Barrett, 6: one-high-product Barrett, 7: 32x32->64 multiply-add,
 // 8: 32x32 high product, 9: 32-bit multiply-add, 10: mac32 (64x64->128
-// multiply-accumulate from 32-bit partial products).
+// multiply-accumulate from 32-bit partial products), 11: forward butterfly
+// with shoup4_32.
 constexpr int kProbeChains = 8;
 template <int KIND>
 __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_t mh, uint64_t ml, uint64_t mp) {
@@ -1391,6 +1392,14 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
             if (KIND == 8) acc[c].lo += __umulhi((uint32_t)a[c], (uint32_t)b[c]);
             if (KIND == 9) acc[c].lo = (uint32_t)a[c] * (uint32_t)b[c] + (uint32_t)acc[c].lo;
             if (KIND == 10) mac32(acc[c], a[c], b[c]);
+            if (KIND == 11) {
+                uint64_t x = a[c], y = b[c];
+                const uint64_t v = shoup4_32(y, b[c], a[c], q);
+                x = csub63(x, q << 2);
+                y = x + (q << 2) - v;
+                x = x + v;
+                acc[c].lo += x ^ y;
+            }
             a[c] = (a[c] + (acc[c].lo & 15)) & 0x0fffffffffffffffULL;
         }
     }
@@ -2737,7 +2746,7 @@ int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_
 
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
     return guarded([&] {
-        KB_REQUIRE(kind >= 0 && kind <= 10 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
+        KB_REQUIRE(kind >= 0 && kind <= 11 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
         int dev = 0, sms = 0;
         KB_CHECK_CUDA(cudaGetDevice(&dev));
         KB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -2756,7 +2765,7 @@ int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
             KB_CHECK_CUDA(cudaEventRecord(e0));
             switch (kind) {
 #define P_K(K) case K: probe_arith_kernel<K><<<blocks, threads>>>(out, (int)iters, q, mh, ml, mp); break;
-                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7) P_K(8) P_K(9) P_K(10)
+                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7) P_K(8) P_K(9) P_K(10) P_K(11)
 #undef P_K
             }
             KB_CHECK_CUDA(cudaEventRecord(e1));
