@@ -242,7 +242,44 @@ def run_reference(args, world, rank):
                                    "so the CPU oracle restatement stands in"},
         "e2e": {"value": round(v, 3), "unit": "ct/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    ref_gpu = reference_gpu_timing()
+    if ref_gpu is not None:
+        line["reference_gpu"] = ref_gpu
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_timing(reps: int = 20):
+    """kunpBFV's own GPU multiply, timed by the reference-kernel harness built
+    from its sources (oracle/_ref/ref_harness), at its own parameter sets
+    (logN 14 and 15): the genuine product as multAndEqual_23 runs it, one pair
+    per call. None when the harness or a GPU is absent."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref", "ref_harness")
+    try:
+        import torch
+        if not (os.path.exists(exe) and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    out = {"form": "tensor (compute_t_QInv_c0c1c2) then the T-base key switch and add-back, one pair per call, "
+                   "CUDA events over " + str(reps) + " calls",
+           "caveat": "the reference's tensor step allocates device memory on every call and also computes its "
+                     "secret-key shortcut product, which this sequence then discards"}
+    for log_n in (14, 15):
+        with tempfile.TemporaryDirectory() as d:
+            try:
+                r = subprocess.run([exe, str(log_n), d, "0", str(reps)], capture_output=True, text=True, timeout=300)
+                lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+                if r.returncode != 0 or not lines:
+                    out[f"logn{log_n}"] = {"error": (r.stderr or r.stdout)[-200:]}
+                    continue
+                t = json.loads(lines[-1])
+                out[f"logn{log_n}"] = {"ms_per_mult": round(t["ms_per_mult"], 4),
+                                       "ct_per_s": round(1e3 / t["ms_per_mult"], 1)}
+            except Exception as e:  # report, keep the CPU line
+                out[f"logn{log_n}"] = {"error": repr(e)[-200:]}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -506,6 +543,38 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     res["per_op_plain"] = {"value": round(BATCH / (ms_plain / 1e3), 2), "unit": "ct/s",
                            "form": "one pair per call, one kernel per building block (about 25 launches and "
                                    "6 device copies per pair), no graph"}
+
+    # this engine at the reference's own parameter sets (logN 14, 15) with the
+    # reference's key switch over the T base: one pair per call (the form the
+    # reference runs) and a 64-pair batch
+    from kunpbfv_b200 import tune
+    refp = {}
+    for log_n in (14, 15):
+        rctx = kb.reference_context(log_n)
+        rsk = kb.SecretKey(rctx, SEED)
+        rs = kb.BFVScheme(rctx, SEED, relin="klss")
+        rs.addMultKey_23(rsk)
+        ra = kb.Ciphertext(rctx, tune._random_pairs(rctx, 64, 7))
+        rb = kb.Ciphertext(rctx, tune._random_pairs(rctx, 64, 8))
+        ro = kb.Ciphertext(rctx, count=64)
+        lq_r = 2 * rctx.q_count * rctx.N
+        a1r = [kb.Ciphertext(rctx, ra.cipher_device.view(-1)[i * lq_r:(i + 1) * lq_r]) for i in range(8)]
+        b1r = [kb.Ciphertext(rctx, rb.cipher_device.view(-1)[i * lq_r:(i + 1) * lq_r]) for i in range(8)]
+        o1r = [kb.Ciphertext(rctx, ro.cipher_device.view(-1)[i * lq_r:(i + 1) * lq_r]) for i in range(8)]
+
+        def one_by_one():
+            for i in range(8):
+                rs.mult_relin(a1r[i], b1r[i], out=o1r[i], stream=stream)
+
+        ms1 = time_cuda(one_by_one, stream, 3) / 8
+        msb = time_cuda(lambda: rs.mult_relin(ra, rb, out=ro, stream=stream), stream, 3) / 64
+        refp[f"logn{log_n}"] = {"q": rctx.q_count, "p": rctx.p_count, "t_primes": rctx.t_count,
+                                "per_op_ms_per_mult": round(ms1, 4), "per_op_ct_per_s": round(1e3 / ms1, 1),
+                                "batched_ms_per_mult": round(msb, 4), "batched_ct_per_s": round(1e3 / msb, 1)}
+        del ra, rb, ro, a1r, b1r, o1r, rs, rsk
+        rctx.close()
+    res["reference_params"] = dict(refp, form="T-base key switch (bit-exact with the reference's genuine "
+                                              "multiply); per-op: one pair per call; batched: 64 pairs per call")
 
     # e2e through the C ABI with page-locked host buffers: kbfv_mul_relin_host
     # copies each chunk in, multiplies it and copies its products out, the

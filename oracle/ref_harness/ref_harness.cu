@@ -12,7 +12,9 @@
 // (include/BFVScheme.cuh:138), so the harness launches that kernel itself
 // with a device copy of the moduli.
 //
-// Usage: ref_harness <logN 14|15> <outdir> [raw_limit_words]
+// Usage: ref_harness <logN 14|15> <outdir> [raw_limit_words] [time_reps]
+// With time_reps > 0 it also times the genuine multiply (one pair per call,
+// CUDA events) and prints {"logN", "reps", "ms_per_mult"} on stdout.
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -61,6 +63,7 @@ static uint64_tt mix64(uint64_tt z) {
 // Writes one manifest line per array: name, length, digest, first 8 values.
 // Arrays up to `g_raw_limit` words are also written raw (<name>.bin).
 static size_t g_raw_limit = 0;
+static int g_time_reps = 0;  // > 0: also time the genuine multiply over this many calls
 static void dump_host(const std::string& name, const uint64_tt* p, size_t count) {
     uint64_tt h = 0;
     for (size_t i = 0; i < count; i++) h += mix64(p[i] ^ ((uint64_tt)i * 0x9E3779B97F4A7C15ULL));
@@ -104,6 +107,7 @@ int main(int argc, char** argv) {
     g_out = argv[2];
     g_manifest = fopen((g_out + "/manifest.txt").c_str(), "w");
     g_raw_limit = argc > 3 ? (size_t)atoll(argv[3]) : 64;
+    g_time_reps = argc > 4 ? atoi(argv[4]) : 0;
     const size_t N = (size_t)1 << logN;
 
     BFVContext context(N);
@@ -377,21 +381,43 @@ int main(int argc, char** argv) {
         const int l = L;
         const int swk_blockNum = (int)ceil(double(K + l + 1) / context.gamma);
         const int cipher_blockNum = (int)ceil(double(l + 1) / K);
-        scheme.compute_t_QInv_c0c1c2(scheme.axbx1_mul, scheme.axax_mul, scheme.bxbx_mul, c1, c2);
+        // tensor, then the key switch of a1*a2 and the add-back into c1
+        auto tensor = [&]() { scheme.compute_t_QInv_c0c1c2(scheme.axbx1_mul, scheme.axax_mul, scheme.bxbx_mul, c1, c2); };
+        auto key_switch = [&]() {
+            context.FromNTTInplace(scheme.axax_mul, 0, K, 1, l + 1, L + 1);
+            context.modUpQjtoT_23(scheme.modUp_QjtoT_temp, scheme.axax_mul, l, 1);
+            context.ToNTTInplace(scheme.modUp_QjtoT_temp, 0, K + L + 1, cipher_blockNum, t_num, t_num);
+            context.external_product_T(scheme.exProduct_T_temp, scheme.modUp_QjtoT_temp, rlk->cipher_device, l);
+            context.FromNTTInplace_for_externalProduct(scheme.exProduct_T_temp, 0, K + L + 1, swk_blockNum, t_num,
+                                                       t_num, Ri * t_num, 2);
+            context.modUpTtoPQl_23(scheme.modUp_TtoQj_buffer, scheme.exProduct_T_temp, l, 2);
+            context.modDownPQltoQl_23(c1.cipher_device, scheme.modUp_TtoQj_buffer, l, 2);
+            context.ToNTTInplace(c1.cipher_device, 0, K, 2, l + 1, L + 1);
+            cipher_add_axbx_batch_device(c1.cipher_device, scheme.axbx1_mul, scheme.bxbx_mul, N, K, l + 1, L + 1);
+        };
+        tensor();
         dump_dev("mult_axax", scheme.axax_mul, q_num * N);
         dump_dev("mult_axbx", scheme.axbx1_mul, q_num * N);
         dump_dev("mult_bxbx", scheme.bxbx_mul, q_num * N);
-        context.FromNTTInplace(scheme.axax_mul, 0, K, 1, l + 1, L + 1);
-        context.modUpQjtoT_23(scheme.modUp_QjtoT_temp, scheme.axax_mul, l, 1);
-        context.ToNTTInplace(scheme.modUp_QjtoT_temp, 0, K + L + 1, cipher_blockNum, t_num, t_num);
-        context.external_product_T(scheme.exProduct_T_temp, scheme.modUp_QjtoT_temp, rlk->cipher_device, l);
-        context.FromNTTInplace_for_externalProduct(scheme.exProduct_T_temp, 0, K + L + 1, swk_blockNum, t_num,
-                                                   t_num, Ri * t_num, 2);
-        context.modUpTtoPQl_23(scheme.modUp_TtoQj_buffer, scheme.exProduct_T_temp, l, 2);
-        context.modDownPQltoQl_23(c1.cipher_device, scheme.modUp_TtoQj_buffer, l, 2);
-        context.ToNTTInplace(c1.cipher_device, 0, K, 2, l + 1, L + 1);
-        cipher_add_axbx_batch_device(c1.cipher_device, scheme.axbx1_mul, scheme.bxbx_mul, N, K, l + 1, L + 1);
+        key_switch();
         dump_dev("mult_out", c1.cipher_device, 2 * q_num * N);
+        // timing of the same genuine multiply, one pair per call as the reference
+        // runs it (its tensor step allocates device memory on every call); the
+        // values keep changing in place, which does not change the work
+        if (g_time_reps > 0) {
+            for (int r = 0; r < 2; r++) { tensor(); key_switch(); }
+            cudaEvent_t e0, e1;
+            ck(cudaEventCreate(&e0), "event");
+            ck(cudaEventCreate(&e1), "event");
+            ck(cudaDeviceSynchronize(), "warm-up");
+            ck(cudaEventRecord(e0), "record");
+            for (int r = 0; r < g_time_reps; r++) { tensor(); key_switch(); }
+            ck(cudaEventRecord(e1), "record");
+            ck(cudaEventSynchronize(e1), "sync");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+            printf("{\"logN\": %d, \"reps\": %d, \"ms_per_mult\": %.5f}\n", logN, g_time_reps, ms / g_time_reps);
+        }
     }
     ck(cudaDeviceSynchronize(), "end");
     fclose(g_manifest);
