@@ -52,7 +52,7 @@ def parse():
                     help="run one kernel on a profiling-sized case and exit (for ncu)")
     ap.add_argument("--rows", type=int, default=1024, help="rows for the ntt16k profiling cases")
     ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
-    ap.add_argument("--serve-rates", default="500,1000,2000,3000,4000",
+    ap.add_argument("--serve-rates", default="500,1000,2000,3000,4000,6000,8000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=2.5,
                     help="shortest arrival window per rate (longer where needed for --serve-requests)")
