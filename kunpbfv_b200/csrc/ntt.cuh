@@ -268,6 +268,39 @@ __device__ __forceinline__ void inv_passes(const PassCtx& c) {
     }
 }
 
+// The first inverse pass (the block's last local stages, lb = 0: groups of
+// 2^R adjacent points) loads its inputs straight from the row: no staging of
+// the row in shared memory and one barrier less (4.7% faster inverse NTT at
+// N=2^14 than a coalesced load-in; the loads of adjacent points hit the same
+// cache lines).
+template <int LOGB, int S0, int R, class SRow>
+__device__ __forceinline__ void inv_pass_load(const PassCtx& c, const SRow& s) {
+    constexpr int T = (1 << LOGB) / 16, G = 1 << R, NG = 16 / G;
+    static_assert(LOGB - S0 - R == 0, "the loading pass holds the last stages");
+#pragma unroll 1
+    for (int g = 0; g < NG; g++) {
+        const int lbase = (g * T + c.t) << R;
+        uint64_t x[G];
+#pragma unroll
+        for (int k = 0; k < G; k++) x[k] = s.load(c.goff + lbase + k);
+        const int s0 = c.sbase + S0;
+        inv_group<R>(x, c.tw, s0, (c.goff + lbase) >> (c.logn - s0), c.q, c.q4, false);
+#pragma unroll
+        for (int k = 0; k < G; k++) c.sm[spad(lbase + k)] = x[k];
+    }
+    __syncthreads();
+}
+template <int LOGB, int RAD, int S0, class SRow>
+__device__ __forceinline__ void inv_passes_load(const PassCtx& c, const SRow& s) {
+    constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
+    if constexpr (S0 + R < LOGB) {
+        inv_passes_load<LOGB, RAD, S0 + R>(c, s);
+        inv_pass_smem<LOGB, S0, R>(c);
+    } else {
+        inv_pass_load<LOGB, S0, R>(c, s);
+    }
+}
+
 // FULL: fully reduce the output to [0, q); otherwise outputs are in [0, 8q).
 template <int LOGB, class Src, class Dst, bool FULL = true>
 __global__ void __launch_bounds__(1 << (LOGB - 4))
@@ -300,8 +333,9 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     }
     __syncthreads();
     fwd_passes<LOGB, RAD, R0>(c);
-    // coalesced write-out; the store target is bound here, so a fused store's
-    // operands hold no registers during the transform
+    // coalesced write-out (a last pass storing its groups of adjacent points
+    // straight to the row measured 14% slower here); the store target is bound
+    // here, so a fused store's operands hold no registers during the transform
     const auto d = dst.bind(row);
 #pragma unroll
     for (int k = 0; k < 16; k++) {
@@ -328,13 +362,7 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const uint64_t q = mods[pidx], q4 = q << 2;
     PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
 
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        const int j = t + k * T;
-        sm[spad(j)] = s.load(c.goff + j);
-    }
-    __syncthreads();
-    inv_passes<LOGB, RAD, R0>(c);
+    inv_passes_load<LOGB, RAD, R0>(c, s);
     // pass 0 (local stages 0..R0-1), coalesced stores
     const auto d = dst.bind(row);
 #pragma unroll 1
