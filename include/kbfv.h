@@ -20,6 +20,12 @@
  *
  * Every function returns KBFV_OK or a negative kbfv_status; kbfv_last_error()
  * describes the most recent failure on the calling thread.
+ *
+ * Threads and streams: calls on different contexts are independent. A context
+ * owns one scratch arena and its helper streams, so calls on the same context
+ * must be issued in order from one host thread (or under the caller's lock)
+ * and ordered on the GPU through one caller stream; the request server
+ * (kbfv_serve.h) gives each ring its own context for that reason.
  */
 #ifndef KBFV_H
 #define KBFV_H
