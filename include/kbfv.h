@@ -25,7 +25,8 @@
  * owns one scratch arena and its helper streams, so calls on the same context
  * must be issued in order from one host thread (or under the caller's lock)
  * and ordered on the GPU through one caller stream; the request server
- * (kbfv_serve.h) gives each ring its own context for that reason.
+ * (kbfv_serve.h) drives each ring's context from its one scheduler thread, so
+ * a context handed to a running server is not used by other threads.
  */
 #ifndef KBFV_H
 #define KBFV_H
