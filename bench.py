@@ -414,9 +414,9 @@ def run_ours(args, world, rank, local):
                    "l2": "inputs 235 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}",
                    "tuned": tuned},
         "decrypt_exact": ok, "noise_budget_bits": round(budget, 2),
-        # 8 kernels per sub-batch; batches of 16+ pairs run as `branches` sub-batches
+        # 9 kernels per sub-batch; batches of 16+ pairs run as `branches` sub-batches
         # (at least 8 pairs each) on forked streams
-        "gpu_launches": 8 * max(1, min(ctx.tune_get("branches"), BATCH // 8)) * args.steps,
+        "gpu_launches": 9 * max(1, min(ctx.tune_get("branches"), BATCH // 8)) * args.steps,
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.skip_extras:
@@ -473,7 +473,7 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
 
     ms_op = time_cuda(per_op, stream, 3)
     res["per_op"] = {"value": round(BATCH / (ms_op / 1e3), 2), "unit": "ct/s",
-                     "form": "one pair per call, 8 eager launches each, no graph"}
+                     "form": "one pair per call, 9-14 eager launches each (small launches split), no graph"}
     # the operation-by-operation form: tensor (kbfv_mul) then relinearisation
     # (kbfv_relinearize) as separate calls, one pair each (13 launches per pair)
     t3 = kb.Tensor3(ctx, count=1)

@@ -1026,15 +1026,12 @@ struct OutCtKeyDst {  // rows: (item, h, l) -> out[item] + (h*nq + l)*N
 // kernel's final store runs the epilogue
 static inline OutCtDst plain_of(const OutCtKeyDst& d) { return OutCtDst{d.pb, d.dc.logn, d.dc.nq}; }
 
-// K5: scale-and-round to R, R -> Q, and (mode 1) the key-switch lift of a1*a2.
-// mode 0: all three outputs over Q to out0 ([item][3][nq]).
-// mode 1: a1*a2 lifted into sd2 ([item][dnum][npq]); cross, b1*b2 to sd ([item][2][nq]).
-// mode 2: a1*a2 over Q into sd2 ([item][nq]); cross, b1*b2 to sd (T-base key switch).
+// K5, in two kernels so that each holds fewer registers (more warps per SM):
+// K5a: t/Q scale-and-round Q|R -> R of each tensor polynomial into rr ([poly][nr]).
 template <int MAXQ>
-__global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__ sc, uint64_t* __restrict__ out0,
-                                uint64_t* __restrict__ sd, uint64_t* __restrict__ sd2, int mode) {
+__global__ void k5_scale_kernel(DevConsts c, const uint64_t* __restrict__ sc, uint64_t* __restrict__ rr_out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int poly = blockIdx.y, item = poly / 3, which = poly % 3;
+    const int poly = blockIdx.y;
     const uint64_t* src = sc + ((size_t)poly * c.nqr << c.logn);
     uint64_t xq[MAXQ], xr[MAXQ + 1], rr[MAXQ + 1];
 #pragma unroll
@@ -1044,7 +1041,26 @@ __global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__ sc, ui
     for (int j = 0; j < MAXQ + 1; j++)
         if (j < c.nr) xr[j] = src[((size_t)(c.nq + j) << c.logn) + k];
     scale_round_coeff<MAXQ>(c, xq, xr, rr);
-    // R -> Q
+    uint64_t* dst = rr_out + ((size_t)poly * c.nr << c.logn);
+#pragma unroll
+    for (int j = 0; j < MAXQ + 1; j++)
+        if (j < c.nr) dst[((size_t)j << c.logn) + k] = rr[j];
+}
+
+// K5b: R -> Q, and (mode 1) the key-switch lift of a1*a2.
+// mode 0: all three outputs over Q to out0 ([item][3][nq]).
+// mode 1: a1*a2 lifted into sd2 ([item][dnum][npq]); cross, b1*b2 to sd ([item][2][nq]).
+// mode 2: a1*a2 over Q into sd2 ([item][nq]); cross, b1*b2 to sd (T-base key switch).
+template <int MAXQ>
+__global__ void k5_lift_kernel(DevConsts c, const uint64_t* __restrict__ rr_in, uint64_t* __restrict__ out0,
+                               uint64_t* __restrict__ sd, uint64_t* __restrict__ sd2, int mode) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int poly = blockIdx.y, item = poly / 3, which = poly % 3;
+    const uint64_t* src = rr_in + ((size_t)poly * c.nr << c.logn);
+    uint64_t rr[MAXQ + 1], xq[MAXQ];
+#pragma unroll
+    for (int j = 0; j < MAXQ + 1; j++)
+        if (j < c.nr) rr[j] = src[((size_t)j << c.logn) + k];
     const BconvTables tb = r2q_tables(c);
     uint64_t y[MAXQ + 1];
     const long long v = bconv_prep<MAXQ + 1>(y, rr, tb.nin, tb.in_mods, tb.hatinv, tb.hatinvs, tb.binv);
@@ -1112,7 +1128,13 @@ static void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0
     const DevConsts& dc = c.dc;
     const int threads = 128;
     dim3 grid((unsigned)(c.n / threads), (unsigned)(count * 3));
-#define L_K5(M) k5_round_kernel<M><<<grid, threads, 0, st>>>(dc, m.sc, out0, m.sd, m.sd2, mode)
+    // the R limbs of the inputs (m.sb, 4 x nr limbs per pair) are dead after K4:
+    // they hold the scale-and-round results (3 x nr limbs per pair)
+#define L_K5(M)                                                                        \
+    do {                                                                               \
+        k5_scale_kernel<M><<<grid, threads, 0, st>>>(dc, m.sc, m.sb);                  \
+        k5_lift_kernel<M><<<grid, threads, 0, st>>>(dc, m.sb, out0, m.sd, m.sd2, mode); \
+    } while (0)
     DISPATCH_MAXQ(dc.nq + 1, L_K5);
 #undef L_K5
     check_launch("k5_round");
