@@ -617,13 +617,14 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
                                "fmaheavy busy ~66% of elapsed with math-pipe throttling the top stall",
                        "butterflies_per_s": round(bfly / (ms_ntt / 1e3), 0)}
     # the bound that does apply: the butterfly issue rate of this GPU, measured
-    # live by the register-chain probe (kbfv_probe_arith kind 3, no memory traffic)
+    # live by the register-chain probe (kbfv_probe_arith kind 11: the kernels'
+    # butterfly, no memory traffic)
     from kunpbfv_b200.api import probe_arith
-    bfly_peak = probe_arith(3) * 1e9
+    bfly_peak = probe_arith(11) * 1e9
     res["roofline"]["arith"] = {"bound": "imad", "unit": "butterflies/s",
                                 "achieved": round(bfly / (ms_ntt / 1e3), 0), "peak": round(bfly_peak, 0),
                                 "frac": round(bfly / (ms_ntt / 1e3) / bfly_peak, 4),
-                                "peak_source": "kbfv_probe_arith(3): 60-bit forward butterflies in register chains"}
+                                "peak_source": "kbfv_probe_arith(11): the kernels' 60-bit forward butterfly in register chains"}
     del x
 
     # standalone NTT, N=65536, 32 primes x 64 polynomials (1 GiB)

@@ -84,11 +84,13 @@ const char* kbfv_last_error(void);
 const char* kbfv_version(void);
 /* Throughput of one 64-bit modular primitive on the current device (Gop/s):
  * independent register chains, no memory traffic. kind 0: 64x64->128
- * multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64, 3: forward NTT butterfly,
+ * multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64, 3: forward NTT butterfly
+ * with the Shoup product from 64-bit multiplies,
  * 4: Shoup product, 5: 128-bit Barrett, 6: one-high-product Barrett,
  * 7: 32x32->64 multiply-add, 8: 32x32 high product, 9: 32-bit multiply-add,
  * 10: 64x64->128 multiply-accumulate from 32-bit partial products with carry
- * chains, 11: forward NTT butterfly from 32-bit partial products. The roofline
+ * chains, 11: forward NTT butterfly from 32-bit partial products (the one the
+ * NTT kernels use). The roofline
  * of the IMAD-bound kernels. */
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops);
 

@@ -860,10 +860,11 @@ def wire_load(ctx: BFVContext, kind: str, data: bytes, out, max_count: int = 1):
     return cnt.value, aux.value
 
 
-PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64", "forward NTT butterfly",
+PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64",
+               "forward NTT butterfly from 64-bit multiplies",
                "Shoup product", "128-bit Barrett", "one-high-product Barrett", "32x32->64 multiply-add",
                "32x32 high product", "32-bit multiply-add", "64x64->128 multiply-accumulate from 32-bit parts",
-               "forward NTT butterfly from 32-bit parts"]
+               "forward NTT butterfly from 32-bit parts (the kernels')"]
 
 
 def probe_arith(kind: int, iters: int = 4096) -> float:

@@ -1379,11 +1379,12 @@ static void require_klss(const Context& c) {
 
 // ---- arithmetic-rate probe: independent register chains of one primitive -------
 // kind 0: 64x64->128 multiply-accumulate, 1: mul.lo.u64, 2: mul.hi.u64,
-// 3: forward butterfly (approximate-quotient Shoup), 4: fully reduced Shoup,
+// 3: forward butterfly with the approximate-quotient Shoup product from 64-bit
+// multiplies (shoup4_64), 4: fully reduced Shoup,
 // 5: 128-bit Barrett, 6: one-high-product Barrett, 7: 32x32->64 multiply-add,
 // 8: 32x32 high product, 9: 32-bit multiply-add, 10: mac32 (64x64->128
 // multiply-accumulate from 32-bit partial products), 11: forward butterfly
-// with shoup4_32.
+// with shoup4_32 (the NTT kernels' butterfly).
 constexpr int kProbeChains = 8;
 template <int KIND>
 __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_t mh, uint64_t ml, uint64_t mp) {
@@ -1402,9 +1403,12 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
             if (KIND == 0) mac64(acc[c], a[c], b[c]);
             if (KIND == 1) acc[c].lo += a[c] * b[c];
             if (KIND == 2) acc[c].lo += __umul64hi(a[c], b[c]);
-            if (KIND == 3) {
+            if (KIND == 3) {  // the butterfly with the Shoup product from 64-bit multiplies
                 uint64_t x = a[c], y = b[c];
-                ct_bfly(x, y, tw_t{b[c], a[c]}, q, q << 2);
+                const uint64_t v = shoup4_64(y, b[c], a[c], q);
+                x = csub63(x, q << 2);
+                y = x + (q << 2) - v;
+                x = x + v;
                 acc[c].lo += x ^ y;
             }
             if (KIND == 4) acc[c].lo += shoup(a[c], b[c], a[c] ^ b[c], q);
@@ -1414,12 +1418,9 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
             if (KIND == 8) acc[c].lo += __umulhi((uint32_t)a[c], (uint32_t)b[c]);
             if (KIND == 9) acc[c].lo = (uint32_t)a[c] * (uint32_t)b[c] + (uint32_t)acc[c].lo;
             if (KIND == 10) mac32(acc[c], a[c], b[c]);
-            if (KIND == 11) {
+            if (KIND == 11) {  // the NTT kernels' butterfly (Shoup product from 32-bit multiplies)
                 uint64_t x = a[c], y = b[c];
-                const uint64_t v = shoup4_32(y, b[c], a[c], q);
-                x = csub63(x, q << 2);
-                y = x + (q << 2) - v;
-                x = x + v;
+                ct_bfly(x, y, tw_t{b[c], a[c]}, q, q << 2);
                 acc[c].lo += x ^ y;
             }
             a[c] = (a[c] + (acc[c].lo & 15)) & 0x0fffffffffffffffULL;

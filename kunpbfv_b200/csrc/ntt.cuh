@@ -258,16 +258,6 @@ __device__ __forceinline__ void inv_pass_smem(const PassCtx& c) {
     __syncthreads();
 }
 
-// inverse passes with S0 >= first, run from the last stages back to `first`
-template <int LOGB, int RAD, int S0>
-__device__ __forceinline__ void inv_passes(const PassCtx& c) {
-    if constexpr (S0 < LOGB) {
-        constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
-        inv_passes<LOGB, RAD, S0 + R>(c);
-        inv_pass_smem<LOGB, S0, R>(c);
-    }
-}
-
 // The first inverse pass (the block's last local stages, lb = 0: groups of
 // 2^R adjacent points) loads its inputs straight from the row: no staging of
 // the row in shared memory and one barrier less (4.7% faster inverse NTT at
