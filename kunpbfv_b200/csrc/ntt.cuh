@@ -258,6 +258,16 @@ __device__ __forceinline__ void inv_pass_smem(const PassCtx& c) {
     __syncthreads();
 }
 
+// inverse passes with S0 >= first, run from the last stages back to `first`
+template <int LOGB, int RAD, int S0>
+__device__ __forceinline__ void inv_passes(const PassCtx& c) {
+    if constexpr (S0 < LOGB) {
+        constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
+        inv_passes<LOGB, RAD, S0 + R>(c);
+        inv_pass_smem<LOGB, S0, R>(c);
+    }
+}
+
 // The first inverse pass (the block's last local stages, lb = 0: groups of
 // 2^R adjacent points) loads its inputs straight from the row: no staging of
 // the row in shared memory and one barrier less (4.7% faster inverse NTT at
@@ -289,6 +299,15 @@ __device__ __forceinline__ void inv_passes_load(const PassCtx& c, const SRow& s)
     } else {
         inv_pass_load<LOGB, S0, R>(c, s);
     }
+}
+
+// Direct loads for groups of up to 4 adjacent points (32-byte lane stride);
+// wider groups (the 2^12-point blocks' last pass holds 16) load coalesced into
+// shared memory first.
+template <int LOGB, int RAD>
+__device__ __forceinline__ constexpr bool inv_direct_load() {
+    constexpr int rest = (LOGB - (RAD < LOGB ? RAD : LOGB)) % RAD;
+    return (rest == 0 ? RAD : rest) <= 2;
 }
 
 // FULL: fully reduce the output to [0, q); otherwise outputs are in [0, 8q).
@@ -352,7 +371,17 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const uint64_t q = mods[pidx], q4 = q << 2;
     PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
 
-    inv_passes_load<LOGB, RAD, R0>(c, s);
+    if constexpr (inv_direct_load<LOGB, RAD>()) {
+        inv_passes_load<LOGB, RAD, R0>(c, s);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int j = t + k * T;
+            sm[spad(j)] = s.load(c.goff + j);
+        }
+        __syncthreads();
+        inv_passes<LOGB, RAD, R0>(c);
+    }
     // pass 0 (local stages 0..R0-1), coalesced stores
     const auto d = dst.bind(row);
 #pragma unroll 1
