@@ -70,3 +70,27 @@ def test_autotune_ntt_split_large_ring(tmp_path):
     assert ctx.tune_get("ntt_block_log") == got["ntt_block_log"]
     assert set(got["ntt_ms"]) == {"0", "12", "13", "14"}
     ctx.tune_set("ntt_block_log", 0)
+
+
+def test_host_chunk_knob_drives_the_default_chunk():
+    """chunk_pairs = 0 takes the context's host_chunk knob; every chunk gives
+    the product of the device multiply."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200 import tune
+    ctx = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
+    sk = kb.SecretKey(ctx, b"\x31" * 32)
+    sch = kb.BFVScheme(ctx, b"\x32" * 32)
+    sch.addMultKey_23(sk)
+    a = tune._random_pairs(ctx, 11, 5)
+    b = tune._random_pairs(ctx, 11, 6)
+    want = sch.mult_relin(kb.Ciphertext(ctx, a), kb.Ciphertext(ctx, b)).cipher_device.cpu()
+    ha, hb = a.cpu().pin_memory(), b.cpu().pin_memory()
+    try:
+        for knob in (0, 1, 3, 128):
+            ctx.tune_set("host_chunk", knob)
+            out = sch.mult_relin_host(ha, hb, chunk_pairs=0)
+            assert torch.equal(out.view(-1), want.view(-1)), knob
+    finally:
+        ctx.tune_set("host_chunk", 0)
