@@ -12,7 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libkbfv.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = [os.path.join(HERE, "csrc", "kbfv.cu"), os.path.join(HERE, "csrc", "serve.cpp")]
+# translation units of libkbfv.so (compiled in parallel)
+SOURCES = [os.path.join(HERE, "csrc", f) for f in
+           ("k5_m8.cu", "k5_m16.cu", "k5_m24.cu", "k5_m33.cu", "mul.cu", "levels.cu", "scheme.cu", "ntt_ops.cu", "klss_api.cu", "context.cu", "serve.cpp")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))
            if f.endswith((".cuh", ".hpp", ".h"))] + [
     os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]

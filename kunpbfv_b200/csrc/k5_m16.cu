@@ -1,0 +1,4 @@
+// K5 kernels for contexts of at most 15 ciphertext primes (the MAXQ = 16 bucket)
+#include "k5_kernels.cuh"
+
+template void k5_launch_m<16>(const DevConsts&, int, const MulScratch&, uint64_t*, int, cudaStream_t);

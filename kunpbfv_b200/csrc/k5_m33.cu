@@ -1,0 +1,4 @@
+// K5 kernels for contexts of at most 32 ciphertext primes (the MAXQ = 33 bucket)
+#include "k5_kernels.cuh"
+
+template void k5_launch_m<33>(const DevConsts&, int, const MulScratch&, uint64_t*, int, cudaStream_t);

@@ -65,7 +65,7 @@ __host__ __device__ inline BconvTables r2q_tables(const DevConsts& c) {
 
 // one thread per coefficient; grid.y = polynomial
 template <int MAXIN>
-__global__ void bconv_kernel(BconvTables tb, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+static __global__ void bconv_kernel(BconvTables tb, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
                              int logn, size_t in_stride, size_t out_stride) {
     extern __shared__ uint64_t sh_hat[];
     for (int i = threadIdx.x; i < tb.nin * tb.nout; i += blockDim.x) sh_hat[i] = tb.hat[i];
@@ -116,7 +116,7 @@ __device__ __forceinline__ void scale_round_coeff(const DevConsts& c, const uint
 }
 
 template <int MAXQ>
-__global__ void scale_round_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
+static __global__ void scale_round_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t* src = in + ((size_t)blockIdx.y * c.nqr << c.logn);
     uint64_t* dst = out + ((size_t)blockIdx.y * c.nr << c.logn);
@@ -178,7 +178,7 @@ __device__ __forceinline__ void modup_coeff(const DevConsts& c, const uint64_t* 
 }
 
 template <int MAXQ>
-__global__ void modup_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
+static __global__ void modup_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t* src = in + ((size_t)blockIdx.y * c.nq << c.logn);
     uint64_t* dst = out + ((size_t)blockIdx.y * c.dnum * c.npq << c.logn);
@@ -209,7 +209,7 @@ __device__ __forceinline__ uint64_t moddown_elem(const DevConsts& c, const uint6
     return shoup(v, c.pinv_q[l], c.pinv_qs[l], ql);
 }
 
-__global__ void moddown_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
+static __global__ void moddown_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t* x = in + ((size_t)blockIdx.y * c.npq << c.logn);
     uint64_t* y = out + ((size_t)blockIdx.y * c.nq << c.logn);
@@ -266,7 +266,7 @@ __device__ __forceinline__ uint64_t decrypt_round_coeff(const DevConsts& c, cons
 }
 
 template <int MAXQ>
-__global__ void decrypt_round_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
+static __global__ void decrypt_round_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t* src = in + ((size_t)blockIdx.y * c.nq << c.logn);
     out[((size_t)blockIdx.y << c.logn) + k] = decrypt_round_coeff<MAXQ>(c, src, k);
@@ -282,7 +282,7 @@ struct LimbIdx {
 };
 
 // ceil(Q*m/t) per limb (bfv_add_timesQ_overt_kernel, include/poly_arithmetic.cuh:902-927)
-__global__ void delta_m_kernel(DevConsts c, const uint64_t* __restrict__ m, uint64_t* __restrict__ out, size_t total) {
+static __global__ void delta_m_kernel(DevConsts c, const uint64_t* __restrict__ m, uint64_t* __restrict__ out, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     const size_t n = (size_t)1 << c.logn;
@@ -293,7 +293,7 @@ __global__ void delta_m_kernel(DevConsts c, const uint64_t* __restrict__ m, uint
     out[i] = shoup(mq, c.tinv_q[l], c.tinv_qs[l], c.mods[l]);
 }
 
-__global__ void add_kernel(DevConsts c, const uint64_t* __restrict__ x, const uint64_t* __restrict__ y,
+static __global__ void add_kernel(DevConsts c, const uint64_t* __restrict__ x, const uint64_t* __restrict__ y,
                            uint64_t* __restrict__ out, size_t total, int limbs) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -307,7 +307,7 @@ __global__ void add_kernel(DevConsts c, const uint64_t* __restrict__ x, const ui
 struct ScalarTab {
     uint64_t c[kMaxQ], cs[kMaxQ];
 };
-__global__ void linear_kernel(DevConsts c, const uint64_t* x, const uint64_t* y, uint64_t* out, size_t total,
+static __global__ void linear_kernel(DevConsts c, const uint64_t* x, const uint64_t* y, uint64_t* out, size_t total,
                               int limbs, int op, ScalarTab tab) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -322,7 +322,7 @@ __global__ void linear_kernel(DevConsts c, const uint64_t* x, const uint64_t* y,
 }
 
 // ct (items x 2 x nq) times pt (items x nq)
-__global__ void mul_plain_kernel(DevConsts c, const uint64_t* __restrict__ ct, const uint64_t* __restrict__ pt,
+static __global__ void mul_plain_kernel(DevConsts c, const uint64_t* __restrict__ ct, const uint64_t* __restrict__ pt,
                                  uint64_t* __restrict__ out, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -334,7 +334,7 @@ __global__ void mul_plain_kernel(DevConsts c, const uint64_t* __restrict__ ct, c
 }
 
 // tensor over Q|R for the C-ABI building block: pairs of [a|b] (nqr limbs each)
-__global__ void tensor_qr_kernel(DevConsts c, const uint64_t* __restrict__ c1, const uint64_t* __restrict__ c2,
+static __global__ void tensor_qr_kernel(DevConsts c, const uint64_t* __restrict__ c1, const uint64_t* __restrict__ c2,
                                  uint64_t* __restrict__ out, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;  // total = pairs * nqr * N
@@ -395,7 +395,7 @@ __device__ __forceinline__ void salsa_block(const SalsaKey& key, uint32_t n0, ui
 }
 
 // raw keystream: block b of the stream written at byte 64*b (tail truncated)
-__global__ void salsa_stream_kernel(SalsaKey key, uint32_t n0, uint32_t n1, uint64_t block0, uint8_t* out,
+static __global__ void salsa_stream_kernel(SalsaKey key, uint32_t n0, uint32_t n1, uint64_t block0, uint8_t* out,
                                     size_t nbytes) {
     const size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (b * 64 >= nbytes) return;
@@ -408,7 +408,7 @@ __global__ void salsa_stream_kernel(SalsaKey key, uint32_t n0, uint32_t n1, uint
 
 // uniform residues: coefficient (limb l, k) of item i <- bytes [(l*N + k)*16, +16)
 // of stream (id0 + i); value floor(u128 * q / 2^128). One thread = 4 coefficients.
-__global__ void sample_uniform_kernel(DevConsts c, SalsaKey key, uint64_t id0, int prime0, int limbs,
+static __global__ void sample_uniform_kernel(DevConsts c, SalsaKey key, uint64_t id0, int prime0, int limbs,
                                       uint64_t* __restrict__ out, size_t item_stride, int items) {
     const size_t n = (size_t)1 << c.logn;
     const size_t per_item = (size_t)limbs * n / 4;
@@ -462,7 +462,7 @@ __device__ __forceinline__ void sample_small_block(const DevConsts& c, const Sal
 }
 
 template <int KIND>
-__global__ void sample_small_kernel(DevConsts c, SalsaKey key, uint64_t id0, int prime0, int limbs,
+static __global__ void sample_small_kernel(DevConsts c, SalsaKey key, uint64_t id0, int prime0, int limbs,
                                     uint64_t* __restrict__ out, size_t item_stride, int items) {
     constexpr int PER = KIND == 0 ? 16 : 8;
     const size_t per_item = ((size_t)1 << c.logn) / PER;
@@ -477,7 +477,7 @@ struct IdTable {
     uint64_t v[128];
 };
 template <int KIND>
-__global__ void sample_small_ids_kernel(DevConsts c, SalsaKey key, IdTable ids, int prime0, int limbs,
+static __global__ void sample_small_ids_kernel(DevConsts c, SalsaKey key, IdTable ids, int prime0, int limbs,
                                         uint64_t* __restrict__ out, size_t item_stride, int items) {
     constexpr int PER = KIND == 0 ? 16 : 8;
     const size_t per_item = ((size_t)1 << c.logn) / PER;
@@ -490,7 +490,7 @@ __global__ void sample_small_ids_kernel(DevConsts c, SalsaKey key, IdTable ids, 
 // Hamming-weight-h ternary secret (convert_HWT, include/Sampler_impl.cuh:68-87):
 // h positions from u32 & (N-1), sign from a byte >= 128; a later draw at the
 // same position overwrites. One thread per item; `out` must be zeroed.
-__global__ void sample_hwt_kernel(DevConsts c, SalsaKey key, uint64_t id0, int h, int prime0, int limbs,
+static __global__ void sample_hwt_kernel(DevConsts c, SalsaKey key, uint64_t id0, int h, int prime0, int limbs,
                                   uint64_t* __restrict__ out, size_t item_stride, int items) {
     const int item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= items) return;
@@ -523,7 +523,7 @@ __global__ void sample_hwt_kernel(DevConsts c, SalsaKey key, uint64_t id0, int h
 // keygen / encrypt combinations (NTT domain)
 // ===========================================================================
 // pk.b = e - a*s over Q (addEncKey, include/BFVScheme.cuh:67-78)
-__global__ void pk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
+static __global__ void pk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
                                   uint64_t* __restrict__ eb, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -533,7 +533,7 @@ __global__ void pk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, c
 
 // rlk digit d: b = e - a*s (+ P*s^2 on the digit's primes) over Q|P
 // (addMultKey_23, include/KeySwitch_23.cuh:35-53)
-__global__ void rlk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
+static __global__ void rlk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
                                    uint64_t* __restrict__ eb, int digit, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -549,7 +549,7 @@ __global__ void rlk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, 
 }
 
 // gadget key component: b = e - a*s + [l == prime] * g * s^2 (g = P * 2^{wj} mod q_prime)
-__global__ void gk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
+static __global__ void gk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
                                   uint64_t* __restrict__ eb, int prime, uint64_t g, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -566,7 +566,7 @@ __global__ void gk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, c
 // the same random words give the same samples: double arithmetic for the
 // uniform one, float arithmetic and CUDA's normcdfinvf for the Gaussian one.
 // ---------------------------------------------------------------------------
-__global__ void compat_uniform_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+static __global__ void compat_uniform_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
                                       int prime0, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -576,7 +576,7 @@ __global__ void compat_uniform_kernel(DevConsts c, const uint64_t* __restrict__ 
     d = __dmul_rn(d, __ull2double_rn(q - 1));
     out[i] = __double2ull_rz(d);
 }
-__global__ void compat_gauss_kernel(DevConsts c, const uint32_t* __restrict__ in, uint64_t* __restrict__ out,
+static __global__ void compat_gauss_kernel(DevConsts c, const uint32_t* __restrict__ in, uint64_t* __restrict__ out,
                                     int prime0, int limbs) {
     const size_t n = (size_t)1 << c.logn;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -595,7 +595,7 @@ __global__ void compat_gauss_kernel(DevConsts c, const uint32_t* __restrict__ in
         out[t * n + i] = dd < 0 ? q + (int64_t)dd : (uint64_t)dd;
     }
 }
-__global__ void compat_zo_kernel(DevConsts c, const uint8_t* __restrict__ in, uint64_t* __restrict__ out,
+static __global__ void compat_zo_kernel(DevConsts c, const uint8_t* __restrict__ in, uint64_t* __restrict__ out,
                                  int prime0, int limbs, double probability) {
     const size_t n = (size_t)1 << c.logn;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -611,7 +611,7 @@ __global__ void compat_zo_kernel(DevConsts c, const uint8_t* __restrict__ in, ui
     }
 }
 // one block per limb, h threads: position word, then sign byte (out pre-zeroed)
-__global__ void compat_hwt_kernel(DevConsts c, const uint8_t* __restrict__ in, uint64_t* __restrict__ out,
+static __global__ void compat_hwt_kernel(DevConsts c, const uint8_t* __restrict__ in, uint64_t* __restrict__ out,
                                   int prime0, int h) {
     const int t = blockIdx.x, j = threadIdx.x;
     if (j >= h) return;
@@ -628,7 +628,7 @@ __device__ __forceinline__ uint32_t galois_perm(uint32_t i, uint64_t g, int logn
     return __brev((uint32_t)(e >> 1)) >> (32 - logn);
 }
 // out[poly][l][i] = in[poly][l][perm(i)]  (polys x limbs rows of N; out != in)
-__global__ void galois_ntt_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+static __global__ void galois_ntt_kernel(DevConsts c, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
                                   uint64_t g, size_t total) {
     const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= total) return;
@@ -638,7 +638,7 @@ __global__ void galois_ntt_kernel(DevConsts c, const uint64_t* __restrict__ in, 
 }
 // key-switch key component for a target polynomial t (NTT form over Q|P):
 // b = e - a*s + [l in digit] * P * t
-__global__ void ksk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
+static __global__ void ksk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, const uint64_t* __restrict__ s,
                                    const uint64_t* __restrict__ target, uint64_t* __restrict__ eb, int digit,
                                    size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -653,7 +653,7 @@ __global__ void ksk_combine_kernel(DevConsts c, const uint64_t* __restrict__ a, 
 
 // encrypt: a = v*pk.a + e0, b = v*pk.b + e1 + dm (encryptZero/encryptMsg,
 // include/BFVScheme.cuh:87-146). work: items x [v | e0 | e1 | dm] x nq (NTT form)
-__global__ void enc_combine_kernel(DevConsts c, const uint64_t* __restrict__ pk, const uint64_t* __restrict__ work,
+static __global__ void enc_combine_kernel(DevConsts c, const uint64_t* __restrict__ pk, const uint64_t* __restrict__ work,
                                    uint64_t* __restrict__ ct, size_t total) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;  // items * nq * N

@@ -19,7 +19,7 @@ __host__ __device__ __forceinline__ int ref_to_row(int i, int np, int nq) { retu
 // Lift blocks into T. which = 0: Qj blocks of a Q polynomial (rows 0..nq-1);
 // which = 1: Ri blocks of a Q|P polynomial (rows in Q|P order).
 // grid: (N/128, blocks, items); out item layout [block][nt].
-__global__ void klss_block_to_t_kernel(DevConsts c, KlssConsts kc, const uint64_t* __restrict__ in,
+static __global__ void klss_block_to_t_kernel(DevConsts c, KlssConsts kc, const uint64_t* __restrict__ in,
                                        uint64_t* __restrict__ out, int which, size_t in_item_stride,
                                        size_t out_item_stride) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -70,7 +70,7 @@ __global__ void klss_block_to_t_kernel(DevConsts c, KlssConsts kc, const uint64_
 // Exact centred T -> P|Q: one polynomial's Ri blocks over T (coefficient form)
 // to its P|Q limbs (rows in Q|P order). in: [poly][nri][nt]; out: [poly][npq].
 // grid: (N/128, nri, polys)
-__global__ void klss_t_to_pq_kernel(DevConsts c, KlssConsts kc, const uint64_t* __restrict__ in,
+static __global__ void klss_t_to_pq_kernel(DevConsts c, KlssConsts kc, const uint64_t* __restrict__ in,
                                     uint64_t* __restrict__ out) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int b = blockIdx.y;

@@ -312,7 +312,7 @@ __device__ __forceinline__ constexpr bool inv_direct_load() {
 
 // FULL: fully reduce the output to [0, q); otherwise outputs are in [0, 8q).
 template <int LOGB, class Src, class Dst, bool FULL = true>
-__global__ void __launch_bounds__(1 << (LOGB - 4))
+static __global__ void __launch_bounds__(1 << (LOGB - 4))
 ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
                      int logn) {
     constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
@@ -356,7 +356,7 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
 
 // WHOLE: the block is the whole ring (logn == LOGB), so n^-1 is applied here.
 template <int LOGB, class Src, class Dst, bool WHOLE = true>
-__global__ void __launch_bounds__(1 << (LOGB - 4))
+static __global__ void __launch_bounds__(1 << (LOGB - 4))
 ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
                      int logn) {
     constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
@@ -440,7 +440,7 @@ __device__ __forceinline__ void ntt_inv_col(const Src& src, const Dst& dst, cons
 
 // grid-stride over all columns of all rows (more than 2^31 columns allowed)
 template <int RC, class Src, class Dst>
-__global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
+static __global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
                                    const uint64_t* __restrict__ mods, int logn, size_t ncol_total) {
     for (size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gid < ncol_total;
          gid += (size_t)gridDim.x * blockDim.x)
@@ -448,7 +448,7 @@ __global__ void ntt_fwd_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw
 }
 
 template <int RC, class Src, class Dst>
-__global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
+static __global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all,
                                    const uint64_t* __restrict__ mods, int logn, size_t ncol_total) {
     for (size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gid < ncol_total;
          gid += (size_t)gridDim.x * blockDim.x)
