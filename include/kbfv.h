@@ -114,6 +114,10 @@ int kbfv_context_decrypt_variant(const kbfv_context* ctx);
 size_t kbfv_mul_relin_scratch_bytes(const kbfv_context* ctx, uint32_t count);
 /* pre-size the context's scratch arena (no allocation happens later for <= count pairs) */
 int kbfv_reserve(kbfv_context* ctx, uint32_t pairs);
+/* bytes of device memory the context's scratch arena holds now: 0 until a call
+ * needs scratch or kbfv_reserve sizes it (no counterpart in the reference, whose
+ * scratch is allocated per call; lets a caller audit what the context holds) */
+size_t kbfv_context_arena_bytes(const kbfv_context* ctx);
 
 /* seed for keygen / encryption calls that pass seed = NULL (the reference
  * seeds its RNG once per scheme, include/RNG.cuh:18-51) */
@@ -399,19 +403,34 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
  * the middle of a request, code running inside another framework's allocator
  * or memory-pool hook (where calling cudaMalloc again is forbidden), and
  * latency-bound paths that cannot afford the implicit device synchronisation of
- * cudaMalloc / cudaFree. Its scratch is a
- * statically sized device array inside libkbfv.so of KBFV_NOALLOC_SCRATCH_BYTES
- * (40 MiB, held by every GPU that loads the library until exit): enough for 2
- * pairs at N=16384 with 7 ciphertext primes and 1 special prime
- * (kbfv_mul_relin_scratch_bytes gives the need). Larger requests return
- * KBFV_ERR_INVALID and launch nothing; nothing on this path calls cudaMalloc,
- * cudaFree or any allocating routine. All calls share the one array: calls
- * that overlap on the GPU (several streams or contexts) race and must be
- * serialised by the caller. The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress); make that first call on each device
- * before any stream capture begins. The context's device must be current.
- * Every scratch word is written before it is read, so nothing needs clearing
- * between calls. */
+ * cudaMalloc / cudaFree. Its scratch is a statically sized device array inside
+ * libkbfv.so of KBFV_NOALLOC_SCRATCH_BYTES (40 MiB).
+ * Limit: one call of `count` pairs needs
+ *   count * N * 8 * (4q + 4r + 3(q + r) + 2q + (dnum + 2)(q + p) [+ nqj*nt + 2*nri*nt with a T base])
+ * bytes (q ciphertext primes, r = q + 1, p special primes; the bracket only for
+ * contexts built with T-base primes): 143 limbs of 128 KiB = 17.9 MiB per pair
+ * at N=16384 with 7 + 1 primes and dnum 1, so 2 pairs; with dnum 7 one pair.
+ * For fewer than 16 pairs kbfv_mul_relin_scratch_bytes(ctx, count) returns the
+ * same figure (from 16 pairs on it counts the batched multiply's sub-batches).
+ * Larger requests return KBFV_ERR_INVALID and launch nothing; nothing on this
+ * path calls cudaMalloc, cudaFree or any allocating routine, and the
+ * context's own scratch arena is never touched (kbfv_context_arena_bytes
+ * stays where it was).
+ * The array is part of the library's multiply module. The CUDA runtime
+ * allocates it when it loads that module in a context: with lazy module
+ * loading (the default since CUDA 12.2) at the first multiply of any kind in
+ * that context, including the first call of this entry point; with eager
+ * loading when the context is created. It is held until the process exits (or
+ * the context is destroyed). A caller with a fixed budget makes one multiply
+ * call on each device during start-up, before any stream capture and before
+ * taking its budget snapshot. The first call of this entry point in each CUDA
+ * context also resolves the array's device address (cudaGetSymbolAddress),
+ * which is why that first call belongs before any stream capture too; later
+ * calls only look the address up. The context's device must be current.
+ * All calls share the one array: calls that overlap on the GPU (several
+ * streams or contexts) race and must be serialised by the caller. Every scratch
+ * word is written before it is read, so nothing needs clearing between calls;
+ * the array keeps the last call's intermediate values. */
 #define KBFV_NOALLOC_SCRATCH_BYTES ((size_t)40 << 20)
 int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                            uint64_t* d_out, uint32_t count, kbfv_stream stream);

@@ -101,6 +101,7 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_context_plain_modulus": (u64, [VP]),
         "kbfv_context_decrypt_variant": (I, [VP]),
         "kbfv_mul_relin_scratch_bytes": (C.c_size_t, [VP, u32]),
+        "kbfv_context_arena_bytes": (C.c_size_t, [VP]),
         "kbfv_reserve": (I, [VP, u32]),
         "kbfv_ntt_fwd": (I, [VP, VP, u32, u32, u32, VP]),
         "kbfv_ntt_inv": (I, [VP, VP, u32, u32, u32, VP]),
@@ -351,6 +352,10 @@ class BFVContext:
 
     def scratch_bytes(self, pairs: int) -> int:
         return int(lib().kbfv_mul_relin_scratch_bytes(self._h, pairs))
+
+    def arena_bytes(self) -> int:
+        """Bytes of device memory the context's scratch arena holds now."""
+        return int(lib().kbfv_context_arena_bytes(self._h))
 
     # ---- device buffers
     def zeros(self, *shape):

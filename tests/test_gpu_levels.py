@@ -96,8 +96,10 @@ def test_level_context_rules():
 
 def test_c4_uneven_batch():
     """16 pairs at depths 0-3 (14, 13, 12, 11 live primes) in one call; every
-    product equals the pair multiplied alone at its level and decrypts exactly;
-    one pair per level is also checked against the oracle."""
+    product equals the oracle's multiply at its level (all 16 pairs), equals
+    the pair multiplied alone at its level (the first 8) and decrypts exactly."""
+    from concurrent.futures import ThreadPoolExecutor
+
     import kunpbfv_b200 as kb
     import oracle
     ctx = kb.BFVContext.from_bits(15, [60] * 14, [60, 60], T, dnum=3)
@@ -124,18 +126,30 @@ def test_c4_uneven_batch():
         if j < 8:
             alone = sch.mult_relin(a, b)
             assert np.array_equal(host(alone.cipher_device), host(o.cipher_device)), j
-    # the oracle on the deepest and the top pair
+    # the oracle on every pair: one oracle per level (the level's live primes,
+    # the top level's digits and special primes, the top-level key restricted
+    # to the live limbs), each level's four pairs in a thread of their own
     top = oracle.Oracle(15, T, ctx.q, ctx.p, alpha=5)
     osk = top.keygen_secret(SEED)
     assert np.array_equal(host(sk.sx_device).reshape(osk.shape), osk)
     orlk = top.keygen_relin(SEED, osk)
-    for j in (0, 3):
-        live = 14 - j
+    ins = [tuple(host(x.cipher_device).reshape(2, 14 - j % 4, ctx.N) for x in pairs[j]) for j in range(16)]
+    got = [host(outs[j].cipher_device).reshape(2, 14 - j % 4, ctx.N) for j in range(16)]
+
+    def level(depth):
+        live = 14 - depth
         o = oracle.Oracle(15, T, ctx.q[:live], ctx.p, alpha=5)
         rl = np.stack([np.stack([np.concatenate([orlk[d][h][:live], orlk[d][h][14:]]) for h in range(2)])
                        for d in range(o.dnum)])
-        a, b = (host(x.cipher_device).reshape(2, live, ctx.N) for x in pairs[j])
-        assert np.array_equal(host(outs[j].cipher_device).reshape(2, live, ctx.N), o.mul_relin(a, b, rl)), j
+        return {j: o.mul_relin(*ins[j], rl) for j in range(depth, 16, 4)}
+
+    with ThreadPoolExecutor(max_workers=4) as ex:
+        want = {}
+        for part in ex.map(level, range(4)):
+            want.update(part)
+    assert sorted(want) == list(range(16))
+    for j in range(16):
+        assert np.array_equal(got[j], want[j]), f"pair {j} at {14 - j % 4} live primes differs from the oracle"
 
 
 def test_gadget_key_switch_bit_exact():

@@ -48,23 +48,37 @@ def test_ntt_plain_modulus_rows():
     assert np.array_equal(back, v)
 
 
-def test_ntt_c2_shape_round_trip_and_sample():
-    """N=65536, 32 primes x 64 polys (1 GiB): round trip bit-exact, and the
-    forward output equals the oracle on a sample of rows."""
+# C2 rows checked against the oracle: two polynomials per prime, all 64
+# polynomials distinct, so every prime's twiddle table and every polynomial
+# slot of the batch is covered by at least one full row
+C2_FWD_ROWS = [(p, (2 * p) % 64) for p in range(32)] + [(p, (2 * p + 37) % 64) for p in range(32)]
+
+
+def test_ntt_c2_shape_vs_oracle_and_round_trip():
+    """N=65536, 32 primes x 64 polys (1 GiB): 64 full forward rows (two per
+    prime, every polynomial once) equal the oracle's transform, 32 full
+    inverse rows (one per prime) equal the oracle's inverse of the GPU's
+    forward output, and the whole batch round-trips bit-exactly."""
     import torch
     log_n = 16
     n = 1 << log_n
     ps = list(chain(log_n, 60, 34))
     ctx, orc = make_pair(log_n, ps[2:34], ps[:1])
     nprime, npoly = 32, 64
+    assert sorted({poly for _, poly in C2_FWD_ROWS}) == list(range(npoly))
     g = torch.Generator(device="cuda").manual_seed(0)
     mods = torch.tensor([orc.primes[i] for i in range(nprime)], dtype=torch.int64, device="cuda")
     x = torch.randint(0, 1 << 62, (npoly, nprime, n), generator=g, device="cuda", dtype=torch.int64)
     x = torch.remainder(x, mods.view(1, nprime, 1))
     x0 = x.clone()
     ctx.ntt_fwd(x, 0, nprime)
-    for poly, prime in [(0, 0), (17, 5), (63, 31)]:
+    fwd = x.clone()
+    for prime, poly in C2_FWD_ROWS:
         want = orc.ntt_fwd(prime, host(x0[poly, prime]))
-        assert np.array_equal(host(x[poly, prime]), want)
+        assert np.array_equal(host(x[poly, prime]), want), f"forward row (poly {poly}, prime {prime})"
     ctx.ntt_inv(x, 0, nprime)
+    for prime in range(nprime):
+        poly = (5 * prime + 1) % npoly
+        want = orc.ntt_inv(prime, host(fwd[poly, prime]))
+        assert np.array_equal(host(x[poly, prime]), want), f"inverse row (poly {poly}, prime {prime})"
     assert torch.equal(x, x0)

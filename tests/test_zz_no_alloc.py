@@ -60,9 +60,48 @@ def test_noalloc_matches_allocating_entry_point_twice():
     assert np.array_equal(dec, (v1 * v2) % T)
 
 
+def test_noalloc_first_call_on_a_fresh_context_allocates_nothing():
+    """A context that never ran an allocating call multiplies through the
+    allocation-free entry point: its scratch arena stays empty and the device's
+    free memory is the same before and after each of two calls, whose results
+    equal the allocating entry point's on another context of the same
+    parameters (keys and ciphertexts are shared: same primes)."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    count = 2
+    _, ctx, sk, sch, c1, c2, v1, v2 = _setup(count)
+    # the expected products on the setup context (this also loads every
+    # multiply kernel into the CUDA context, so no lazy kernel load can land
+    # inside the measured calls)
+    want = sch.mult_relin(c1, c2)
+    fresh = kb.BFVContext(log_n=14, plain_modulus=T, q_count=ctx.q_count, q=ctx.q, p_count=ctx.p_count, p=ctx.p,
+                          dnum=1)
+    assert fresh.primes == ctx.primes
+    assert fresh.arena_bytes() == 0
+    outs = [kb.Ciphertext(fresh, count=count) for _ in range(2)]
+    torch.cuda.synchronize()
+    for call, out in enumerate(outs):
+        free_before, _ = torch.cuda.mem_get_info()
+        assert _noalloc(kb, fresh, sch, c1, c2, out, count) == 0, kb.lib().kbfv_last_error()
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        assert free_after == free_before, f"call {call}: device free memory moved by {free_before - free_after} B"
+        assert fresh.arena_bytes() == 0, f"call {call} allocated the context's scratch arena"
+        assert torch.equal(out.cipher_device, want.cipher_device), f"call {call} differs"
+    dec = kb.api.to_host(ctx.decode(sch.decryptMsg(sk, outs[1]).mx_device)).reshape(count, ctx.N)
+    assert np.array_equal(dec, (v1 * v2) % T)
+
+
 def test_noalloc_rejects_oversized_batches():
-    kb, ctx, sk, sch, c1, c2, v1, v2 = _setup(1)
-    out = kb.Ciphertext(ctx, count=3)
-    rc = _noalloc(kb, ctx, sch, c1, c2, out, 3)  # 3 pairs need ~55 MB > 40 MiB
+    import torch
+    count = 3  # 3 pairs need 3 x 143 limbs of 128 KiB = 53.6 MiB > 40 MiB
+    kb, ctx, sk, sch, c1, c2, v1, v2 = _setup(count)
+    assert ctx.scratch_bytes(count) > (40 << 20)
+    out = kb.Ciphertext(ctx, count=count)
+    before = out.cipher_device.clone()
+    rc = _noalloc(kb, ctx, sch, c1, c2, out, count)
+    torch.cuda.synchronize()
     assert rc == -1
     assert b"static array holds" in kb.lib().kbfv_last_error()
+    assert torch.equal(out.cipher_device, before), "a rejected call must launch nothing"
