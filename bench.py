@@ -73,12 +73,13 @@ def run_kernel_case(args):
         from kunpbfv_b200.api import PROBE_KINDS, probe_arith
         print(json.dumps({name: round(probe_arith(k), 1) for k, name in enumerate(PROBE_KINDS)}))
         return
-    qs, ps = c3_primes()
-    ctx = kb.BFVContext(log_n=LOG_N, plain_modulus=T, q_count=NQ, q=qs, p_count=NP, p=ps, dnum=1)
+    ctx = c3_context(kb)
     if args.kernel.startswith("ntt16k"):
         rows = args.rows
         x = torch.randint(0, 1 << 59, (rows, ctx.N), dtype=torch.int64, device="cuda")
         fn = ctx.ntt_inv if args.kernel.endswith("inv") else ctx.ntt_fwd
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures only these launches
         for _ in range(args.steps):
             fn(x, 0, NQ)
     else:
@@ -91,14 +92,27 @@ def run_kernel_case(args):
         rng = np.random.default_rng(0)
         v = rng.integers(0, T, size=(args.pairs, ctx.N), dtype=np.uint64)
         c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(to_device(v))), enc_id=0)
+        out = kb.Ciphertext(ctx, count=args.pairs)
+        ctx.reserve(args.pairs)
+        sch.mult_relin(c1, c1, out=out)  # loads the kernels and sizes the scratch
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures only these launches
         for _ in range(args.steps):
-            sch.mult_relin(c1, c1)
+            sch.mult_relin(c1, c1, out=out)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel_case": args.kernel, "steps": args.steps}))
+    torch.cuda.profiler.stop()
+    print(json.dumps({"kernel_case": args.kernel, "steps": args.steps, "branches": ctx.tune_get("branches")}))
 
 
-def c3_primes():
-    import oracle  # prime search only (same rule as the library)
+def c3_context(kb):
+    """C3's parameter set from the library's own prime generator
+    (kbfv_params_create: the largest 60-bit primes = 1 mod 2N, P first)."""
+    return kb.BFVContext.from_bits(LOG_N, [60] * NQ, [60] * NP, T, dnum=1)
+
+
+def c3_primes_oracle():
+    """The same primes from the oracle's generator (CPU legs only)."""
+    import oracle
     ps = oracle.primes_bits(1 << LOG_N, 60, NQ + NP)
     return ps[NP:NP + NQ], ps[:NP]
 
@@ -114,7 +128,7 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples (every 100 ms) kept only while the timed region runs:
+    """nvidia-smi samples (every 20 ms) kept only while the timed region runs:
     mark() at its start and end."""
 
     def __init__(self, index=0):
@@ -130,7 +144,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
         except Exception:
@@ -194,54 +208,94 @@ def max_over_ranks(world, v):
 
 
 # ---------------------------------------------------------------------------
-# reference arm: the CPU restatement of the reference's path, all host threads
+# CPU legs: the oracle's restatement of the reference's multiply on the host
+# cores. One method for the reference arm and for the cpu_baseline leg of our
+# arm: a persistent pool of one thread per core; a step is every thread
+# multiplying its own PAIRS_PER_THREAD pairs (the C oracle runs with the GIL
+# released), the step ends when the last thread is done.
 # ---------------------------------------------------------------------------
+PAIRS_PER_THREAD = 2
+CPU_STEP_BUDGET_S = 240.0  # the reference arm's timed steps stop here (stated in its line)
+
+
+class CpuOracle:
+    def __init__(self, seed_rng: int):
+        import numpy as np
+
+        import oracle
+        qs, ps = c3_primes_oracle()
+        self.o = o = oracle.Oracle(LOG_N, T, qs, ps, dnum=1)
+        sk = o.keygen_secret(SEED)
+        pk = o.keygen_public(SEED, sk)
+        self.rlk = o.keygen_relin(SEED, sk)
+        self.cores = os.cpu_count() or 1
+        rng = np.random.default_rng(seed_rng)
+        self.work = []  # per thread: its pairs
+        for t in range(self.cores):
+            pairs = []
+            for k in range(PAIRS_PER_THREAD):
+                i = t * PAIRS_PER_THREAD + k
+                v1 = rng.integers(0, T, size=o.n, dtype=np.uint64)
+                v2 = rng.integers(0, T, size=o.n, dtype=np.uint64)
+                pairs.append((o.encrypt(SEED, 2 * i, pk, o.encode(v1)), o.encrypt(SEED, 2 * i + 1, pk, o.encode(v2))))
+            self.work.append(pairs)
+        from concurrent.futures import ThreadPoolExecutor
+        self.pool = ThreadPoolExecutor(max_workers=self.cores)
+        self.pairs_per_step = self.cores * PAIRS_PER_THREAD
+
+    def _thread(self, t):
+        for a, b in self.work[t]:
+            self.o.mul_relin(a, b, self.rlk)
+
+    def step(self) -> float:
+        t0 = time.perf_counter()
+        list(self.pool.map(self._thread, range(self.cores)))
+        return time.perf_counter() - t0
+
+    def run(self, steps: int, warmup: int, budget_s: float | None = None):
+        """(median seconds per step, steps timed): at most `steps`, stopping
+        early once the timed steps exceed budget_s."""
+        for _ in range(max(1, warmup)):
+            self.step()
+        times = []
+        for _ in range(max(1, steps)):
+            times.append(self.step())
+            if budget_s is not None and sum(times) >= budget_s:
+                break
+        return statistics.median(times), len(times)
+
+    def close(self):
+        self.pool.shutdown()
+
+    def describe(self, per_step: float, steps: int) -> str:
+        return (f"{self.pairs_per_step} pairs per step ({PAIRS_PER_THREAD} per thread on {self.cores} threads), "
+                f"{steps} steps, median {per_step * 1e3:.1f} ms per step; C oracle restatement of the "
+                f"reference's multiply (kunpBFV has no CPU path)")
+
+
 def run_reference(args, world, rank):
+    """The reference arm: the CPU oracle restatement on all host cores, on our
+    arm's config, metric and unit; --steps steps after --warmup warm-up steps
+    (stopping early only if the timed steps pass CPU_STEP_BUDGET_S)."""
     if rank != 0:
         return
-    import numpy as np
-
-    import oracle
-    qs, ps = c3_primes()
-    o = oracle.Oracle(LOG_N, T, qs, ps, dnum=1)
-    sk = o.keygen_secret(SEED)
-    pk = o.keygen_public(SEED, sk)
-    rlk = o.keygen_relin(SEED, sk)
-    rng = np.random.default_rng(0)
-    cores = os.cpu_count() or 1
-    npairs = max(cores, 8)
-    cts = []
-    for i in range(npairs):
-        v1 = rng.integers(0, T, size=o.n, dtype=np.uint64)
-        v2 = rng.integers(0, T, size=o.n, dtype=np.uint64)
-        cts.append((o.encrypt(SEED, 2 * i, pk, o.encode(v1)), o.encrypt(SEED, 2 * i + 1, pk, o.encode(v2))))
-
-    def one_step():
-        from concurrent.futures import ThreadPoolExecutor
-        with ThreadPoolExecutor(max_workers=cores) as ex:
-            list(ex.map(lambda p: o.mul_relin(p[0], p[1], rlk), cts))
-
-    for _ in range(max(1, min(args.warmup, 1))):
-        one_step()
-    times = []
-    steps = max(1, min(args.steps, 5))
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        one_step()
-        times.append(time.perf_counter() - t0)
-    per_step = statistics.median(times)
-    v = npairs / per_step
+    cpu = CpuOracle(seed_rng=0)
+    per_step, steps = cpu.run(args.steps, args.warmup, budget_s=CPU_STEP_BUDGET_S)
+    cpu.close()
+    v = cpu.pairs_per_step / per_step
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ct/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"mult+relin N=16384 7x60q+1p t=65537 dnum=1, {npairs} pairs per step on CPU",
-                   "parallelism": f"{cores} host threads"},
-        "cpu_baseline": {"value": round(v, 3), "unit": "ct/s", "cores": cores, "kind": "port",
-                         "sample": f"{npairs} pairs per step, {steps} steps; kunpBFV has no CPU path, "
-                                   "so the CPU oracle restatement stands in"},
+        "config": {"workload": "mult+relin N=16384 7x60q+1p t=65537 dnum=1 (HPS tensor + hybrid key switch)",
+                   "batch_pairs_per_step": cpu.pairs_per_step, "parallelism": f"{cpu.cores} host threads"},
+        "steps_requested": args.steps,
+        "cpu_baseline": {"value": round(v, 3), "unit": "ct/s", "cores": cpu.cores, "kind": "port",
+                         "sample": cpu.describe(per_step, steps)},
         "e2e": {"value": round(v, 3), "unit": "ct/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if steps < args.steps:
+        line["steps_note"] = f"timed steps stopped at {CPU_STEP_BUDGET_S:.0f} s of CPU time"
     ref_gpu = reference_gpu_timing()
     if ref_gpu is not None:
         line["reference_gpu"] = ref_gpu
@@ -286,42 +340,14 @@ def reference_gpu_timing(reps: int = 20):
 # our arm
 # ---------------------------------------------------------------------------
 def cpu_baseline_sample(seconds=12.0):
-    """Oracle mult+relin on the host cores (bounded sample)."""
-    import numpy as np
-
-    import oracle
-    qs, ps = c3_primes()
-    o = oracle.Oracle(LOG_N, T, qs, ps, dnum=1)
-    sk = o.keygen_secret(SEED)
-    pk = o.keygen_public(SEED, sk)
-    rlk = o.keygen_relin(SEED, sk)
-    rng = np.random.default_rng(1)
-    cores = os.cpu_count() or 1
-    cts = []
-    for i in range(cores):
-        v1 = rng.integers(0, T, size=o.n, dtype=np.uint64)
-        v2 = rng.integers(0, T, size=o.n, dtype=np.uint64)
-        cts.append((o.encrypt(SEED, 2 * i, pk, o.encode(v1)), o.encrypt(SEED, 2 * i + 1, pk, o.encode(v2))))
-    done = [0]
-    lock = threading.Lock()
-    stop = time.perf_counter() + seconds
-
-    def worker(p):
-        while time.perf_counter() < stop:
-            o.mul_relin(p[0], p[1], rlk)
-            with lock:
-                done[0] += 1
-
-    t0 = time.perf_counter()
-    th = [threading.Thread(target=worker, args=(p,)) for p in cts]
-    for x in th:
-        x.start()
-    for x in th:
-        x.join()
-    el = time.perf_counter() - t0
-    return {"value": round(done[0] / el, 3), "unit": "ct/s", "cores": cores, "kind": "port",
-            "sample": f"{done[0]} pairs in {el:.1f} s on {cores} threads (CPU oracle restatement; "
-                      "kunpBFV has no CPU path)"}
+    """The CPU oracle on the host cores, by the reference arm's method, over a
+    bounded sample (about `seconds` of timed steps)."""
+    cpu = CpuOracle(seed_rng=1)
+    est = cpu.step()  # warm-up step, also the estimate of one step
+    per_step, steps = cpu.run(max(3, int(seconds / max(est, 1e-3))), 0, budget_s=seconds)
+    cpu.close()
+    return {"value": round(cpu.pairs_per_step / per_step, 3), "unit": "ct/s", "cores": cpu.cores, "kind": "port",
+            "sample": cpu.describe(per_step, steps)}
 
 
 def run_ours(args, world, rank, local):
@@ -334,8 +360,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
-    qs, ps = c3_primes()
-    ctx = kb.BFVContext(log_n=LOG_N, plain_modulus=T, q_count=NQ, q=qs, p_count=NP, p=ps, dnum=1)
+    ctx = c3_context(kb)
     sk = kb.SecretKey(ctx, SEED)
     sch = kb.BFVScheme(ctx, SEED)
     sch.addEncKey(sk)
@@ -421,7 +446,7 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and not args.skip_extras:
         try:
-            line.update(extras(args, ctx, sch, c1, c2, out, stream, dev))
+            line.update(extras(args, ctx, sch, c1, c2, out, stream, dev, ms))
         except Exception as e:  # report, keep the headline line
             line["extras_error"] = repr(e)
         try:
@@ -438,6 +463,49 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def step_roofline(ms_step, hbm_peak, peak_kind):
+    """The headline step against the IMAD bound: every primitive of the 9-kernel
+    pipeline counted per pair (kunpbfv_b200.roofline.pipeline_counts), each at
+    the rate kbfv_probe_arith measures for it live on this GPU; and, from the
+    committed ncu summary of the same kernel sources, the IMAD-pipe instructions
+    per pair against the measured IMAD issue rate. Beside them the step's HBM
+    rate (inputs, outputs and the key read once per launch)."""
+    from kunpbfv_b200 import roofline as rl
+    from kunpbfv_b200.api import probe_arith
+    pc = rl.pipeline_counts(1 << LOG_N, LOG_N, NQ, NP, 1)
+    rates = {k: probe_arith(kind) * 1e9 for k, kind in rl.PROBE_KIND.items()}
+    floor_s = rl.arithmetic_floor_s(pc["counts"], rates)
+    step_s = ms_step / 1e3
+    n = 1 << LOG_N
+    bytes_pair = 4 * NQ * n * 8 + 2 * NQ * n * 8 + 2 * (NQ + NP) * n * 8 // BATCH
+    out = {"bound": "imad", "unit": "modmul/s",
+           "modmuls_per_pair": pc["products"],
+           "reductions_per_pair": pc["counts"]["b128"],
+           "counts_per_pair": pc["counts"], "ntt_rows_per_pair": pc["ntt_rows"], "formula": pc["formula"],
+           "achieved": round(pc["products"] * BATCH / step_s, 0),
+           "peak": round(pc["products"] / floor_s, 0),
+           "frac": round(floor_s * BATCH / step_s, 4),
+           "floor_ms_per_step": round(floor_s * BATCH * 1e3, 4), "ms_per_step": round(ms_step, 4),
+           "peak_source": "each class at its kbfv_probe_arith rate (register chains, no memory traffic): " +
+                          ", ".join(f"{k} kind {v}" for k, v in rl.PROBE_KIND.items()),
+           "rates_gops": {k: round(v / 1e9, 1) for k, v in rates.items()},
+           "hbm": {"bytes_per_pair": bytes_pair, "achieved_gbs": round(bytes_pair * BATCH / step_s / 1e9, 1),
+                   "frac": round(bytes_pair * BATCH / step_s / 1e9 / hbm_peak, 4), "peak_kind": peak_kind}}
+    imad_peak = probe_arith(12) * 1e9 / 32  # warp-level IMAD instructions per second
+    prof = rl.read_profile("mult_relin_imad_n16384.md")
+    imad = {"unit": "warp inst/s", "peak": round(imad_peak, 0),
+            "peak_source": "kbfv_probe_arith(12): dependent 32-bit multiply-adds, 8 chains per thread"}
+    if rl.profile_matches(prof):
+        ipp = float(prof["fmaheavy_warp_inst_per_pair"])
+        imad.update({"inst_per_pair": ipp, "achieved": round(ipp * BATCH / step_s, 0),
+                     "frac": round(ipp * BATCH / step_s / imad_peak, 4),
+                     "source": "profiles/mult_relin_imad_n16384.md (sm__inst_executed_pipe_fmaheavy.sum)"})
+    else:
+        imad["note"] = "no ncu summary of the current kernel sources"
+    out["imad"] = imad
+    return out
+
+
 def time_cuda(fn, stream, iters, warm=2):
     import torch
     for _ in range(warm):
@@ -452,7 +520,7 @@ def time_cuda(fn, stream, iters, warm=2):
     return a.elapsed_time(b) / iters
 
 
-def extras(args, ctx, sch, c1, c2, out, stream, dev):
+def extras(args, ctx, sch, c1, c2, out, stream, dev, ms_step):
     import torch
 
     import kunpbfv_b200 as kb
@@ -606,10 +674,16 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
     ach = alg / (ms_ntt / 1e3) / 1e9
     bfly = rows * (N // 2) * LOG_N
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of this launch at
-    # 2048 rows, from one ncu capture of `bench.py --kernel ntt16k --rows 2048`
-    traffic = 270470912 + 208796416 if rows == 2048 else None
+    # 2048 rows, from the committed ncu summary of the same kernel sources
+    from kunpbfv_b200 import roofline as rl
+    prof = rl.read_profile("ntt_fwd_block_n16384.md")
+    traffic = None
+    if rl.profile_matches(prof) and rows == int(prof.get("traffic_rows", 0)):
+        traffic = int(prof["traffic_bytes"])
     res["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                        "frac": round(ach / peak, 4), "traffic": traffic,
+                       "traffic_source": ("profiles/ntt_fwd_block_n16384.md (ncu capture of these kernel sources)"
+                                          if traffic is not None else "no ncu summary of the current kernel sources"),
                        "kernel": f"ntt_fwd_block_kernel<14> on {rows} rows ({peak_kind} peak)",
                        "ms_per_launch": round(ms_ntt, 4),
                        "algorithmic_bytes": alg,
@@ -626,10 +700,10 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev):
                                 "frac": round(bfly / (ms_ntt / 1e3) / bfly_peak, 4),
                                 "peak_source": "kbfv_probe_arith(11): the kernels' 60-bit forward butterfly in register chains"}
     del x
+    res["roofline"]["step"] = step_roofline(ms_step, peak, peak_kind)
 
     # standalone NTT, N=65536, 32 primes x 64 polynomials (1 GiB)
-    qs2 = __import__("oracle").primes_bits(1 << 16, 60, 34)
-    ctx2 = kb.BFVContext(log_n=16, plain_modulus=786433, q_count=32, q=qs2[2:34], p_count=1, p=qs2[:1], dnum=1)
+    ctx2 = kb.BFVContext.from_bits(16, [60] * 32, [60], 786433, dnum=1)
     mods = torch.tensor(ctx2.q, dtype=torch.int64, device=dev)
     y = torch.randint(0, 1 << 62, (64, 32, 1 << 16), dtype=torch.int64, device=dev)
     y = torch.remainder(y, mods.view(1, 32, 1))

@@ -90,8 +90,9 @@ const char* kbfv_version(void);
  * 7: 32x32->64 multiply-add, 8: 32x32 high product, 9: 32-bit multiply-add,
  * 10: 64x64->128 multiply-accumulate from 32-bit partial products with carry
  * chains, 11: forward NTT butterfly from 32-bit partial products (the one the
- * NTT kernels use). The roofline
- * of the IMAD-bound kernels. */
+ * NTT kernels use), 12: 32-bit multiply-add issue rate (16 dependent
+ * multiply-adds per chain step: the IMAD pipe's peak). The roofline of the
+ * IMAD-bound kernels. */
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops);
 
 /* ---- context ---------------------------------------------------------

@@ -869,7 +869,8 @@ PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64",
                "forward NTT butterfly from 64-bit multiplies",
                "Shoup product", "128-bit Barrett", "one-high-product Barrett", "32x32->64 multiply-add",
                "32x32 high product", "32-bit multiply-add", "64x64->128 multiply-accumulate from 32-bit parts",
-               "forward NTT butterfly from 32-bit parts (the kernels')"]
+               "forward NTT butterfly from 32-bit parts (the kernels')",
+               "32-bit multiply-add issue rate (IMAD pipe)"]
 
 
 def probe_arith(kind: int, iters: int = 4096) -> float:

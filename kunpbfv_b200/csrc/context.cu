@@ -441,8 +441,10 @@ uint8_t* ensure_scratch(Context& c, size_t bytes) {
 // 5: 128-bit Barrett, 6: one-high-product Barrett, 7: 32x32->64 multiply-add,
 // 8: 32x32 high product, 9: 32-bit multiply-add, 10: mac32 (64x64->128
 // multiply-accumulate from 32-bit partial products), 11: forward butterfly
-// with shoup4_32 (the NTT kernels' butterfly).
+// with shoup4_32 (the NTT kernels' butterfly), 12: 32-bit multiply-add issue
+// rate (16 dependent mad.lo.u32 per chain step, the IMAD pipe's peak).
 constexpr int kProbeChains = 8;
+constexpr int kImadPerStep = 16;
 template <int KIND>
 __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_t mh, uint64_t ml, uint64_t mp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -475,6 +477,13 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
             if (KIND == 8) acc[c].lo += __umulhi((uint32_t)a[c], (uint32_t)b[c]);
             if (KIND == 9) acc[c].lo = (uint32_t)a[c] * (uint32_t)b[c] + (uint32_t)acc[c].lo;
             if (KIND == 10) mac32(acc[c], a[c], b[c]);
+            if (KIND == 12) {  // IMAD issue: 16 multiply-adds per chain step, one bookkeeping update
+                uint32_t x = (uint32_t)acc[c].lo;
+                const uint32_t m = (uint32_t)b[c] | 1u, k = (uint32_t)a[c];
+#pragma unroll
+                for (int u = 0; u < kImadPerStep; u++) x = x * m + k;
+                acc[c].lo = x;
+            }
             if (KIND == 11) {  // the NTT kernels' butterfly (Shoup product from 32-bit multiplies)
                 uint64_t x = a[c], y = b[c];
                 ct_bfly(x, y, tw_t{b[c], a[c]}, q, q << 2);
@@ -714,7 +723,7 @@ int kbfv_set_seed(kbfv_context* ctx, const uint8_t seed[32]) {
 
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
     return guarded([&] {
-        KB_REQUIRE(kind >= 0 && kind <= 11 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
+        KB_REQUIRE(kind >= 0 && kind <= 12 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
         int dev = 0, sms = 0;
         KB_CHECK_CUDA(cudaGetDevice(&dev));
         KB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -733,7 +742,7 @@ int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
             KB_CHECK_CUDA(cudaEventRecord(e0));
             switch (kind) {
 #define P_K(K) case K: probe_arith_kernel<K><<<blocks, threads>>>(out, (int)iters, q, mh, ml, mp); break;
-                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7) P_K(8) P_K(9) P_K(10) P_K(11)
+                P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7) P_K(8) P_K(9) P_K(10) P_K(11) P_K(12)
 #undef P_K
             }
             KB_CHECK_CUDA(cudaEventRecord(e1));
@@ -744,7 +753,7 @@ int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
         cudaEventDestroy(e1);
         cudaFree(out);
         check_launch("probe_arith");
-        *gops = (double)blocks * threads * iters * kProbeChains / (ms * 1e6);
+        *gops = (double)blocks * threads * iters * kProbeChains * (kind == 12 ? kImadPerStep : 1) / (ms * 1e6);
     });
 }
 

@@ -5,7 +5,7 @@ slots), so the oracle is pinned by (a) independent restatements of the
 definitions it claims (naive NTT evaluation, schoolbook negacyclic product,
 big-integer CRT), (b) libsodium's XSalsa20 through PyNaCl, and (c) the
 committed fixtures in tests/golden/ produced by the reference's own kernels
-(see tests/golden/README.md).
+(the recipe is in the docstring of tests/golden/make_ref_fixtures.py).
 """
 import numpy as np
 import pytest
