@@ -1,7 +1,10 @@
 // kbfv_compat.hpp -- kunpBFV's class API (BFVContext, BFVScheme, Plaintext,
 // Ciphertext, SecretKey) rebuilt on the C ABI in kbfv.h, so drivers written for
-// kunpBFV (correct_mult.cu, perf_mult.cu) run on the B200 path with only their
-// #includes changed. Header-only; link libkbfv.so and cudart.
+// kunpBFV (correct_mult.cu, perf_mult.cu, ...) run on the B200 path. Unmodified
+// drivers compile against the include tree include/kunpbfv/ (its include/*.cuh
+// forward the reference's header names here and put the classes in the global
+// namespace); new code can include this header and use namespace kbfv_compat.
+// Header-only; link libkbfv.so and cudart.
 //
 // Behaviour kept from the reference: encode() overwrites its input with the
 // plaintext coefficients (include/Encoder.cuh:32), encode_ntt() takes
@@ -20,6 +23,7 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "kbfv.h"
@@ -41,35 +45,127 @@ inline void check_cuda(cudaError_t e) {
 
 class BFVContext;
 
+// A device buffer of `words` uint64 words that copies deeply: copy construction
+// and assignment allocate their own buffer (reallocating when the size differs)
+// and copy the contents device to device, like the reference's Plaintext and
+// Ciphertext (include/Plaintext.cuh:21-48, include/Ciphertext.cuh:42-78);
+// moves hand the buffer over.
+struct DeviceWords {
+    uint64_tt* p = nullptr;
+    size_t words = 0;
+    DeviceWords() = default;
+    explicit DeviceWords(size_t n, bool zero) { reset(n, zero); }
+    DeviceWords(const DeviceWords& o) { copy_from(o); }
+    DeviceWords(DeviceWords&& o) noexcept : p(o.p), words(o.words) { o.p = nullptr; o.words = 0; }
+    DeviceWords& operator=(const DeviceWords& o) {
+        if (this != &o) copy_from(o);
+        return *this;
+    }
+    DeviceWords& operator=(DeviceWords&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p; words = o.words;
+            o.p = nullptr; o.words = 0;
+        }
+        return *this;
+    }
+    ~DeviceWords() { release(); }
+    void reset(size_t n, bool zero) {
+        if (n != words) {
+            release();
+            if (n) check_cuda(cudaMalloc(&p, sizeof(uint64_tt) * n));
+            words = n;
+        }
+        if (zero && n) check_cuda(cudaMemset(p, 0, sizeof(uint64_tt) * n));
+    }
+    void copy_from(const DeviceWords& o) {
+        reset(o.words, false);
+        if (o.words) check_cuda(cudaMemcpy(p, o.p, sizeof(uint64_tt) * o.words, cudaMemcpyDeviceToDevice));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        words = 0;
+    }
+};
+
 class Plaintext {
+    DeviceWords buf_;
+
 public:
     uint64_tt* mx_device = nullptr;  // (L+1) x N words: coefficients in the first N, or NTT form over Q
     int N = 0, L = 0, l = 0, slots = 0;
     Plaintext() = default;
-    Plaintext(int N_, int L_, int l_, int slots_) : N(N_), L(L_), l(l_), slots(slots_) {
-        check_cuda(cudaMalloc(&mx_device, sizeof(uint64_tt) * N * (L + 1)));
-        check_cuda(cudaMemset(mx_device, 0, sizeof(uint64_tt) * N * (L + 1)));
+    Plaintext(int N_, int L_, int l_, int slots_)
+        : buf_((size_t)N_ * (L_ + 1), true), N(N_), L(L_), l(l_), slots(slots_) {
+        mx_device = buf_.p;
     }
-    Plaintext(const Plaintext&) = delete;
-    Plaintext& operator=(const Plaintext&) = delete;
-    ~Plaintext() { if (mx_device) cudaFree(mx_device); }
+    // host values (N x (L+1) words) copied in (include/Plaintext.cuh:13-18)
+    Plaintext(uint64_tt* m_host, int N_, int L_, int l_, int slots_) : Plaintext(N_, L_, l_, slots_) {
+        check_cuda(cudaMemcpy(mx_device, m_host, sizeof(uint64_tt) * buf_.words, cudaMemcpyHostToDevice));
+    }
+    Plaintext(const Plaintext& o) : buf_(o.buf_), N(o.N), L(o.L), l(o.l), slots(o.slots) { mx_device = buf_.p; }
+    Plaintext(Plaintext&& o) noexcept : buf_(std::move(o.buf_)), N(o.N), L(o.L), l(o.l), slots(o.slots) {
+        mx_device = buf_.p;
+        o.mx_device = nullptr;
+    }
+    Plaintext& operator=(const Plaintext& o) {
+        if (this == &o) return *this;
+        buf_ = o.buf_;
+        N = o.N; L = o.L; l = o.l; slots = o.slots;
+        mx_device = buf_.p;
+        return *this;
+    }
+    Plaintext& operator=(Plaintext&& o) noexcept {
+        if (this == &o) return *this;
+        buf_ = std::move(o.buf_);
+        N = o.N; L = o.L; l = o.l; slots = o.slots;
+        mx_device = buf_.p;
+        o.mx_device = nullptr;
+        return *this;
+    }
+    virtual ~Plaintext() = default;
 };
 
 class Ciphertext {
+    DeviceWords buf_;
+    void bind() {
+        cipher_device = buf_.p;
+        ax_device = cipher_device;
+        bx_device = cipher_device ? cipher_device + (size_t)N * (L + 1) : nullptr;
+    }
+
 public:
     uint64_tt* cipher_device = nullptr;  // [ax | bx], (L+1) x N words each, NTT form over Q
     uint64_tt* ax_device = nullptr;
     uint64_tt* bx_device = nullptr;
     int N = 0, L = 0, l = 0, slots = 0;
     Ciphertext() = default;
-    Ciphertext(int N_, int L_, int l_, int slots_) : N(N_), L(L_), l(l_), slots(slots_) {
-        check_cuda(cudaMalloc(&cipher_device, sizeof(uint64_tt) * N * (L + 1) * 2));
-        ax_device = cipher_device;
-        bx_device = cipher_device + (size_t)N * (L + 1);
+    Ciphertext(int N_, int L_, int l_, int slots_)
+        : buf_((size_t)N_ * (L_ + 1) * 2, false), N(N_), L(L_), l(l_), slots(slots_) {
+        bind();
     }
-    Ciphertext(const Ciphertext&) = delete;
-    Ciphertext& operator=(const Ciphertext&) = delete;
-    ~Ciphertext() { if (cipher_device) cudaFree(cipher_device); }
+    Ciphertext(const Ciphertext& o) : buf_(o.buf_), N(o.N), L(o.L), l(o.l), slots(o.slots) { bind(); }
+    Ciphertext(Ciphertext&& o) noexcept : buf_(std::move(o.buf_)), N(o.N), L(o.L), l(o.l), slots(o.slots) {
+        bind();
+        o.bind();
+    }
+    Ciphertext& operator=(const Ciphertext& o) {
+        if (this == &o) return *this;
+        buf_ = o.buf_;
+        N = o.N; L = o.L; l = o.l; slots = o.slots;
+        bind();
+        return *this;
+    }
+    Ciphertext& operator=(Ciphertext&& o) noexcept {
+        if (this == &o) return *this;
+        buf_ = std::move(o.buf_);
+        N = o.N; L = o.L; l = o.l; slots = o.slots;
+        bind();
+        o.bind();
+        return *this;
+    }
+    virtual ~Ciphertext() = default;
 };
 
 class BFVContext {
@@ -127,6 +223,8 @@ private:
 };
 
 class SecretKey {
+    DeviceWords buf_;
+
 public:
     uint64_tt* sx_device = nullptr;  // (K+L+1) x N words, NTT form over Q|P
     int N = 0, L = 0, K = 0;
@@ -140,12 +238,24 @@ public:
             std::random_device rd;
             for (int i = 0; i < 32; i++) seed[i] = (uint8_t)rd();
         }
-        check_cuda(cudaMalloc(&sx_device, sizeof(uint64_tt) * N * (K + L + 1)));
+        buf_.reset((size_t)N * (K + L + 1), false);
+        sx_device = buf_.p;
         check(kbfv_keygen_secret(ctx.handle, seed, 1, 64, reinterpret_cast<uint64_t*>(sx_device), stream));
     }
-    SecretKey(const SecretKey&) = delete;
-    SecretKey& operator=(const SecretKey&) = delete;
-    ~SecretKey() { if (sx_device) cudaFree(sx_device); }
+    // deep copies (the reference's SecretKey copies shallowly and frees twice)
+    SecretKey(const SecretKey& o) : buf_(o.buf_), N(o.N), L(o.L), K(o.K) {
+        sx_device = buf_.p;
+        std::memcpy(seed, o.seed, 32);
+    }
+    SecretKey& operator=(const SecretKey& o) {
+        if (this == &o) return *this;
+        buf_ = o.buf_;
+        N = o.N; L = o.L; K = o.K;
+        std::memcpy(seed, o.seed, 32);
+        sx_device = buf_.p;
+        return *this;
+    }
+    virtual ~SecretKey() = default;
 };
 
 class BFVScheme {

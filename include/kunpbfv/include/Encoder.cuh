@@ -1,0 +1,5 @@
+// Drop-in for kunpBFV's include/Encoder.cuh: a driver written for the reference
+// (#include "include/Encoder.cuh") compiles unmodified with -I <this repo>/include/kunpbfv
+// and runs on libkbfv.so.
+#pragma once
+#include "../../kbfv_compat_global.hpp"

@@ -89,3 +89,23 @@ def test_compat_header_compiles_and_links(tmp_path):
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert out.exists()
+
+
+REF = "/root/reference"
+DRIVERS = ["correct_mult", "correct_add", "correct_encrypt", "perf_mult", "perf_add", "perf_encrypt", "bfv_demo"]
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "include")), reason="reference sources absent")
+def test_reference_drivers_compile_unmodified(tmp_path):
+    """The reference's seven driver programs compile, byte for byte as they
+    are, against the drop-in headers include/kunpbfv/ and link to libkbfv.so
+    (the recipe is oracle/Makefile's `drivers` target)."""
+    import subprocess
+    from kunpbfv_b200 import build
+    build.build()
+    out = tmp_path / "drivers"
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s", "drivers", f"DRIVER_OUT={out}"],
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for d in DRIVERS:
+        assert (out / d).exists(), d

@@ -1,12 +1,20 @@
-"""A C++ driver in the reference's style, built against include/kbfv_compat.hpp
-and libkbfv.so, runs the full encode/encrypt/multiply/decrypt flow on the GPU."""
+"""The boundary on the GPU: C++ drivers built against the reference's class API
+(include/kbfv_compat.hpp) run the full encode/encrypt/multiply/decrypt flow.
+
+- a reference-style driver (tests/cpp/compat_mult.cpp) checks every slot;
+- the reference's own driver programs, compiled unmodified against the drop-in
+  headers include/kunpbfv/ (oracle/Makefile `drivers`, built into
+  oracle/_ref/drivers/ where the reference sources are present), print their
+  expected and decrypted slots, which must agree."""
 import os
+import re
 import subprocess
 
 import pytest
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER_DIR = os.path.join(ROOT, "oracle", "_ref", "drivers")
 
 
 @pytest.fixture(scope="module")
@@ -26,3 +34,46 @@ def test_reference_style_driver(driver, n):
     print(r.stdout, r.stderr)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "wrong=0" in r.stdout
+
+
+def _run_reference_driver(name):
+    exe = os.path.join(DRIVER_DIR, name)
+    if not os.path.exists(exe):
+        pytest.skip("the reference's drivers were not built (reference sources absent when oracle/ was built)")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=900)
+    print(r.stdout[-3000:], r.stderr[-3000:])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return r.stdout
+
+
+def _slots(out, label):
+    m = re.search(label + r":\s*([0-9 ]+)", out)
+    assert m, f"no '{label}' line in the driver's output"
+    return [int(x) for x in m.group(1).split()]
+
+
+@pytest.mark.parametrize("name", ["correct_mult", "correct_add", "correct_encrypt"])
+def test_reference_correctness_driver_unmodified(name):
+    """The reference's correct_*.cu print 8 expected and 8 decrypted slots
+    (correct_mult: m1*m2*m1, correct_add: m1+m2+m1, correct_encrypt: m);
+    on libkbfv.so they agree."""
+    out = _run_reference_driver(name)
+    want, got = _slots(out, "预期结果"), _slots(out, "实际结果")
+    assert len(want) == len(got) == 8
+    assert want == got, (want, got)
+
+
+@pytest.mark.parametrize("name", ["perf_mult", "perf_add", "perf_encrypt"])
+def test_reference_perf_driver_unmodified(name):
+    """The reference's perf_*.cu time their operations with CUDA events over 40
+    rounds after 10 warm-up rounds; every reported time is positive."""
+    out = _run_reference_driver(name)
+    times = [float(x) for x in re.findall(r"\(us\):\s*([0-9.]+)\s*avg", out)]
+    assert times and all(t > 0 for t in times), out
+
+
+def test_reference_demo_unmodified():
+    """bfv_demo.cu runs its 100 iterations of encode / encrypt / add / multiply /
+    decrypt and prints its checks."""
+    out = _run_reference_driver("bfv_demo")
+    assert "HMULT" in out and "CADD" in out
