@@ -463,6 +463,51 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def c4_uneven(stream):
+    """Config C4: N=32768, 14 x 60-bit q + 2 x 60-bit special primes, digits of
+    5 primes (dnum 3); 16 pairs at 14, 13, 12 and 11 live primes (4 each) in one
+    kbfv_mul_relin_levels call (one launch sequence over the mixed levels),
+    against the same pairs as four batched calls, one per level."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200 import tune
+    from kunpbfv_b200.api import VP, _ptr, lib
+    ctx = kb.BFVContext.from_bits(15, [60] * 14, [60, 60], T, dnum=3)
+    sk = kb.SecretKey(ctx, SEED)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addMultKey_23(sk)
+    pairs, outs = [], []
+    for j in range(16):
+        lv = ctx.at_level(14 - j % 4)
+        pairs.append((kb.Ciphertext(lv, tune._random_pairs(lv, 1, 10 + j)),
+                      kb.Ciphertext(lv, tune._random_pairs(lv, 1, 50 + j))))
+        outs.append(kb.Ciphertext(lv, count=1))
+    ms_one = time_cuda(lambda: sch.mult_relin_levels(pairs, outs=outs, stream=stream), stream, 10)
+    one = [o.cipher_device.clone() for o in outs]
+    groups = {}
+    for j, (a, b) in enumerate(pairs):
+        groups.setdefault(a.ctx.q_count, []).append(j)
+
+    def per_level():
+        for live, js in groups.items():
+            n = len(js)
+            A = (VP * n)(*[_ptr(pairs[j][0].cipher_device) for j in js])
+            B = (VP * n)(*[_ptr(pairs[j][1].cipher_device) for j in js])
+            O = (VP * n)(*[_ptr(outs[j].cipher_device) for j in js])
+            lib().kbfv_mul_relin_batch(ctx.at_level(live).handle, _ptr(sch.rlk), A, B, O, n, stream.cuda_stream)
+
+    ms_lv = time_cuda(per_level, stream, 10)
+    same = all(torch.equal(x, o.cipher_device) for x, o in zip(one, outs))
+    ctx.close()
+    return {"pairs": 16, "levels": [14, 13, 12, 11], "one_call_ms": round(ms_one, 4),
+            "one_call_ct_per_s": round(16 / ms_one * 1e3, 1), "per_level_calls_ms": round(ms_lv, 4),
+            "bit_identical": bool(same),
+            "form": "kbfv_mul_relin_levels: one launch sequence over the mixed levels (9 pipeline stages, "
+                    "each NTT a column pass + 2^12-point blocks at N=32768); per_level_calls: four "
+                    "kbfv_mul_relin_batch calls on the level contexts, one after another"}
+
+
 def step_roofline(ms_step, hbm_peak, peak_kind):
     """The headline step against the IMAD bound: every primitive of the 9-kernel
     pipeline counted per pair (kunpbfv_b200.roofline.pipeline_counts), each at
@@ -643,6 +688,8 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev, ms_step):
         rctx.close()
     res["reference_params"] = dict(refp, form="T-base key switch (bit-exact with the reference's genuine "
                                               "multiply); per-op: one pair per call; batched: 64 pairs per call")
+
+    res["c4_uneven"] = c4_uneven(stream)
 
     # e2e through the C ABI with page-locked host buffers: kbfv_mul_relin_host
     # copies each chunk in, multiplies it and copies its products out, the

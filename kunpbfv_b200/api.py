@@ -821,10 +821,13 @@ class BFVScheme:
             ct = self.mod_switch(ct, stream)
         return ct
 
-    def mult_relin_levels(self, pairs, stream=None):
-        """[(ct_a, ct_b)] at possibly different levels -> products, one call"""
+    def mult_relin_levels(self, pairs, outs=None, stream=None):
+        """[(ct_a, ct_b)] at possibly different levels -> products, one call (one
+        launch sequence for up to 128 pairs in up to 8 levels); `outs` may give
+        the output ciphertexts (each at its pair's level)"""
         n = len(pairs)
-        outs = [Ciphertext(a.ctx, count=1) for a, _ in pairs]
+        if outs is None:
+            outs = [Ciphertext(a.ctx, count=1) for a, _ in pairs]
         lv = (C.c_uint32 * n)(*[a.ctx.q_count for a, _ in pairs])
         A = (VP * n)(*[_ptr(a.cipher_device) for a, _ in pairs])
         B = (VP * n)(*[_ptr(b.cipher_device) for _, b in pairs])

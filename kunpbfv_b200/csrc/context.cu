@@ -568,11 +568,7 @@ int kbfv_context_destroy(kbfv_context* ctx) {
                 if (e) cudaEventDestroy(e);
         }
         if (c.hfork) cudaEventDestroy(c.hfork);
-        for (int i = 0; i < 3; i++) {
-            if (c.lane[i]) cudaStreamDestroy(c.lane[i]);
-            if (c.lane_join[i]) cudaEventDestroy(c.lane_join[i]);
-        }
-        if (c.lane_fork) cudaEventDestroy(c.lane_fork);
+        if (c.d_level_consts) cudaFree(c.d_level_consts);
         delete ctx;
     });
 }

@@ -130,9 +130,11 @@ struct Context {
     cudaEvent_t hin[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t hcomp[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t hout[4] = {nullptr, nullptr, nullptr, nullptr};
-    // batches of pairs at several levels: one lane (stream) per level group
-    cudaStream_t lane[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t lane_fork = nullptr, lane_join[3] = {nullptr, nullptr, nullptr};
+    // batches of pairs at several levels run as one launch sequence: slot l of
+    // this device array holds the DevConsts of the level with l live primes (the
+    // top level's own in slot nq), uploaded when that level is first used
+    DevConsts* d_level_consts = nullptr;
+    std::vector<uint8_t> level_uploaded;
 };
 
 }  // namespace kbfv

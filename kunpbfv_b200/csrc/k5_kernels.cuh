@@ -3,7 +3,7 @@
 // prime count (MAXQ) is instantiated in its own translation unit
 // (k5_m<MAXQ>.cu) so that the unrolled variants compile in parallel.
 #pragma once
-#include "pipeline.cuh"
+#include "mixed.cuh"
 
 // K5 in one kernel, for launches of one or two pairs (one launch less on the
 // per-call path): scale-and-round to R, R -> Q, and (mode 1) the key-switch
@@ -132,4 +132,84 @@ void k5_launch_m(const DevConsts& dc, int count, const MulScratch& m, uint64_t* 
         k5_lift_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sb, out0, m.sd, m.sd2, mode);
     }
     check_launch("k5_round");
+}
+
+// ---- mixed-level batches (see mixed.cuh): the level of each CTA's item
+// chooses the constants; scratch has the top level's per-item layout ----------
+
+// K5a over a mixed batch: grid.y = item x 3 tensor polynomials
+template <int MAXQ>
+static __global__ void k5_scale_mixed_kernel(Groups G, const uint64_t* __restrict__ sc, uint64_t* __restrict__ rr_out) {
+    __shared__ DevConsts c;
+    const int item = blockIdx.y / 3, which = blockIdx.y % 3, g = G.group_of_item(item);
+    load_level_consts(c, G.lv[g]);
+    const int logn = G.logn;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t* src = sc + (((size_t)item * 3 * G.top_nqr + (size_t)which * c.nqr) << logn);
+    uint64_t xq[MAXQ], xr[MAXQ + 1], rr[MAXQ + 1];
+#pragma unroll
+    for (int i = 0; i < MAXQ; i++)
+        if (i < c.nq) xq[i] = src[((size_t)i << logn) + k];
+#pragma unroll
+    for (int j = 0; j < MAXQ + 1; j++)
+        if (j < c.nr) xr[j] = src[((size_t)(c.nq + j) << logn) + k];
+    scale_round_coeff<MAXQ>(c, xq, xr, rr);
+    uint64_t* dst = rr_out + (((size_t)item * 3 * G.top_nr + (size_t)which * c.nr) << logn);
+#pragma unroll
+    for (int j = 0; j < MAXQ + 1; j++)
+        if (j < c.nr) dst[((size_t)j << logn) + k] = rr[j];
+}
+
+// K5b over a mixed batch: R -> Q; a1*a2 lifted into the digits (sd2), the cross
+// term and b1*b2 to sd
+template <int MAXQ>
+static __global__ void k5_lift_mixed_kernel(Groups G, const uint64_t* __restrict__ rr_in, uint64_t* __restrict__ sd,
+                                            uint64_t* __restrict__ sd2) {
+    __shared__ DevConsts c;
+    const int item = blockIdx.y / 3, which = blockIdx.y % 3, g = G.group_of_item(item);
+    load_level_consts(c, G.lv[g]);
+    const int logn = G.logn;
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t* src = rr_in + (((size_t)item * 3 * G.top_nr + (size_t)which * c.nr) << logn);
+    uint64_t rr[MAXQ + 1], xq[MAXQ];
+#pragma unroll
+    for (int j = 0; j < MAXQ + 1; j++)
+        if (j < c.nr) rr[j] = src[((size_t)j << logn) + k];
+    const BconvTables tb = r2q_tables(c);
+    uint64_t y[MAXQ + 1];
+    const long long v = bconv_prep<MAXQ + 1>(y, rr, tb.nin, tb.in_mods, tb.hatinv, tb.hatinvs, tb.binv);
+#pragma unroll
+    for (int i = 0; i < MAXQ; i++) {
+        if (i < c.nq)
+            xq[i] = bconv_out<MAXQ + 1>(y, tb.nin, tb.hat + (size_t)i * tb.nin, tb.alpha[v * tb.nout + i],
+                                        c.mods[i], c.mu_hi[i], c.mu_lo[i]);
+    }
+    if (which == 0) {
+        modup_coeff<MAXQ>(c, xq, sd2 + (((size_t)item * G.top_dnum * G.top_npq) << logn), k);
+    } else {
+        uint64_t* dst = sd + (((size_t)item * 2 * G.top_nq + (size_t)(which - 1) * c.nq) << logn);
+#pragma unroll
+        for (int i = 0; i < MAXQ; i++)
+            if (i < c.nq) dst[((size_t)i << logn) + k] = xq[i];
+    }
+}
+
+// K2 (Q -> R) of a mixed batch; MAXQ bounds the top level's ciphertext primes + 1
+template <int MAXQ>
+void bconv_mixed_launch_m(const Groups& G, int count, const MulScratch& m, cudaStream_t st) {
+    const int threads = 256;
+    dim3 grid((unsigned)((1u << G.logn) / threads), (unsigned)(count * 4));
+    const size_t sh = (size_t)G.top_nq * G.top_nr * 8;
+    bconv_mixed_kernel<MAXQ><<<grid, threads, sh, st>>>(G, m.sa, m.sb);
+    check_launch("bconv_mixed");
+}
+
+// K5a + K5b of a mixed batch
+template <int MAXQ>
+void k5_mixed_launch_m(const Groups& G, int count, const MulScratch& m, cudaStream_t st) {
+    const int threads = 128;
+    dim3 grid((unsigned)((1u << G.logn) / threads), (unsigned)(count * 3));
+    k5_scale_mixed_kernel<MAXQ><<<grid, threads, 0, st>>>(G, m.sc, m.sb);
+    k5_lift_mixed_kernel<MAXQ><<<grid, threads, 0, st>>>(G, m.sb, m.sd, m.sd2);
+    check_launch("k5_mixed");
 }

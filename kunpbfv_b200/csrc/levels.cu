@@ -1,7 +1,9 @@
 // libkbfv: levels (contexts for fewer live primes), the BFV modulus switch,
 // multiplies of batches at mixed levels, key switching over a gadget
 // decomposition, and Galois automorphisms.
-#include "pipeline.cuh"
+#include <numeric>
+
+#include "mixed.cuh"
 
 // ---- modulus switch (divide by the last prime and round) ---------------------
 struct LastLimbSrc {  // row = polynomial: its last limb
@@ -70,6 +72,114 @@ struct GaloisASrc {
         return GaloisRow{ct + (((size_t)item * 2 * nq + l) << logn), g, logn};
     }
 };
+
+// ---- multiplies of batches at mixed levels (see mixed.cuh) -------------------
+// The DevConsts of the level with `live` primes in the top context's device
+// array: the level context is built and its constants uploaded on first use
+// (synchronous copies: make a first call per level before any stream capture).
+static const DevConsts* level_consts(kbfv_context* top_h, Context& top, int live) {
+    if (!top.d_level_consts) {
+        KB_CHECK_CUDA(cudaMalloc(&top.d_level_consts, sizeof(DevConsts) * (size_t)(top.nq + 1)));
+        top.level_uploaded.assign((size_t)top.nq + 1, 0);
+    }
+    if (!top.level_uploaded[live]) {
+        kbfv_context* lv = nullptr;
+        const int rc = kbfv_context_at_level(top_h, (uint32_t)live, &lv);
+        if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
+        KB_CHECK_CUDA(cudaMemcpy(top.d_level_consts + live, &lv->c.dc, sizeof(DevConsts), cudaMemcpyHostToDevice));
+        top.level_uploaded[live] = 1;
+    }
+    return top.d_level_consts + live;
+}
+
+static Groups groups_header(const Context& top) {
+    Groups G;
+    std::memset(&G, 0, sizeof G);
+    G.logn = top.logn;
+    G.np = top.np;
+    G.top_nq = top.nq;
+    G.top_nr = top.nr;
+    G.top_npq = top.nq + top.np;
+    G.top_nqr = top.nq + top.nr;
+    G.top_dnum = top.dnum;
+    G.key_nq = top.nq;
+    G.key_npq = top.nq + top.np;
+    G.dp = fast_div((uint32_t)top.np);
+    return G;
+}
+
+// open group G.ng for level `lvl`, its first item `first`
+static void add_group(kbfv_context* top_h, Context& top, Groups& G, int lvl, int first) {
+    const int g = G.ng++;
+    G.first[g] = first;
+    G.lv[g] = level_consts(top_h, top, lvl);
+    G.nq[g] = lvl;
+    G.nr[g] = lvl + 1;
+    G.npq[g] = lvl + top.np;
+    G.nqr[g] = 2 * lvl + 1;
+    G.dnum[g] = (lvl + top.alpha - 1) / top.alpha;  // the level keeps the top level's digit size
+    G.dq[g] = fast_div((uint32_t)G.nq[g]);
+    G.dr[g] = fast_div((uint32_t)G.nr[g]);
+    G.dpq[g] = fast_div((uint32_t)G.npq[g]);
+    G.dqr[g] = fast_div((uint32_t)G.nqr[g]);
+}
+
+// rows of a stage with per(g) rows per item of group g
+template <class F>
+static StageRows stage_rows(const Groups& G, F per, int* total) {
+    StageRows R;
+    std::memset(&R, 0, sizeof R);
+    int acc = 0;
+    for (int g = 0; g < G.ng; g++) {
+        R.start[g] = acc;
+        R.per[g] = fast_div((uint32_t)per(g));
+        acc += (G.first[g + 1] - G.first[g]) * per(g);
+    }
+    R.start[G.ng] = acc;
+    *total = acc;
+    return R;
+}
+
+// The hybrid multiply + relinearise of a mixed batch (items ordered by level as
+// G describes) as one launch sequence: the stages of mul_relin_chunk, each over
+// all items, every row with its own level's constants.
+static void mul_relin_mixed(Context& top, const uint64_t* rlk, const PtrBatch& pb, const Groups& G, int count,
+                            const MulScratch& m, cudaStream_t st) {
+    const DevConsts& dc = top.dc;  // ring degree and launch shapes; rows take their level's tables
+    int n = 0;
+    // K1: INTT over Q of [a1, b1, a2, b2]
+    const StageRows r1 = stage_rows(G, [&](int g) { return 4 * G.nq[g]; }, &n);
+    ntt_inv(dc, MixedPairQRows{pb, G, r1}, MixedRows{m.sa, (size_t)4 * G.top_nq, G, r1, 0}, n, st);
+    // K2: Q -> R
+#define L_BM(M) bconv_mixed_launch_m<M>(G, count, m, st)
+    DISPATCH_MAXQ(G.top_nq + 1, L_BM);
+#undef L_BM
+    // K3: NTT over R in place, fully reduced
+    const StageRows r3 = stage_rows(G, [&](int g) { return 4 * G.nr[g]; }, &n);
+    const MixedRows rrows{m.sb, (size_t)4 * G.top_nr, G, r3, 1};
+    ntt_fwd<MixedRows, MixedRows, true>(dc, rrows, rrows, n, st);
+    // K4: tensor fused into INTT over Q|R
+    const StageRows r4 = stage_rows(G, [&](int g) { return 3 * G.nqr[g]; }, &n);
+    ntt_inv(dc, MixedTensorSrc{pb, m.sb, G, r4}, MixedRows{m.sc, (size_t)3 * G.top_nqr, G, r4, 3}, n, st);
+    // K5: scale-and-round, R -> Q, digit lift
+#define L_KM(M) k5_mixed_launch_m<M>(G, count, m, st)
+    DISPATCH_MAXQ(G.top_nq + 1, L_KM);
+#undef L_KM
+    // K6a: NTT over Q|P of the digits in place, fully reduced
+    const StageRows r6 = stage_rows(G, [&](int g) { return G.dnum[g] * G.npq[g]; }, &n);
+    const MixedRows drows{m.sd2, (size_t)G.top_dnum * G.top_npq, G, r6, 2};
+    ntt_fwd<MixedRows, MixedRows, true>(dc, drows, drows, n, st);
+    // K6b: key product over P fused into INTT over P
+    const StageRows r6b = stage_rows(G, [&](int) { return 2 * G.np; }, &n);
+    ntt_inv(dc, MixedKeyIPSrc{m.sd2, rlk, G, r6b}, MixedSeRowsP{m.se, G, r6b}, n, st);
+    // K7: mod down + add fused into NTT over Q, the key product over Q added at its store
+    const StageRows r7 = stage_rows(G, [&](int g) { return 2 * G.nq[g]; }, &n);
+    const MixedOutCtKeyDst dst{pb, m.sd2, rlk, G, r7};
+    if (G.np == 1)
+        ntt_fwd(dc, MixedModDownSrc<true>{m.se, m.sd, G, r7}, dst, n, st);
+    else
+        ntt_fwd(dc, MixedModDownSrc<false>{m.se, m.sd, G, r7}, dst, n, st);
+}
 
 extern "C" {
 
@@ -149,49 +259,67 @@ int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32
     return guarded([&] {
         Context& c = CX(ctx);
         KB_REQUIRE(!c.parent, KBFV_ERR_INVALID, "call on the top-level context");
+        require_batchable(c);
+        KB_REQUIRE(d_rlk, KBFV_ERR_NO_KEY, "relinearisation key missing");
         KB_REQUIRE(live_q && ct_a && ct_b && out, KBFV_ERR_INVALID, "null pointer array");
-        std::map<uint32_t, std::vector<uint32_t>> groups;
         for (uint32_t i = 0; i < count; i++) {
             KB_REQUIRE(live_q[i] >= 1 && live_q[i] <= (uint32_t)c.nq, KBFV_ERR_LEVEL, "live prime count out of range");
-            groups[live_q[i]].push_back(i);
+            KB_REQUIRE(ct_a[i] && ct_b[i] && out[i], KBFV_ERR_INVALID, "null ciphertext pointer");
         }
-        // the level groups run concurrently: the first on the caller's stream, the
-        // next ones on the context's lane streams (forked from and joined back into
-        // the caller's stream); each level context has its own scratch arena
+        // pairs ordered by level, highest first (stable); each product still goes
+        // to its own output pointer
+        std::vector<uint32_t> order(count);
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return live_q[x] > live_q[y]; });
         cudaStream_t st = S(stream);
-        const int ng = (int)groups.size();
-        const int lanes = std::min(ng, 4);
-        if (lanes > 1) {
-            if (!c.lane_fork) {
-                for (int k = 0; k < 3; k++) {
-                    KB_CHECK_CUDA(cudaStreamCreateWithFlags(&c.lane[k], cudaStreamNonBlocking));
-                    KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.lane_join[k], cudaEventDisableTiming));
+        for (uint32_t off = 0; off < count;) {
+            // one chunk: up to kMaxBatch pairs in up to kMaxGroups levels
+            uint32_t end = off;
+            int levels_seen = 0;
+            while (end < count && end - off < (uint32_t)kMaxBatch) {
+                if (end == off || live_q[order[end]] != live_q[order[end - 1]]) {
+                    if (levels_seen == kMaxGroups) break;
+                    levels_seen++;
                 }
-                KB_CHECK_CUDA(cudaEventCreateWithFlags(&c.lane_fork, cudaEventDisableTiming));
+                end++;
             }
-            KB_CHECK_CUDA(cudaEventRecord(c.lane_fork, st));
-            for (int k = 1; k < lanes; k++) KB_CHECK_CUDA(cudaStreamWaitEvent(c.lane[k - 1], c.lane_fork, 0));
-        }
-        int g = 0;
-        for (auto it = groups.rbegin(); it != groups.rend(); ++it, ++g) {  // highest level first
-            kbfv_context* lv = nullptr;
-            int rc = kbfv_context_at_level(ctx, it->first, &lv);
-            if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
-            std::vector<const uint64_t*> A, B;
-            std::vector<uint64_t*> O;
-            for (uint32_t i : it->second) {
-                A.push_back(ct_a[i]);
-                B.push_back(ct_b[i]);
-                O.push_back(out[i]);
+            const int cnt = (int)(end - off);
+            // sub-batches on the caller's stream and auxiliary streams (as in
+            // kbfv_mul_relin_batch); pairs dealt round-robin, so each sub-batch
+            // keeps the level order and a similar mix of levels
+            const int nb = branch_count(c, cnt);
+            const int per = (cnt + nb - 1) / nb;
+            const size_t region = branch_region_bytes(c, per);
+            uint8_t* base = ensure_scratch(c, region * nb);
+            if (nb > 1) {
+                ensure_branch_streams(c);
+                KB_CHECK_CUDA(cudaEventRecord(c.fork_ev, st));
+                for (int k = 1; k < nb; k++) KB_CHECK_CUDA(cudaStreamWaitEvent(c.aux[k - 1], c.fork_ev, 0));
             }
-            const int lane = g % lanes;
-            cudaStream_t ls = lane == 0 ? st : c.lane[lane - 1];
-            rc = kbfv_mul_relin_batch(lv, d_rlk, A.data(), B.data(), O.data(), (uint32_t)A.size(), (kbfv_stream)ls);
-            if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
-        }
-        for (int k = 1; k < lanes; k++) {
-            KB_CHECK_CUDA(cudaEventRecord(c.lane_join[k - 1], c.lane[k - 1]));
-            KB_CHECK_CUDA(cudaStreamWaitEvent(st, c.lane_join[k - 1], 0));
+            for (int k = 0; k < nb; k++) {
+                Groups G = groups_header(c);
+                PtrBatch pb;
+                std::memset(&pb, 0, sizeof pb);
+                int n = 0;
+                for (int j = k; j < cnt; j += nb) {
+                    const uint32_t it = order[off + j];
+                    const int lvl = (int)live_q[it];
+                    if (G.ng == 0 || G.nq[G.ng - 1] != lvl) add_group(ctx, c, G, lvl, n);
+                    pb.a[n] = ct_a[it];
+                    pb.b[n] = ct_b[it];
+                    pb.o[n] = out[it];
+                    n++;
+                }
+                G.first[G.ng] = n;
+                if (n == 0) continue;
+                mul_relin_mixed(c, d_rlk, pb, G, n, mul_scratch_layout(c, n, base + (size_t)k * region),
+                                k == 0 ? st : c.aux[k - 1]);
+            }
+            for (int k = 1; k < nb; k++) {
+                KB_CHECK_CUDA(cudaEventRecord(c.join_ev[k - 1], c.aux[k - 1]));
+                KB_CHECK_CUDA(cudaStreamWaitEvent(st, c.join_ev[k - 1], 0));
+            }
+            off = end;
         }
     });
 }

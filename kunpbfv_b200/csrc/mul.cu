@@ -56,7 +56,7 @@ void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb, int co
     ks_tail(dc, m.sd2, rlk, dc.dnum, m.se, m.sd, pb, count, st);
 }
 
-static void ensure_branch_streams(Context& c) {
+void ensure_branch_streams(Context& c) {
     if (c.fork_ev) return;
     for (int i = 0; i < 3; i++) {
         KB_CHECK_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));

@@ -13,17 +13,44 @@
 // front of (forward) or behind (inverse) 2^12-point block kernels (the launch
 // code picks the split). Moduli must be below 2^60 (lazy range 8q < 2^63).
 //
-// Rows are described by Src/Dst functors: src.prime(row) and
-// src.bind(row) -> {load(j), store(j, v)}. This lets pipeline stages fuse their per-element
+// Rows are described by Src/Dst functors: src.prime(row) (or src.tables(row,
+// inverse), see RowTab) and src.bind(row) -> {load(j), store(j, v)}. This lets pipeline stages fuse their per-element
 // prologue (e.g. a tensor product) and epilogue (e.g. a key product) into the
 // transform's first load and last store, which are always coalesced
 // (consecutive threads touch consecutive j).
 #pragma once
+#include <type_traits>
+#include <utility>
+
 #include "arith.cuh"
 
 namespace kbfv {
 
 typedef ulonglong2 tw_t;  // (w, floor(w * 2^64 / q))
+
+// The twiddle table and modulus of one row. By default they come from the
+// launch's prime table (tw_all + prime(row) * N, mods[prime(row)]); a functor
+// whose rows belong to different parameter sets (the levels of a mixed-level
+// batch) provides `tables(row, inverse)` itself.
+struct RowTab {
+    const tw_t* tw;
+    uint64_t q;
+};
+template <class T, class = void>
+struct has_row_tables : std::false_type {};
+template <class T>
+struct has_row_tables<T, std::void_t<decltype(std::declval<const T&>().tables(0, false))>> : std::true_type {};
+
+template <class Src>
+__device__ __forceinline__ RowTab row_tab(const Src& s, int row, bool inverse, const tw_t* __restrict__ tw_all,
+                                          const uint64_t* __restrict__ mods, int logn) {
+    if constexpr (has_row_tables<Src>::value) {
+        return s.tables(row, inverse);
+    } else {
+        const int p = s.prime(row);
+        return RowTab{tw_all + ((size_t)p << logn), mods[p]};
+    }
+}
 
 __device__ __forceinline__ int spad(int j) { return j + (j >> 4); }
 
@@ -322,10 +349,10 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const int row = blockIdx.x / nblk;
     const int blk = blockIdx.x % nblk;
     const int t = threadIdx.x;
-    const int pidx = src.prime(row);
+    const RowTab rt = row_tab(src, row, false, tw_all, mods, logn);
     const auto s = src.bind(row);
-    const uint64_t q = mods[pidx], q4 = q << 2;
-    PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
+    const uint64_t q = rt.q, q4 = q << 2;
+    PassCtx c{sm, rt.tw, t, logn - LOGB, blk << LOGB, logn, q, q4};
 
     // pass 0 straight from global memory: groups gi + k * 2^lb0 (consecutive lanes, coalesced);
     // groups one after another so fused loaders keep their temporaries in registers
@@ -366,10 +393,10 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const int row = blockIdx.x / nblk;
     const int blk = blockIdx.x % nblk;
     const int t = threadIdx.x;
-    const int pidx = src.prime(row);
+    const RowTab rt = row_tab(src, row, true, tw_all, mods, logn);
     const auto s = src.bind(row);
-    const uint64_t q = mods[pidx], q4 = q << 2;
-    PassCtx c{sm, tw_all + ((size_t)pidx << logn), t, logn - LOGB, blk << LOGB, logn, q, q4};
+    const uint64_t q = rt.q, q4 = q << 2;
+    PassCtx c{sm, rt.tw, t, logn - LOGB, blk << LOGB, logn, q, q4};
 
     if constexpr (inv_direct_load<LOGB, RAD>()) {
         inv_passes_load<LOGB, RAD, R0>(c, s);
@@ -407,11 +434,11 @@ __device__ __forceinline__ void ntt_fwd_col(const Src& src, const Dst& dst, cons
                                             const uint64_t* __restrict__ mods, int logn, size_t gid) {
     const int cols = 1 << (logn - RC);
     const int row = (int)(gid >> (logn - RC)), c = (int)(gid & (cols - 1));
-    const int pidx = src.prime(row);
+    const RowTab rt = row_tab(src, row, false, tw_all, mods, logn);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
-    const uint64_t q = mods[pidx], q4 = q << 2;
-    const tw_t* tw = tw_all + ((size_t)pidx << logn);
+    const uint64_t q = rt.q, q4 = q << 2;
+    const tw_t* tw = rt.tw;
     uint64_t x[1 << RC];
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) x[k] = s.load(c + k * cols);
@@ -425,11 +452,11 @@ __device__ __forceinline__ void ntt_inv_col(const Src& src, const Dst& dst, cons
                                             const uint64_t* __restrict__ mods, int logn, size_t gid) {
     const int cols = 1 << (logn - RC);
     const int row = (int)(gid >> (logn - RC)), c = (int)(gid & (cols - 1));
-    const int pidx = src.prime(row);
+    const RowTab rt = row_tab(src, row, true, tw_all, mods, logn);
     const auto s = src.bind(row);
     const auto d = dst.bind(row);
-    const uint64_t q = mods[pidx], q4 = q << 2;
-    const tw_t* tw = tw_all + ((size_t)pidx << logn);
+    const uint64_t q = rt.q, q4 = q << 2;
+    const tw_t* tw = rt.tw;
     uint64_t x[1 << RC];
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) x[k] = s.load(c + k * cols);

@@ -344,6 +344,8 @@ void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0, int m
 // key-switch tail: key product, mod down and add, written to the outputs of pb
 void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* key, int ndig, uint64_t* se,
              const uint64_t* add, const PtrBatch& pb, int count, cudaStream_t st);
+// the auxiliary streams and fork / join events of the sub-batches (created once)
+void ensure_branch_streams(Context& c);
 // the whole multiply + relinearise of one sub-batch (9 launches)
 void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb, int count, const MulScratch& m,
                      cudaStream_t st);

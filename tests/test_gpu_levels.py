@@ -217,3 +217,29 @@ def test_c4_gadget_at_each_depth():
     hb = host(b.cipher_device).reshape(2, 2, 14, ctx.N)[0]
     want = top.relinearize_gadget(top.mul_tensor(ha, hb), ogk, 20)
     assert np.array_equal(host(out.cipher_device).reshape(2, 2, 14, ctx.N)[0], want)
+
+
+def test_mixed_levels_span_several_launch_sequences():
+    """Pairs at 10 different levels in shuffled order (more levels than one
+    launch sequence groups): every product equals the pair multiplied alone at
+    its level."""
+    import kunpbfv_b200 as kb
+    ctx = kb.BFVContext.from_bits(12, [40] * 10, [50], T, dnum=5)
+    assert ctx.alpha == 2
+    sk = kb.SecretKey(ctx, SEED)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    rng = np.random.default_rng(9)
+    levels = [10, 3, 7, 1, 9, 4, 2, 8, 6, 5, 10, 1, 5, 7]
+    pairs = []
+    for j, live in enumerate(levels):
+        v = rng.integers(0, T, size=(2, ctx.N), dtype=np.uint64)
+        a = sch.mod_switch_to(sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v[0]))), enc_id=900 + 2 * j), live)
+        b = sch.mod_switch_to(sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v[1]))), enc_id=901 + 2 * j), live)
+        pairs.append((a, b))
+    outs = sch.mult_relin_levels(pairs)
+    for j, ((a, b), o) in enumerate(zip(pairs, outs)):
+        assert o.ctx.q_count == levels[j]
+        alone = sch.mult_relin(a, b)
+        assert np.array_equal(host(alone.cipher_device), host(o.cipher_device)), (j, levels[j])
