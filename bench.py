@@ -367,11 +367,12 @@ def run_ours(args, world, rank, local):
     sch.addMultKey_23(sk)
     ctx.reserve(BATCH)
     # the autotuner's choice of the speed-only knobs for this parameter set and
-    # batch (sub-batches of the multiply, host chunk, NTT split); every choice
-    # gives identical results, and the tuner checks that while it times them
+    # batch (sub-batches and launch shapes of the multiply pipeline, host chunk,
+    # NTT split); every choice gives identical results, and the tuner checks
+    # that while it times them
     from kunpbfv_b200 import tune
     tuned = tune.autotune(ctx, sch, pairs=BATCH, cache_path=None)
-    tuned = {k: tuned[k] for k in ("branches", "host_chunk", "ntt_block_log") if k in tuned}
+    tuned = {k: tuned[k] for k in ("ntt_block_log", "host_chunk") + tune.PIPELINE_CHOICES if k in tuned}
     rng = np.random.default_rng(rank)
     v1 = rng.integers(0, T, size=(BATCH, ctx.N), dtype=np.uint64)
     v2 = rng.integers(0, T, size=(BATCH, ctx.N), dtype=np.uint64)

@@ -264,8 +264,17 @@ typedef enum {
                                     rings above 2^v points run as a column pass of log_n - v
                                     stages and blocks of 2^v points */
     KBFV_TUNE_BRANCHES = 1,      /* 1..4 (default 2): sub-batches of a batched multiply */
-    KBFV_TUNE_HOST_CHUNK = 2     /* 0..128 (default 0 = ~32 MiB of inputs): pairs per chunk of
+    KBFV_TUNE_HOST_CHUNK = 2,    /* 0..128 (default 0 = ~32 MiB of inputs): pairs per chunk of
                                     kbfv_mul_relin_host when its chunk_pairs is 0 */
+    KBFV_TUNE_SPLIT_ROWS = 3,    /* 0..2^20 (default 48): at N = 2^14, transforms of at most this
+                                    many rows (inside the multiply pipeline too) run as a radix-4
+                                    column pass and 2^12-point blocks instead of one block per row */
+    KBFV_TUNE_BCONV_THREADS = 4, /* 64, 128, 256 (default) or 512: CTA size of the base conversion
+                                    Q -> R (the multiply's K2 and kbfv_bconv_*) */
+    KBFV_TUNE_K5_THREADS = 5,    /* 64, 128 (default) or 256: CTA size of the multiply's
+                                    scale-and-round / R -> Q / digit-lift kernels (K5) */
+    KBFV_TUNE_K5_FUSED_PAIRS = 6 /* 0..128 (default 2): batches of at most this many pairs run K5
+                                    as one kernel, larger ones as two (fewer registers each) */
 } kbfv_tune_knob;
 int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value);
 int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value);

@@ -139,6 +139,7 @@ void build_context(Context& c, const kbfv_params& prm) {
     }
 
     DevConsts& dc = c.dc;
+    dc.shape = LaunchShape{kSplitRows14Default, 256, 128, 2};
     dc.logn = c.logn; dc.nq = c.nq; dc.np = c.np; dc.nr = c.nr; dc.nt = c.nt;
     dc.dnum = c.dnum; dc.alpha = c.alpha; dc.npq = c.nq + c.np; dc.nqr = c.nq + c.nr;
     dc.idx_p = c.nq; dc.idx_r = c.nq + c.np; dc.idx_t = c.nq + c.np + c.nr; dc.idx_pt = nall - 1;
@@ -635,7 +636,32 @@ int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
                 KB_REQUIRE(value >= 0 && value <= kMaxBatch, KBFV_ERR_INVALID, "host chunk must be 0..128");
                 c.host_chunk = (int)value;
                 break;
+            case KBFV_TUNE_SPLIT_ROWS:
+                KB_REQUIRE(value >= 0 && value <= (1 << 20), KBFV_ERR_INVALID, "split rows must be 0..2^20");
+                c.dc.shape.split_rows14 = (int)value;
+                break;
+            case KBFV_TUNE_BCONV_THREADS:
+                KB_REQUIRE(value == 64 || value == 128 || value == 256 || value == 512, KBFV_ERR_INVALID,
+                           "base-conversion CTA size must be 64, 128, 256 or 512");
+                c.dc.shape.bconv_threads = (int)value;
+                break;
+            case KBFV_TUNE_K5_THREADS:
+                KB_REQUIRE(value == 64 || value == 128 || value == 256, KBFV_ERR_INVALID,
+                           "K5 CTA size must be 64, 128 or 256");
+                c.dc.shape.k5_threads = (int)value;
+                break;
+            case KBFV_TUNE_K5_FUSED_PAIRS:
+                KB_REQUIRE(value >= 0 && value <= kMaxBatch, KBFV_ERR_INVALID, "K5 fused pairs must be 0..128");
+                c.dc.shape.k5_fused_pairs = (int)value;
+                break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
+        }
+        // the levels of a top context run with the top level's knobs
+        for (void* lv : c.levels) {
+            if (!lv) continue;
+            Context& l = reinterpret_cast<kbfv_context*>(lv)->c;
+            l.dc.shape = c.dc.shape;
+            l.branches = c.branches;
         }
     });
 }
@@ -648,6 +674,10 @@ int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value) {
             case KBFV_TUNE_NTT_BLOCK_LOG: *value = c.ntt_block_log; break;
             case KBFV_TUNE_BRANCHES: *value = c.branches; break;
             case KBFV_TUNE_HOST_CHUNK: *value = c.host_chunk; break;
+            case KBFV_TUNE_SPLIT_ROWS: *value = c.dc.shape.split_rows14; break;
+            case KBFV_TUNE_BCONV_THREADS: *value = c.dc.shape.bconv_threads; break;
+            case KBFV_TUNE_K5_THREADS: *value = c.dc.shape.k5_threads; break;
+            case KBFV_TUNE_K5_FUSED_PAIRS: *value = c.dc.shape.k5_fused_pairs; break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
     });

@@ -15,6 +15,15 @@ constexpr int kMaxPrimes = 96;   // whole prime table [Q|P|R|T|t]
 constexpr int kMaxQ = 32;        // ciphertext primes per context
 constexpr int kMaxP = 8;         // special primes
 
+// Launch shapes of the multiply pipeline (speed only; kbfv_tune_set). Set by
+// build_context; kernels never read them.
+struct LaunchShape {
+    int split_rows14;    // N = 2^14 transforms of at most this many rows: column pass + 2^12-point blocks
+    int bconv_threads;   // CTA size of the Q -> R base conversion
+    int k5_threads;      // CTA size of K5
+    int k5_fused_pairs;  // batches of at most this many pairs run K5 as one kernel
+};
+
 // Everything a kernel needs, passed by value (all pointers into one device pool).
 struct DevConsts {
     int logn;
@@ -54,6 +63,7 @@ struct DevConsts {
     // Gaussian table
     const uint64_t* gauss_cdt;
     int gauss_bound;
+    LaunchShape shape;
 };
 
 constexpr int kMaxBlk = 16;  // primes per block of the T-base key switch (p_count or gamma)

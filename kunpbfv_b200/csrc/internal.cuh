@@ -117,11 +117,12 @@ static inline Dst plain_of(const Dst& d) { return d; }
 // column pass and 2^12-point blocks: four times the CTAs cover the SMs, 15-23 us
 // instead of 29-31 us per launch of 8-45 rows on the B200. At 64 rows the
 // split alone is still faster, but beside a concurrent sub-batch it cost the
-// batched multiply ~1%, so 64-row launches keep the whole-ring blocks.
-constexpr int kSplitRows14 = 48;
+// batched multiply ~1%, so 64-row launches keep the whole-ring blocks. The
+// default of LaunchShape::split_rows14 (KBFV_TUNE_SPLIT_ROWS).
+constexpr int kSplitRows14Default = 48;
 
 // Forward NTT of `rows` rows read through `s` and written through `d`.
-// For logn <= 14 one block kernel (N = 2^14 with at most kSplitRows14 rows:
+// For logn <= 14 one block kernel (N = 2^14 with at most shape.split_rows14 rows:
 // as for 15/16 with a radix-4 column pass); for 15/16 a radix-8/16 column pass
 // (s -> plain_of(d)) then 2^12-point block kernels from plain_of(d) to d in
 // place (d must also be readable): several 256-thread CTAs per SM run faster
@@ -136,7 +137,7 @@ static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 12: launch_fwd_block<12, Src, Dst, FULL>(dc, s, d, rows, 12, st); break;
         case 13: launch_fwd_block<13, Src, Dst, FULL>(dc, s, d, rows, 13, st); break;
         case 14: {
-            if (rows > kSplitRows14) {
+            if (rows > dc.shape.split_rows14) {
                 launch_fwd_block<14, Src, Dst, FULL>(dc, s, d, rows, 14, st);
                 break;
             }
@@ -177,7 +178,7 @@ static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 12: launch_inv_block<12, Src, Dst, true>(dc, s, d, rows, 12, st); break;
         case 13: launch_inv_block<13, Src, Dst, true>(dc, s, d, rows, 13, st); break;
         case 14: {
-            if (rows > kSplitRows14) {
+            if (rows > dc.shape.split_rows14) {
                 launch_inv_block<14, Src, Dst, true>(dc, s, d, rows, 14, st);
                 break;
             }

@@ -121,11 +121,11 @@ static __global__ void k5_lift_kernel(DevConsts c, const uint64_t* __restrict__ 
 
 template <int MAXQ>
 void k5_launch_m(const DevConsts& dc, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st) {
-    const int threads = 128;
+    const int threads = dc.shape.k5_threads;
     dim3 grid((unsigned)((1u << dc.logn) / threads), (unsigned)(count * 3));
     // the R limbs of the inputs (m.sb, 4 x nr limbs per pair) are dead after K4:
     // they hold the scale-and-round results (3 x nr limbs per pair)
-    if (count <= 2) {
+    if (count <= dc.shape.k5_fused_pairs) {
         k5_round_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sc, out0, m.sd, m.sd2, mode);
     } else {
         k5_scale_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sc, m.sb);
@@ -196,18 +196,18 @@ static __global__ void k5_lift_mixed_kernel(Groups G, const uint64_t* __restrict
 
 // K2 (Q -> R) of a mixed batch; MAXQ bounds the top level's ciphertext primes + 1
 template <int MAXQ>
-void bconv_mixed_launch_m(const Groups& G, int count, const MulScratch& m, cudaStream_t st) {
-    const int threads = 256;
+void bconv_mixed_launch_m(const Groups& G, const LaunchShape& sh, int count, const MulScratch& m, cudaStream_t st) {
+    const int threads = sh.bconv_threads;
     dim3 grid((unsigned)((1u << G.logn) / threads), (unsigned)(count * 4));
-    const size_t sh = (size_t)G.top_nq * G.top_nr * 8;
-    bconv_mixed_kernel<MAXQ><<<grid, threads, sh, st>>>(G, m.sa, m.sb);
+    const size_t smem = (size_t)G.top_nq * G.top_nr * 8;
+    bconv_mixed_kernel<MAXQ><<<grid, threads, smem, st>>>(G, m.sa, m.sb);
     check_launch("bconv_mixed");
 }
 
 // K5a + K5b of a mixed batch
 template <int MAXQ>
-void k5_mixed_launch_m(const Groups& G, int count, const MulScratch& m, cudaStream_t st) {
-    const int threads = 128;
+void k5_mixed_launch_m(const Groups& G, const LaunchShape& sh, int count, const MulScratch& m, cudaStream_t st) {
+    const int threads = sh.k5_threads;
     dim3 grid((unsigned)((1u << G.logn) / threads), (unsigned)(count * 3));
     k5_scale_mixed_kernel<MAXQ><<<grid, threads, 0, st>>>(G, m.sc, m.sb);
     k5_lift_mixed_kernel<MAXQ><<<grid, threads, 0, st>>>(G, m.sb, m.sd, m.sd2);

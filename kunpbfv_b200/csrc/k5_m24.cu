@@ -2,5 +2,5 @@
 #include "k5_kernels.cuh"
 
 template void k5_launch_m<24>(const DevConsts&, int, const MulScratch&, uint64_t*, int, cudaStream_t);
-template void bconv_mixed_launch_m<24>(const Groups&, int, const MulScratch&, cudaStream_t);
-template void k5_mixed_launch_m<24>(const Groups&, int, const MulScratch&, cudaStream_t);
+template void bconv_mixed_launch_m<24>(const Groups&, const LaunchShape&, int, const MulScratch&, cudaStream_t);
+template void k5_mixed_launch_m<24>(const Groups&, const LaunchShape&, int, const MulScratch&, cudaStream_t);

@@ -151,7 +151,7 @@ static void mul_relin_mixed(Context& top, const uint64_t* rlk, const PtrBatch& p
     const StageRows r1 = stage_rows(G, [&](int g) { return 4 * G.nq[g]; }, &n);
     ntt_inv(dc, MixedPairQRows{pb, G, r1}, MixedRows{m.sa, (size_t)4 * G.top_nq, G, r1, 0}, n, st);
     // K2: Q -> R
-#define L_BM(M) bconv_mixed_launch_m<M>(G, count, m, st)
+#define L_BM(M) bconv_mixed_launch_m<M>(G, dc.shape, count, m, st)
     DISPATCH_MAXQ(G.top_nq + 1, L_BM);
 #undef L_BM
     // K3: NTT over R in place, fully reduced
@@ -162,7 +162,7 @@ static void mul_relin_mixed(Context& top, const uint64_t* rlk, const PtrBatch& p
     const StageRows r4 = stage_rows(G, [&](int g) { return 3 * G.nqr[g]; }, &n);
     ntt_inv(dc, MixedTensorSrc{pb, m.sb, G, r4}, MixedRows{m.sc, (size_t)3 * G.top_nqr, G, r4, 3}, n, st);
     // K5: scale-and-round, R -> Q, digit lift
-#define L_KM(M) k5_mixed_launch_m<M>(G, count, m, st)
+#define L_KM(M) k5_mixed_launch_m<M>(G, dc.shape, count, m, st)
     DISPATCH_MAXQ(G.top_nq + 1, L_KM);
 #undef L_KM
     // K6a: NTT over Q|P of the digits in place, fully reduced
@@ -215,6 +215,8 @@ int kbfv_context_at_level(kbfv_context* ctx, uint32_t live_q, kbfv_context** out
                 throw;
             }
             h->c.parent = &c;
+            h->c.dc.shape = c.dc.shape;
+            h->c.branches = c.branches;
             h->c.dc.key_nq = c.nq;
             h->c.dc.key_npq = c.nq + c.np;
             std::memcpy(h->c.seed, c.seed, 32);

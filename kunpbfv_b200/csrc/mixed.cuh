@@ -312,9 +312,9 @@ static inline MixedOutCtDst plain_of(const MixedOutCtKeyDst& d) { return MixedOu
 
 // K2 and K5 of a mixed batch (instantiated per MAXQ bucket in k5_m<MAXQ>.cu)
 template <int MAXQ>
-void bconv_mixed_launch_m(const Groups& G, int count, const MulScratch& m, cudaStream_t st);
+void bconv_mixed_launch_m(const Groups& G, const LaunchShape& sh, int count, const MulScratch& m, cudaStream_t st);
 template <int MAXQ>
-void k5_mixed_launch_m(const Groups& G, int count, const MulScratch& m, cudaStream_t st);
+void k5_mixed_launch_m(const Groups& G, const LaunchShape& sh, int count, const MulScratch& m, cudaStream_t st);
 
 // The level constants of item `item` copied into shared memory by the CTA (one
 // item per CTA row of the per-coefficient kernels), so that the kernels' reads

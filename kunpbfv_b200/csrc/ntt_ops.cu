@@ -45,7 +45,7 @@ static void ntt_rows(const Context& c, RowsIO io, int rows, bool fwd, cudaStream
 void launch_bconv(const DevConsts& dc, const BconvTables& tb, const uint64_t* in, uint64_t* out, int polys,
                          size_t in_stride, size_t out_stride, cudaStream_t st) {
     if (polys <= 0) return;
-    const int threads = 256;
+    const int threads = dc.shape.bconv_threads;
     dim3 grid((unsigned)((1u << dc.logn) / threads), (unsigned)polys);
     const size_t sh = (size_t)tb.nin * tb.nout * 8;
 #define L_BC(M) bconv_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride)

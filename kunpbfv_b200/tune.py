@@ -6,7 +6,13 @@ Knobs (include/kbfv.h, ``kbfv_tune_knob``):
   2^v points: a column pass of ``log_n - v`` stages and block kernels of 2^v
   points, v in 12..14, or 0 for the built-in shapes;
 * ``branches`` - sub-batches (one stream each) of a batched multiply, 1..4;
-* ``host_chunk`` - pairs per chunk of the host-memory multiply, 0..128.
+* ``host_chunk`` - pairs per chunk of the host-memory multiply, 0..128;
+* the launch shapes inside the multiply pipeline: ``split_rows`` (at N=2^14,
+  transforms of at most this many rows run as a radix-4 column pass and
+  2^12-point blocks instead of one 1024-thread block per row), ``bconv_threads``
+  (CTA size of the Q -> R base conversion), ``k5_threads`` (CTA size of the
+  scale-and-round / R -> Q / digit-lift kernels) and ``k5_fused_pairs``
+  (batches of at most this many pairs run those as one kernel).
 
 Each candidate is timed on the device with CUDA events (two warm-up calls,
 then the median of three timed trials of ``reps`` calls). Knobs never change
@@ -29,6 +35,16 @@ DEFAULT_CACHE = os.environ.get("KBFV_TUNE_CACHE",
 NTT_BLOCK_LOGS = (0, 12, 13, 14)  # 0: built-in shapes
 BRANCHES = (1, 2, 3, 4)
 HOST_CHUNKS = (4, 8, 12, 16, 24)
+# the multiply pipeline's launch shapes, tuned one after another on the batch
+# (coordinate descent from the defaults, first candidate of each list)
+PIPELINE_KNOBS = {
+    "branches": (2, 1, 3, 4),
+    "bconv_threads": (256, 128, 512, 64),
+    "k5_threads": (128, 64, 256),
+    "split_rows": (48, 0, 256, 1 << 20),
+}
+# tuned on a two-pair multiply (the per-call size it governs)
+K5_FUSED_PAIRS = (2, 0, 4)
 
 
 def cache_key(device: str, log_n: int, q_count: int, p_count: int, dnum: int, pairs: int) -> str:
@@ -129,33 +145,6 @@ def _random_pairs(ctx, pairs: int, seed: int):
     return _random_rows(ctx, rows, 0, ctx.q_count, seed).view(pairs, 2, ctx.q_count, ctx.N)
 
 
-def tune_branches(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
-    """Sub-batches of the batched multiply (hybrid key switch)."""
-    import torch
-
-    from .api import Ciphertext
-    ctx = scheme.context
-    keep = ctx.tune_get("branches")
-    c1 = Ciphertext(ctx, _random_pairs(ctx, pairs, 2))
-    c2 = Ciphertext(ctx, _random_pairs(ctx, pairs, 3))
-    out = Ciphertext(ctx, count=pairs)
-    ms, want = {}, None
-    try:
-        for b in BRANCHES:
-            ctx.tune_set("branches", b)
-            scheme.mult_relin(c1, c2, out=out)
-            torch.cuda.synchronize()
-            if want is None:
-                want = out.cipher_device.clone()
-            elif not torch.equal(out.cipher_device, want):
-                raise RuntimeError(f"{b} sub-batches changed the product")
-            ms[b] = round(time_ms(lambda: scheme.mult_relin(c1, c2, out=out), reps), 4)
-    finally:
-        ctx.tune_set("branches", keep)
-    best = min(ms, key=ms.get)
-    return {"branches": best, "ms": {str(k): v for k, v in ms.items()}}
-
-
 def tune_host_chunk(scheme, pairs: int = 64, reps: int = 3) -> Dict[str, object]:
     """Pairs per chunk of the host-memory multiply (page-locked buffers)."""
     import torch
@@ -180,8 +169,66 @@ def tune_host_chunk(scheme, pairs: int = 64, reps: int = 3) -> Dict[str, object]
     return {"host_chunk": best, "ms": {str(k): v for k, v in ms.items()}}
 
 
+def _sweep(ctx, knob, values, run, out, want, reps):
+    """Time `run` for every value of `knob` (others as set); every output must
+    equal `want`. Leaves the fastest value applied; returns {value: ms}."""
+    import torch
+    ms = {}
+    for v in values:
+        ctx.tune_set(knob, v)
+        run()
+        torch.cuda.synchronize()
+        if not torch.equal(out.cipher_device, want):
+            raise RuntimeError(f"{knob}={v} changed the product")
+        ms[v] = round(time_ms(run, reps), 4)
+    ctx.tune_set(knob, min(ms, key=ms.get))
+    return ms
+
+
+def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
+    """The multiply pipeline's knobs (PIPELINE_KNOBS on a batch of `pairs`,
+    K5_FUSED_PAIRS on two pairs), one at a time from the defaults; every
+    candidate's product is compared with the default shapes' product."""
+    import torch
+
+    from .api import Ciphertext
+    ctx = scheme.context
+    keep = {k: ctx.tune_get(k) for k in list(PIPELINE_KNOBS) + ["k5_fused_pairs"]}
+    c1 = Ciphertext(ctx, _random_pairs(ctx, pairs, 2))
+    c2 = Ciphertext(ctx, _random_pairs(ctx, pairs, 3))
+    out = Ciphertext(ctx, count=pairs)
+    two = min(2, pairs)
+    d1 = Ciphertext(ctx, c1.cipher_device[:two].clone())
+    d2 = Ciphertext(ctx, c2.cipher_device[:two].clone())
+    out2 = Ciphertext(ctx, count=two)
+    result: Dict[str, object] = {}
+    try:
+        for k, vals in PIPELINE_KNOBS.items():  # defaults first: the reference products
+            ctx.tune_set(k, vals[0])
+        ctx.tune_set("k5_fused_pairs", K5_FUSED_PAIRS[0])
+        scheme.mult_relin(c1, c2, out=out)
+        scheme.mult_relin(d1, d2, out=out2)
+        torch.cuda.synchronize()
+        want, want2 = out.cipher_device.clone(), out2.cipher_device.clone()
+        for k, vals in PIPELINE_KNOBS.items():
+            ms = _sweep(ctx, k, vals, lambda: scheme.mult_relin(c1, c2, out=out), out, want, reps)
+            result[k], result[k + "_ms"] = min(ms, key=ms.get), {str(v): t for v, t in ms.items()}
+        ms = _sweep(ctx, "k5_fused_pairs", K5_FUSED_PAIRS, lambda: scheme.mult_relin(d1, d2, out=out2), out2,
+                    want2, reps)
+        result["k5_fused_pairs"], result["k5_fused_pairs_ms"] = min(ms, key=ms.get), {
+            str(v): t for v, t in ms.items()}
+    except Exception:
+        for k, v in keep.items():
+            ctx.tune_set(k, v)
+        raise
+    return result
+
+
+PIPELINE_CHOICES = ("branches", "bconv_threads", "k5_threads", "split_rows", "k5_fused_pairs")
+
+
 def apply_choice(ctx, choice: dict) -> None:
-    for knob in ("ntt_block_log", "branches", "host_chunk"):
+    for knob in ("ntt_block_log", "host_chunk") + PIPELINE_CHOICES:
         if knob in choice:
             ctx.tune_set(knob, int(choice[knob]))
 
@@ -202,8 +249,7 @@ def autotune(ctx, scheme=None, pairs: int = 64, cache_path: Optional[str] = DEFA
     r = tune_ntt(ctx, ntt_rows)
     choice["ntt_block_log"], choice["ntt_ms"] = r["ntt_block_log"], r["ms"]
     if scheme is not None and scheme.rlk is not None and scheme.relin == "hybrid":
-        r = tune_branches(scheme, pairs)
-        choice["branches"], choice["branches_ms"] = r["branches"], r["ms"]
+        choice.update(tune_pipeline(scheme, pairs))
         if host:
             r = tune_host_chunk(scheme, pairs)
             choice["host_chunk"], choice["host_chunk_ms"] = r["host_chunk"], r["ms"]

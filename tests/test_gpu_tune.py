@@ -54,6 +54,8 @@ def test_autotune_applies_and_caches(tmp_path):
     assert ctx.tune_get("branches") == got["branches"]
     assert ctx.tune_get("host_chunk") == got["host_chunk"]
     assert set(got["branches_ms"]) == {str(b) for b in tune.BRANCHES}
+    for k in ("bconv_threads", "k5_threads", "split_rows", "k5_fused_pairs"):
+        assert ctx.tune_get(k) == got[k], k
     # a fresh context of the same parameters takes the cached choice without timing
     ctx2 = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
     hit = tune.autotune(ctx2, None, pairs=32, cache_path=cache)
@@ -94,3 +96,54 @@ def test_host_chunk_knob_drives_the_default_chunk():
             assert torch.equal(out.view(-1), want.view(-1)), knob
     finally:
         ctx.tune_set("host_chunk", 0)
+
+
+@pytest.mark.parametrize("knob,values", [("bconv_threads", (64, 128, 256, 512)), ("k5_threads", (64, 128, 256)),
+                                         ("split_rows", (0, 48, 1 << 20)), ("k5_fused_pairs", (0, 2, 4))])
+def test_pipeline_shapes_keep_the_product(knob, values):
+    """Every launch shape of the multiply pipeline gives the oracle's product
+    (N=16384, 7 + 1 primes; 3 pairs: K5 fused or split by k5_fused_pairs,
+    112-row transforms split or not by split_rows)."""
+    import kunpbfv_b200 as kb
+    import oracle
+    from tests.gpu_util import c3_pair
+    ctx, orc = c3_pair()
+    seed = b"\x44" * 32
+    sk = kb.SecretKey(ctx, seed)
+    sch = kb.BFVScheme(ctx, seed)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    rng = np.random.default_rng(12)
+    v1 = rng.integers(0, 65537, size=(3, ctx.N), dtype=np.uint64)
+    v2 = rng.integers(0, 65537, size=(3, ctx.N), dtype=np.uint64)
+    c1 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v1))), enc_id=5)
+    c2 = sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v2))), enc_id=9)
+    osk = orc.keygen_secret(seed)
+    orlk = orc.keygen_relin(seed, osk)
+    h1 = host(c1.cipher_device).reshape(3, 2, 7, ctx.N)
+    h2 = host(c2.cipher_device).reshape(3, 2, 7, ctx.N)
+    want = np.stack([orc.mul_relin(h1[i], h2[i], orlk) for i in range(3)])
+    keep = ctx.tune_get(knob)
+    try:
+        for v in values:
+            ctx.tune_set(knob, v)
+            assert ctx.tune_get(knob) == v
+            got = host(sch.mult_relin(c1, c2).cipher_device).reshape(want.shape)
+            assert np.array_equal(got, want), (knob, v)
+    finally:
+        ctx.tune_set(knob, keep)
+
+
+def test_pipeline_knob_bounds_and_levels():
+    import kunpbfv_b200 as kb
+    ctx = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
+    for knob, bad in (("bconv_threads", 100), ("bconv_threads", 1024), ("k5_threads", 512), ("k5_threads", 32),
+                      ("split_rows", -1), ("k5_fused_pairs", 129)):
+        with pytest.raises(kb.KbfvError):
+            ctx.tune_set(knob, bad)
+    assert (ctx.tune_get("split_rows"), ctx.tune_get("bconv_threads"), ctx.tune_get("k5_threads"),
+            ctx.tune_get("k5_fused_pairs")) == (48, 256, 128, 2)
+    lv = ctx.at_level(2)
+    ctx.tune_set("k5_threads", 64)
+    assert lv.tune_get("k5_threads") == 64  # levels follow the top level's knobs
+    assert ctx.at_level(1).tune_get("k5_threads") == 64  # and so do levels made later
