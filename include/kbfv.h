@@ -273,8 +273,11 @@ typedef enum {
                                     Q -> R (the multiply's K2 and kbfv_bconv_*) */
     KBFV_TUNE_K5_THREADS = 5,    /* 64, 128 (default) or 256: CTA size of the multiply's
                                     scale-and-round / R -> Q / digit-lift kernels (K5) */
-    KBFV_TUNE_K5_FUSED_PAIRS = 6 /* 0..128 (default 2): batches of at most this many pairs run K5
+    KBFV_TUNE_K5_FUSED_PAIRS = 6, /* 0..128 (default 2): batches of at most this many pairs run K5
                                     as one kernel, larger ones as two (fewer registers each) */
+    KBFV_TUNE_BCONV_CPT = 7      /* 1 or 2 (default): coefficients per thread of the Q -> R base
+                                    conversion (2: 16-byte loads and stores, table reads shared by
+                                    two independent multiply-accumulate chains) */
 } kbfv_tune_knob;
 int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value);
 int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value);

@@ -38,7 +38,7 @@ _ERR_NAMES = {
 
 # kbfv_tune_knob (include/kbfv.h)
 TUNE_KNOBS = {"ntt_block_log": 0, "branches": 1, "host_chunk": 2, "split_rows": 3, "bconv_threads": 4,
-              "k5_threads": 5, "k5_fused_pairs": 6}
+              "k5_threads": 5, "k5_fused_pairs": 6, "bconv_cpt": 7}
 
 
 class KbfvError(RuntimeError):

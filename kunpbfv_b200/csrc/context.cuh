@@ -20,6 +20,7 @@ constexpr int kMaxP = 8;         // special primes
 struct LaunchShape {
     int split_rows14;    // N = 2^14 transforms of at most this many rows: column pass + 2^12-point blocks
     int bconv_threads;   // CTA size of the Q -> R base conversion
+    int bconv_cpt;       // coefficients per thread of the base conversion (1 or 2)
     int k5_threads;      // CTA size of K5
     int k5_fused_pairs;  // batches of at most this many pairs run K5 as one kernel
 };

@@ -84,6 +84,49 @@ static __global__ void bconv_kernel(BconvTables tb, const uint64_t* __restrict__
     }
 }
 
+// Two coefficients per thread (k and k + 1: 16-byte loads and stores): the
+// table reads of each output prime (the hat row in shared memory, modulus,
+// Barrett constants) serve both, and the two multiply-accumulate chains are
+// independent. Per coefficient the arithmetic is bconv_kernel's.
+template <int MAXIN>
+static __global__ void bconv2_kernel(BconvTables tb, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                     int logn, size_t in_stride, size_t out_stride) {
+    extern __shared__ uint64_t sh_hat[];
+    for (int i = threadIdx.x; i < tb.nin * tb.nout; i += blockDim.x) sh_hat[i] = tb.hat[i];
+    __syncthreads();
+    const size_t k = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);
+    const uint64_t* src = in + blockIdx.y * in_stride;
+    uint64_t* dst = out + blockIdx.y * out_stride;
+    uint64_t y0[MAXIN], y1[MAXIN];
+#pragma unroll
+    for (int i = 0; i < MAXIN; i++) {
+        if (i < tb.nin) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(src + ((size_t)i << logn) + k);
+            y0[i] = v.x;
+            y1[i] = v.y;
+        }
+    }
+    const long long v0 = bconv_prep<MAXIN>(y0, y0, tb.nin, tb.in_mods, tb.hatinv, tb.hatinvs, tb.binv);
+    const long long v1 = bconv_prep<MAXIN>(y1, y1, tb.nin, tb.in_mods, tb.hatinv, tb.hatinvs, tb.binv);
+    for (int j = 0; j < tb.nout; j++) {
+        const uint64_t* hr = sh_hat + j * tb.nin;
+        const uint64_t o = tb.out_mods[j], mh = tb.out_mu_hi[j], ml = tb.out_mu_lo[j];
+        u128 a0{0, 0}, a1{0, 0};
+#pragma unroll
+        for (int i = 0; i < MAXIN; i++) {
+            if (i < tb.nin) {
+                const uint64_t h = hr[i];
+                mac(a0, y0[i], h);
+                mac(a1, y1[i], h);
+            }
+        }
+        ulonglong2 r;
+        r.x = sub_mod(barrett128(a0, o, mh, ml), tb.alpha[v0 * tb.nout + j], o);
+        r.y = sub_mod(barrett128(a1, o, mh, ml), tb.alpha[v1 * tb.nout + j], o);
+        *reinterpret_cast<ulonglong2*>(dst + ((size_t)j << logn) + k) = r;
+    }
+}
+
 // ===========================================================================
 // t/Q scale-and-round Q|R -> R (scaleAndRound_HPS_QR_R_kernel,
 // include/poly_arithmetic.cuh:1263-1307). x: nq values then nr values.

@@ -45,10 +45,14 @@ static void ntt_rows(const Context& c, RowsIO io, int rows, bool fwd, cudaStream
 void launch_bconv(const DevConsts& dc, const BconvTables& tb, const uint64_t* in, uint64_t* out, int polys,
                          size_t in_stride, size_t out_stride, cudaStream_t st) {
     if (polys <= 0) return;
-    const int threads = dc.shape.bconv_threads;
-    dim3 grid((unsigned)((1u << dc.logn) / threads), (unsigned)polys);
+    const int threads = dc.shape.bconv_threads, cpt = dc.shape.bconv_cpt;
+    dim3 grid((unsigned)((1u << dc.logn) / (threads * cpt)), (unsigned)polys);
     const size_t sh = (size_t)tb.nin * tb.nout * 8;
-#define L_BC(M) bconv_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride)
+#define L_BC(M)                                                                                        \
+    do {                                                                                               \
+        if (cpt == 2) bconv2_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride); \
+        else bconv_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride);  \
+    } while (0)
     DISPATCH_MAXQ(tb.nin, L_BC);
 #undef L_BC
     check_launch("bconv");

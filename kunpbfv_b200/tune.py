@@ -12,7 +12,8 @@ Knobs (include/kbfv.h, ``kbfv_tune_knob``):
   2^12-point blocks instead of one 1024-thread block per row), ``bconv_threads``
   (CTA size of the Q -> R base conversion), ``k5_threads`` (CTA size of the
   scale-and-round / R -> Q / digit-lift kernels) and ``k5_fused_pairs``
-  (batches of at most this many pairs run those as one kernel).
+  (batches of at most this many pairs run those as one kernel), ``bconv_cpt``
+  (coefficients per thread of the base conversion).
 
 Each candidate is timed on the device with CUDA events (two warm-up calls,
 then the median of three timed trials of ``reps`` calls). Knobs never change
@@ -40,6 +41,7 @@ HOST_CHUNKS = (4, 8, 12, 16, 24)
 PIPELINE_KNOBS = {
     "branches": (2, 1, 3, 4),
     "bconv_threads": (256, 128, 512, 64),
+    "bconv_cpt": (2, 1),
     "k5_threads": (128, 64, 256),
     "split_rows": (48, 0, 256, 1 << 20),
 }
@@ -224,7 +226,7 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
     return result
 
 
-PIPELINE_CHOICES = ("branches", "bconv_threads", "k5_threads", "split_rows", "k5_fused_pairs")
+PIPELINE_CHOICES = ("branches", "bconv_threads", "bconv_cpt", "k5_threads", "split_rows", "k5_fused_pairs")
 
 
 def apply_choice(ctx, choice: dict) -> None:

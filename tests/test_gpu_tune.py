@@ -99,7 +99,8 @@ def test_host_chunk_knob_drives_the_default_chunk():
 
 
 @pytest.mark.parametrize("knob,values", [("bconv_threads", (64, 128, 256, 512)), ("k5_threads", (64, 128, 256)),
-                                         ("split_rows", (0, 48, 1 << 20)), ("k5_fused_pairs", (0, 2, 4))])
+                                         ("split_rows", (0, 48, 1 << 20)), ("k5_fused_pairs", (0, 2, 4)),
+                                         ("bconv_cpt", (1, 2))])
 def test_pipeline_shapes_keep_the_product(knob, values):
     """Every launch shape of the multiply pipeline gives the oracle's product
     (N=16384, 7 + 1 primes; 3 pairs: K5 fused or split by k5_fused_pairs,
@@ -142,7 +143,7 @@ def test_pipeline_knob_bounds_and_levels():
         with pytest.raises(kb.KbfvError):
             ctx.tune_set(knob, bad)
     assert (ctx.tune_get("split_rows"), ctx.tune_get("bconv_threads"), ctx.tune_get("k5_threads"),
-            ctx.tune_get("k5_fused_pairs")) == (48, 256, 128, 2)
+            ctx.tune_get("k5_fused_pairs"), ctx.tune_get("bconv_cpt")) == (48, 256, 128, 2, 2)
     lv = ctx.at_level(2)
     ctx.tune_set("k5_threads", 64)
     assert lv.tune_get("k5_threads") == 64  # levels follow the top level's knobs
