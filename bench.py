@@ -52,6 +52,7 @@ def parse():
                     help="run one kernel on a profiling-sized case and exit (for ncu)")
     ap.add_argument("--rows", type=int, default=1024, help="rows for the ntt16k profiling cases")
     ap.add_argument("--pairs", type=int, default=16, help="pairs for the pipeline1 profiling case")
+    ap.add_argument("--set", default="", help="tuning knobs for the profiling cases, e.g. bconv_cpt=1,k5_threads=256")
     ap.add_argument("--serve-rates", default="500,1000,2000,3000,4000,6000,8000",
                     help="Poisson arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-seconds", type=float, default=2.5,
@@ -74,6 +75,9 @@ def run_kernel_case(args):
         print(json.dumps({name: round(probe_arith(k), 1) for k, name in enumerate(PROBE_KINDS)}))
         return
     ctx = c3_context(kb)
+    for kv in filter(None, args.set.split(",")):
+        knob, value = kv.split("=")
+        ctx.tune_set(knob.strip(), int(value))
     if args.kernel.startswith("ntt16k"):
         rows = args.rows
         x = torch.randint(0, 1 << 59, (rows, ctx.N), dtype=torch.int64, device="cuda")
