@@ -468,6 +468,26 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def per_op_native():
+    """The per-call forms timed from native code over the C ABI
+    (kunpbfv_b200/perop_bench: no interpreter between calls): the fused one-pair
+    call, the plain one-kernel-per-building-block form and the batched call, 64
+    pairs, same parameters as the headline."""
+    from kunpbfv_b200 import build as kb_build
+    exe = kb_build.PEROP_BIN
+    if not os.path.exists(exe):
+        return {"error": "perop_bench not built"}
+    r = subprocess.run([exe, str(BATCH), "3"], capture_output=True, text=True, timeout=300)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": (r.stderr or r.stdout)[-300:]}
+    d = json.loads(lines[-1])
+    d["form"] = ("C++ loop over the C ABI: fused = kbfv_mul_relin with count 1 per pair; plain = one kernel per "
+                 "building block (about 25 launches and 10 device copies per pair) then kbfv_relinearize; "
+                 "batched = one kbfv_mul_relin of all pairs (no CUDA graph)")
+    return d
+
+
 def c4_uneven(stream):
     """Config C4: N=32768, 14 x 60-bit q + 2 x 60-bit special primes, digits of
     5 primes (dnum 3); 16 pairs at 14, 13, 12 and 11 live primes (4 each) in one
@@ -591,7 +611,8 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev, ms_step):
 
     ms_op = time_cuda(per_op, stream, 3)
     res["per_op"] = {"value": round(BATCH / (ms_op / 1e3), 2), "unit": "ct/s",
-                     "form": "one pair per call, 9-14 eager launches each (small launches split), no graph"}
+                     "form": "one pair per call through the Python binding (ctypes pointer arrays built per "
+                             "call), 9-14 eager launches each (small launches split), no graph"}
     # the operation-by-operation form: tensor (kbfv_mul) then relinearisation
     # (kbfv_relinearize) as separate calls, one pair each (13 launches per pair)
     t3 = kb.Tensor3(ctx, count=1)
@@ -610,7 +631,8 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev, ms_step):
 
     ms_split = time_cuda(per_op_split, stream, 3)
     res["per_op_split"] = {"value": round(BATCH / (ms_split / 1e3), 2), "unit": "ct/s",
-                           "form": "one pair per call, multiply then relinearise as separate calls, no graph"}
+                           "form": "one pair per call through the Python binding, multiply then relinearise as "
+                                   "separate calls, no graph"}
 
     # the plain one-op-per-launch form: the HPS tensor composed from the
     # building-block entry points (INTT, base conversion, NTT, tensor, INTT,
@@ -659,8 +681,8 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev, ms_step):
         raise RuntimeError("the building-block multiply differs from the fused one")
     ms_plain = time_cuda(per_op_plain, stream, 3)
     res["per_op_plain"] = {"value": round(BATCH / (ms_plain / 1e3), 2), "unit": "ct/s",
-                           "form": "one pair per call, one kernel per building block (about 25 launches and "
-                                   "6 device copies per pair), no graph"}
+                           "form": "one pair per call through the Python binding, one kernel per building block "
+                                   "(about 25 launches and 6 device copies per pair), no graph"}
 
     # this engine at the reference's own parameter sets (logN 14, 15) with the
     # reference's key switch over the T base: one pair per call (the form the
@@ -694,6 +716,7 @@ def extras(args, ctx, sch, c1, c2, out, stream, dev, ms_step):
     res["reference_params"] = dict(refp, form="T-base key switch (bit-exact with the reference's genuine "
                                               "multiply); per-op: one pair per call; batched: 64 pairs per call")
 
+    res["per_op_native"] = per_op_native()
     res["c4_uneven"] = c4_uneven(stream)
 
     # e2e through the C ABI with page-locked host buffers: kbfv_mul_relin_host

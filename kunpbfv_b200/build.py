@@ -11,6 +11,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libkbfv.so")
+# native timing program of the per-call forms (bench.py runs it), linked to LIB
+PEROP_SRC = os.path.join(HERE, "csrc", "perop_bench.cpp")
+PEROP_BIN = os.path.join(HERE, "perop_bench")
 OBJDIR = os.path.join(HERE, "_build")
 # translation units of libkbfv.so (compiled in parallel)
 SOURCES = [os.path.join(HERE, "csrc", f) for f in
@@ -55,8 +58,19 @@ def _stale_obj(src: str) -> bool:
     return any(os.path.getmtime(d) > t for d in [src] + HEADERS if os.path.exists(d))
 
 
+def build_perop(force: bool = False) -> str:
+    """The per-call timing program (host code over the C ABI)."""
+    if force or not os.path.exists(PEROP_BIN) or any(
+            os.path.getmtime(d) > os.path.getmtime(PEROP_BIN) for d in (PEROP_SRC, LIB)):
+        subprocess.run([nvcc(), "-std=c++17", "-O2", PEROP_SRC, "-L", HERE, "-lkbfv", "-Xlinker", "-rpath",
+                        "-Xlinker", "$ORIGIN", "-o", PEROP_BIN + ".tmp"], check=True)
+        os.replace(PEROP_BIN + ".tmp", PEROP_BIN)
+    return PEROP_BIN
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
+        build_perop()
         return LIB
     os.makedirs(OBJDIR, exist_ok=True)
     todo = [s for s in SOURCES if force or _stale_obj(s)]
@@ -76,6 +90,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             *[_obj(s) for s in SOURCES], "-lpthread"]
     subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
+    build_perop(force=True)
     return LIB
 
 
