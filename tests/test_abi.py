@@ -91,7 +91,15 @@ def test_compat_header_compiles_and_links(tmp_path):
     assert out.exists()
 
 
-REF = "/root/reference"
+def _reference_dir():
+    """Where the oracle recipe finds the reference sources (oracle/Makefile's REF)."""
+    import re as _re
+    with open(os.path.join(ROOT, "oracle", "Makefile")) as f:
+        m = _re.search(r"^REF\s*\?=\s*(\S+)", f.read(), _re.M)
+    return os.environ.get("REF") or (m.group(1) if m else "")
+
+
+REF = _reference_dir()
 DRIVERS = ["correct_mult", "correct_add", "correct_encrypt", "perf_mult", "perf_add", "perf_encrypt", "bfv_demo"]
 
 
