@@ -431,9 +431,11 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
  * stays where it was).
  * The array is part of the library's multiply module. The CUDA runtime
  * allocates it when it loads that module in a context: with lazy module
- * loading (the default since CUDA 12.2) at the first multiply of any kind in
- * that context, including the first call of this entry point; with eager
- * loading when the context is created. It is held until the process exits (or
+ * loading (the default since CUDA 12.2) at the first call in that context of
+ * kbfv_mul_relin, kbfv_mul_relin_batch, kbfv_mul_relin_host, kbfv_mul,
+ * kbfv_relinearize or of this entry point (or of the gadget, T-base and
+ * Galois key switches built on them; kbfv_mul_relin_levels runs kernels of
+ * another module); with eager loading when the context is created. It is held until the process exits (or
  * the context is destroyed). A caller with a fixed budget makes one multiply
  * call on each device during start-up, before any stream capture and before
  * taking its budget snapshot. The first call of this entry point in each CUDA
