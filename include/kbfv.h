@@ -91,8 +91,11 @@ const char* kbfv_version(void);
  * 10: 64x64->128 multiply-accumulate from 32-bit partial products with carry
  * chains, 11: forward NTT butterfly from 32-bit partial products (the one the
  * NTT kernels use), 12: 32-bit multiply-add issue rate (16 dependent
- * multiply-adds per chain step: the IMAD pipe's peak). The roofline of the
- * IMAD-bound kernels. */
+ * multiply-adds per chain step: the IMAD pipe's peak), 13: the same for
+ * 32x32->64 multiply-adds, 14: 60x60-bit multiply-accumulate from 30-bit
+ * halves (four 32x32->64 multiply-adds into three column sums), 15: the same
+ * as 12 for 32-bit high multiply-adds. The roofline of the IMAD-bound
+ * kernels. */
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops);
 
 /* ---- context ---------------------------------------------------------
@@ -275,9 +278,19 @@ typedef enum {
                                     scale-and-round / R -> Q / digit-lift kernels (K5) */
     KBFV_TUNE_K5_FUSED_PAIRS = 6, /* 0..128 (default 2): batches of at most this many pairs run K5
                                     as one kernel, larger ones as two (fewer registers each) */
-    KBFV_TUNE_BCONV_CPT = 7      /* 1 or 2 (default): coefficients per thread of the Q -> R base
+    KBFV_TUNE_BCONV_CPT = 7,     /* 1 or 2 (default): coefficients per thread of the Q -> R base
                                     conversion (2: 16-byte loads and stores, table reads shared by
                                     two independent multiply-accumulate chains) */
+    KBFV_TUNE_FUSE_Q2R_PAIRS = 8, /* 0..128 (default 1): multiplies of at most this many pairs (per
+                                    sub-batch) run the Q -> R base extension in the loader of the
+                                    forward NTT over R: the inverse NTT over Q stores its outputs
+                                    scaled by (Q/q_i)^-1, and there is no base-conversion launch
+                                    and no HBM round trip of the R limbs; each R row then reads
+                                    all q_count Q limbs, which larger batches pay for in L2 traffic */
+    KBFV_TUNE_L2_PREFETCH = 9    /* 0 or 1 (default): NTT block kernels whose input is plain rows
+                                    (standalone transforms, the multiply's INTT of its inputs and
+                                    its NTTs over R and Q|P) ask L2 for the block one wave of CTAs
+                                    ahead of their own */
 } kbfv_tune_knob;
 int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value);
 int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value);

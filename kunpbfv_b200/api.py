@@ -38,7 +38,8 @@ _ERR_NAMES = {
 
 # kbfv_tune_knob (include/kbfv.h)
 TUNE_KNOBS = {"ntt_block_log": 0, "branches": 1, "host_chunk": 2, "split_rows": 3, "bconv_threads": 4,
-              "k5_threads": 5, "k5_fused_pairs": 6, "bconv_cpt": 7}
+              "k5_threads": 5, "k5_fused_pairs": 6, "bconv_cpt": 7,
+              "fuse_q2r_pairs": 8, "l2_prefetch": 9}
 
 
 class KbfvError(RuntimeError):
@@ -874,7 +875,8 @@ PROBE_KINDS = ["64x64->128 multiply-accumulate", "mul.lo.u64", "mul.hi.u64",
                "Shoup product", "128-bit Barrett", "one-high-product Barrett", "32x32->64 multiply-add",
                "32x32 high product", "32-bit multiply-add", "64x64->128 multiply-accumulate from 32-bit parts",
                "forward NTT butterfly from 32-bit parts (the kernels')",
-               "32-bit multiply-add issue rate (IMAD pipe)"]
+               "32-bit multiply-add issue rate (IMAD pipe)", "32x32->64 multiply-add issue rate",
+               "60x60-bit multiply-accumulate from 30-bit halves", "32-bit high multiply-add issue rate"]
 
 
 def probe_arith(kind: int, iters: int = 4096) -> float:

@@ -141,7 +141,7 @@ void build_context(Context& c, const kbfv_params& prm) {
     DevConsts& dc = c.dc;
     // two coefficients per base-conversion thread: 16% fewer IMAD instructions,
     // 8% faster than one at N=16384, 7 + 1 primes, 32-pair sub-batches (B200)
-    dc.shape = LaunchShape{kSplitRows14Default, 256, 2, 128, 2};
+    dc.shape = LaunchShape{kSplitRows14Default, 256, 2, 128, 2, 1, 1};
     dc.logn = c.logn; dc.nq = c.nq; dc.np = c.np; dc.nr = c.nr; dc.nt = c.nt;
     dc.dnum = c.dnum; dc.alpha = c.alpha; dc.npq = c.nq + c.np; dc.nqr = c.nq + c.nr;
     dc.idx_p = c.nq; dc.idx_r = c.nq + c.np; dc.idx_t = c.nq + c.np + c.nr; dc.idx_pt = nall - 1;
@@ -182,6 +182,18 @@ void build_context(Context& c, const kbfv_params& prm) {
 
     HostBconv q2r = make_bconv(Q, R), r2q = make_bconv(R, Q);
     c.h_q2r_hatinv = q2r.hatinv;
+    // last-stage constants of the inverse NTT over Q scaled by (Q/q_i)^-1: the
+    // transform then stores the base extension's y_i = [x_i (Q/q_i)^-1]_{q_i}
+    std::vector<tw_t> q2r_fold((size_t)2 * c.nq);
+    for (int i = 0; i < c.nq; i++) {
+        const uint64_t q = c.mods[i];
+        for (int k = 0; k < 2; k++) {
+            const uint64_t v = H::mulmod(twi[((size_t)i << c.logn) + k].x, q2r.hatinv[i], q);
+            q2r_fold[2 * i + k].x = v;
+            q2r_fold[2 * i + k].y = H::shoup(v, q);
+        }
+    }
+    size_t o_q2rf = blob.add(q2r_fold);
     size_t o_q2r[5] = {blob.add(q2r.hatinv), blob.add(q2r.hatinvs), blob.add(q2r.hat), blob.add(q2r.alpha),
                        blob.add(q2r.inv)};
     size_t o_r2q[5] = {blob.add(r2q.hatinv), blob.add(r2q.hatinvs), blob.add(r2q.hat), blob.add(r2q.alpha),
@@ -397,6 +409,7 @@ void build_context(Context& c, const kbfv_params& prm) {
     dc.tw_fwd = (const tw_t*)(base + o_twf); dc.tw_inv = (const tw_t*)(base + o_twi);
     dc.q2r_hatinv = U(o_q2r[0]); dc.q2r_hatinvs = U(o_q2r[1]); dc.q2r_hat = U(o_q2r[2]);
     dc.q2r_alpha = U(o_q2r[3]); dc.q2r_inv = D(o_q2r[4]);
+    dc.q2r_fold = (const tw_t*)(base + o_q2rf);
     dc.r2q_hatinv = U(o_r2q[0]); dc.r2q_hatinvs = U(o_r2q[1]); dc.r2q_hat = U(o_r2q[2]);
     dc.r2q_alpha = U(o_r2q[3]); dc.r2q_inv = D(o_r2q[4]);
     dc.sr_frac = D(o_srf); dc.sr_c = U(o_src);
@@ -445,7 +458,11 @@ uint8_t* ensure_scratch(Context& c, size_t bytes) {
 // 8: 32x32 high product, 9: 32-bit multiply-add, 10: mac32 (64x64->128
 // multiply-accumulate from 32-bit partial products), 11: forward butterfly
 // with shoup4_32 (the NTT kernels' butterfly), 12: 32-bit multiply-add issue
-// rate (16 dependent mad.lo.u32 per chain step, the IMAD pipe's peak).
+// rate (16 dependent mad.lo.u32 per chain step, the IMAD pipe's peak),
+// 13: 32x32->64 multiply-add issue rate (16 dependent mad.wide.u32 per step),
+// 14: 60x60-bit multiply-accumulate from 30-bit halves (mac30: four
+// mad.wide.u32 into three 64-bit column sums), 15: 32-bit high multiply-add
+// issue rate (16 dependent mad.hi.u32 per step).
 constexpr int kProbeChains = 8;
 constexpr int kImadPerStep = 16;
 template <int KIND>
@@ -485,6 +502,35 @@ __global__ void probe_arith_kernel(uint64_t* out, int iters, uint64_t q, uint64_
                 const uint32_t m = (uint32_t)b[c] | 1u, k = (uint32_t)a[c];
 #pragma unroll
                 for (int u = 0; u < kImadPerStep; u++) x = x * m + k;
+                acc[c].lo = x;
+            }
+            if (KIND == 13) {  // wide multiply-add issue: x = lo32(x) * m + x (64-bit)
+                uint64_t x = acc[c].lo;
+                const uint32_t m = (uint32_t)b[c] | 1u;
+#pragma unroll
+                for (int u = 0; u < kImadPerStep; u++)
+                    asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(x) : "r"((uint32_t)x), "r"(m));
+                acc[c].lo = x;
+            }
+            if (KIND == 14) {  // mac30: columns lo (a0 b0), mid (a0 b1 + a1 b0), hi (a1 b1)
+                constexpr uint64_t M30 = (1ULL << 30) - 1;
+                const uint32_t a0 = (uint32_t)(a[c] & M30), a1 = (uint32_t)(a[c] >> 30);
+                const uint32_t b0 = (uint32_t)(b[c] & M30), b1 = (uint32_t)(b[c] >> 30);
+                uint64_t lo = acc[c].lo, hi = acc[c].hi, mid = lo ^ hi;
+                asm("mad.wide.u32 %0, %3, %5, %0;\n\t"
+                    "mad.wide.u32 %1, %3, %6, %1;\n\t"
+                    "mad.wide.u32 %1, %4, %5, %1;\n\t"
+                    "mad.wide.u32 %2, %4, %6, %2;"
+                    : "+l"(lo), "+l"(mid), "+l"(hi)
+                    : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+                acc[c].lo = lo + (mid << 30);
+                acc[c].hi = hi + (mid >> 34);
+            }
+            if (KIND == 15) {  // high multiply-add issue: x = hi32(x * m) + k
+                uint32_t x = (uint32_t)acc[c].lo;
+                const uint32_t m = (uint32_t)b[c] | 0x80000001u, k = (uint32_t)a[c];
+#pragma unroll
+                for (int u = 0; u < kImadPerStep; u++) asm("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x) : "r"(m), "r"(k));
                 acc[c].lo = x;
             }
             if (KIND == 11) {  // the NTT kernels' butterfly (Shoup product from 32-bit multiplies)
@@ -660,6 +706,14 @@ int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
                 KB_REQUIRE(value == 1 || value == 2, KBFV_ERR_INVALID, "base-conversion coefficients per thread: 1 or 2");
                 c.dc.shape.bconv_cpt = (int)value;
                 break;
+            case KBFV_TUNE_FUSE_Q2R_PAIRS:
+                KB_REQUIRE(value >= 0 && value <= kMaxBatch, KBFV_ERR_INVALID, "fused Q -> R pairs must be 0..128");
+                c.dc.shape.fuse_q2r_pairs = (int)value;
+                break;
+            case KBFV_TUNE_L2_PREFETCH:
+                KB_REQUIRE(value == 0 || value == 1, KBFV_ERR_INVALID, "L2 prefetch: 0 or 1");
+                c.dc.shape.l2_prefetch = (int)value;
+                break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
         // the levels of a top context run with the top level's knobs
@@ -685,6 +739,8 @@ int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value) {
             case KBFV_TUNE_K5_THREADS: *value = c.dc.shape.k5_threads; break;
             case KBFV_TUNE_K5_FUSED_PAIRS: *value = c.dc.shape.k5_fused_pairs; break;
             case KBFV_TUNE_BCONV_CPT: *value = c.dc.shape.bconv_cpt; break;
+            case KBFV_TUNE_FUSE_Q2R_PAIRS: *value = c.dc.shape.fuse_q2r_pairs; break;
+            case KBFV_TUNE_L2_PREFETCH: *value = c.dc.shape.l2_prefetch; break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
     });
@@ -756,7 +812,7 @@ int kbfv_set_seed(kbfv_context* ctx, const uint8_t seed[32]) {
 
 int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
     return guarded([&] {
-        KB_REQUIRE(kind >= 0 && kind <= 12 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
+        KB_REQUIRE(kind >= 0 && kind <= 15 && gops && iters >= 1, KBFV_ERR_INVALID, "bad probe arguments");
         int dev = 0, sms = 0;
         KB_CHECK_CUDA(cudaGetDevice(&dev));
         KB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -776,6 +832,7 @@ int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
             switch (kind) {
 #define P_K(K) case K: probe_arith_kernel<K><<<blocks, threads>>>(out, (int)iters, q, mh, ml, mp); break;
                 P_K(0) P_K(1) P_K(2) P_K(3) P_K(4) P_K(5) P_K(6) P_K(7) P_K(8) P_K(9) P_K(10) P_K(11) P_K(12)
+                P_K(13) P_K(14) P_K(15)
 #undef P_K
             }
             KB_CHECK_CUDA(cudaEventRecord(e1));
@@ -786,7 +843,8 @@ int kbfv_probe_arith(int kind, uint32_t iters, double* gops) {
         cudaEventDestroy(e1);
         cudaFree(out);
         check_launch("probe_arith");
-        *gops = (double)blocks * threads * iters * kProbeChains * (kind == 12 ? kImadPerStep : 1) / (ms * 1e6);
+        const bool issue = kind == 12 || kind == 13 || kind == 15;
+        *gops = (double)blocks * threads * iters * kProbeChains * (issue ? kImadPerStep : 1) / (ms * 1e6);
     });
 }
 

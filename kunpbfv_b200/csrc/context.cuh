@@ -23,6 +23,9 @@ struct LaunchShape {
     int bconv_cpt;       // coefficients per thread of the base conversion (1 or 2)
     int k5_threads;      // CTA size of K5
     int k5_fused_pairs;  // batches of at most this many pairs run K5 as one kernel
+    int fuse_q2r_pairs;  // batches of at most this many pairs run the Q -> R base extension in the
+                         // loader of the NTT over R (no K2 launch)
+    int l2_prefetch;     // 1: block kernels ask L2 for the block one wave of CTAs ahead
 };
 
 // Everything a kernel needs, passed by value (all pointers into one device pool).
@@ -40,6 +43,7 @@ struct DevConsts {
     // HPS base extension Q -> R
     const uint64_t *q2r_hatinv, *q2r_hatinvs, *q2r_hat, *q2r_alpha;
     const double* q2r_inv;
+    const tw_t* q2r_fold;  // [nq][2]: the inverse NTT's last-stage constants times (Q/q_i)^-1 mod q_i
     // HPS base extension R -> Q
     const uint64_t *r2q_hatinv, *r2q_hatinvs, *r2q_hat, *r2q_alpha;
     const double* r2q_inv;

@@ -78,32 +78,47 @@ static inline unsigned stride_blocks(size_t total, unsigned threads) {
     return (unsigned)std::min<size_t>((total + threads - 1) / threads, (size_t)1 << 20);
 }
 
+// CTAs of `kernel` that fit on the device at once (SMs x CTAs per SM)
+static inline int resident_ctas(const void* kernel, int threads, int smem) {
+    int dev = 0, sms = 0, per = 0;
+    KB_CHECK_CUDA(cudaGetDevice(&dev));
+    KB_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    KB_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+    return sms * std::max(per, 1);
+}
+
 template <int LOGB, class Src, class Dst, bool FULL = true>
 static void launch_fwd_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
     constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;
     static bool configured = false;
+    static int resident = 0;  // CTAs of this kernel resident at once on the device
     if (!configured) {
         KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_fwd_block_kernel<LOGB, Src, Dst, FULL>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        resident = resident_ctas((const void*)ntt_fwd_block_kernel<LOGB, Src, Dst, FULL>,
+                                 BlockShape<LOGB>::THREADS, SMEM);
         configured = true;
     }
     const int nblk = 1 << (logn - LOGB);
     ntt_fwd_block_kernel<LOGB, Src, Dst, FULL><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
-        s, d, dc.tw_fwd, dc.mods, logn);
+        s, d, dc.tw_fwd, dc.mods, logn, dc.shape.l2_prefetch ? resident : 0);
 }
 
 template <int LOGB, class Src, class Dst, bool WHOLE>
 static void launch_inv_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
     constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;
     static bool configured = false;
+    static int resident = 0;  // CTAs of this kernel resident at once on the device
     if (!configured) {
         KB_CHECK_CUDA(cudaFuncSetAttribute(ntt_inv_block_kernel<LOGB, Src, Dst, WHOLE>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+        resident = resident_ctas((const void*)ntt_inv_block_kernel<LOGB, Src, Dst, WHOLE>,
+                                 BlockShape<LOGB>::THREADS, SMEM);
         configured = true;
     }
     const int nblk = 1 << (logn - LOGB);
     ntt_inv_block_kernel<LOGB, Src, Dst, WHOLE><<<rows * nblk, BlockShape<LOGB>::THREADS, SMEM, st>>>(
-        s, d, dc.tw_inv, dc.mods, logn);
+        s, d, dc.tw_inv, dc.mods, logn, dc.shape.l2_prefetch ? resident : 0);
 }
 
 // The view of a store target that the column pass of a split transform writes

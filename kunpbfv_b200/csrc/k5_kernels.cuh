@@ -1,9 +1,11 @@
 // K5 of the multiply pipeline, per coefficient: t/Q scale-and-round Q|R -> R,
-// the base extension R -> Q and the key-switch digit lift. Each bucket of the
+// the base extension R -> Q and the key-switch digit lift; and K3 with the
+// Q -> R base extension in its loader (q2r_ntt.cuh). Each bucket of the
 // prime count (MAXQ) is instantiated in its own translation unit
 // (k5_m<MAXQ>.cu) so that the unrolled variants compile in parallel.
 #pragma once
 #include "mixed.cuh"
+#include "q2r_ntt.cuh"
 
 // K5 in one kernel, for launches of one or two pairs (one launch less on the
 // per-call path): scale-and-round to R, R -> Q, and (mode 1) the key-switch

@@ -1,6 +1,7 @@
 // K5 kernels for contexts of at most 15 ciphertext primes (the MAXQ = 16 bucket)
 #include "k5_kernels.cuh"
 
+template void q2r_ntt_launch_m<16>(const DevConsts&, const uint64_t*, uint64_t*, int, cudaStream_t);
 template void k5_launch_m<16>(const DevConsts&, int, const MulScratch&, uint64_t*, int, cudaStream_t);
 template void bconv_mixed_launch_m<16>(const Groups&, const LaunchShape&, int, const MulScratch&, cudaStream_t);
 template void k5_mixed_launch_m<16>(const Groups&, const LaunchShape&, int, const MulScratch&, cudaStream_t);

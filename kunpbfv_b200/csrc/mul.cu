@@ -25,13 +25,22 @@ void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* key, int 
 
 void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st) {
     const DevConsts& dc = c.dc;
-    // K1: INTT over Q of [a1, b1, a2, b2]
-    ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), count * 4 * dc.nq, st);
-    // K2: Q -> R (centred)
-    launch_bconv(dc, q2r_tables(dc), m.sa, m.sb, count * 4, (size_t)dc.nq << dc.logn, (size_t)dc.nr << dc.logn, st);
-    // K3: NTT over R in place, fully reduced (the tensor's products use barrett_prod)
-    ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr),
-                                   count * 4 * dc.nr, st);
+    if (count <= dc.shape.fuse_q2r_pairs) {
+        // K1 stores y_i = [x_i (Q/q_i)^-1]_{q_i}; K3's loader extends them to R
+        ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, QHatRowsIO{m.sa, dc.logn, dc.nq, dc.q2r_fold},
+                count * 4 * dc.nq, st);
+#define L_Q2R(M) q2r_ntt_launch_m<M>(dc, m.sa, m.sb, count * 4, st)
+        DISPATCH_MAXQ(dc.nq, L_Q2R);
+#undef L_Q2R
+    } else {
+        // K1: INTT over Q of [a1, b1, a2, b2]
+        ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, rows_io(dc, m.sa, 0, dc.nq), count * 4 * dc.nq, st);
+        // K2: Q -> R (centred)
+        launch_bconv(dc, q2r_tables(dc), m.sa, m.sb, count * 4, (size_t)dc.nq << dc.logn, (size_t)dc.nr << dc.logn, st);
+        // K3: NTT over R in place, fully reduced (the tensor's products use barrett_prod)
+        ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sb, dc.idx_r, dc.nr), rows_io(dc, m.sb, dc.idx_r, dc.nr),
+                                       count * 4 * dc.nr, st);
+    }
     // K4: tensor (Q part from the NTT-form inputs, R part from K3) fused into INTT over Q|R
     TensorSrc ts{pb, m.sb, dc};
     ntt_inv(dc, ts, QRRowsIO{m.sc, dc.logn, dc.nq, dc.nqr, dc.idx_r}, count * 3 * dc.nqr, st);

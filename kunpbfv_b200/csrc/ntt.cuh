@@ -52,6 +52,48 @@ __device__ __forceinline__ RowTab row_tab(const Src& s, int row, bool inverse, c
     }
 }
 
+// The two constants of the inverse transform's last stage (n^-1 and
+// psi_br^-1[1] * n^-1, with their Shoup companions): tw[0] and tw[1] of the
+// row's table, unless the store target scales its row by a constant c, in
+// which case `fold(row)` points to the same two constants times c (the
+// product comes out scaled at no extra multiply).
+template <class T, class = void>
+struct has_fold : std::false_type {};
+template <class T>
+struct has_fold<T, std::void_t<decltype(std::declval<const T&>().fold(0))>> : std::true_type {};
+
+template <class Dst>
+__device__ __forceinline__ const tw_t* fold_tab(const Dst& d, int row, const tw_t* tw) {
+    if constexpr (has_fold<Dst>::value) return d.fold(row);
+    else return tw;
+}
+
+// A source that can name its rows' input ranges (`prefetch(row, off, n)`)
+// lets a block kernel ask L2 for the block that starts one wave of CTAs after
+// its own: the copy runs while this CTA computes, and the later CTA's first
+// pass reads L2 instead of waiting on HBM (one CTA per SM at N = 2^14, so
+// its load phase is otherwise not overlapped with any computation).
+template <class T, class = void>
+struct has_prefetch : std::false_type {};
+template <class T>
+struct has_prefetch<T, std::void_t<decltype(std::declval<const T&>().prefetch(0, 0, 0))>> : std::true_type {};
+
+// asynchronous copy of `bytes` (a multiple of 16, 16-byte aligned) into L2
+__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// the block `ahead` CTAs after this one (ahead = CTAs resident at once; 0: none)
+template <int LOGB, class Src>
+__device__ __forceinline__ void prefetch_next(const Src& src, int ahead, int nblk) {
+    if constexpr (has_prefetch<Src>::value) {
+        if (ahead > 0 && threadIdx.x == 0) {
+            const unsigned nxt = blockIdx.x + (unsigned)ahead;
+            if (nxt < gridDim.x) src.prefetch((int)(nxt / nblk), (int)(nxt % nblk) << LOGB, 1 << LOGB);
+        }
+    }
+}
+
 __device__ __forceinline__ int spad(int j) { return j + (j >> 4); }
 
 // Shoup product with a quotient estimate from three 32-bit partial products
@@ -158,8 +200,8 @@ __device__ __forceinline__ void fwd_group(uint64_t* x, const tw_t* __restrict__ 
 }
 
 // R inverse stages (reverse order). `fold` (only with s0 == 0, hi == 0) applies
-// n^-1 at global stage 0 using tw[0] = n^-1, tw[1] = psi_br^-1[1] * n^-1 and
-// fully reduces.
+// n^-1 at global stage 0 using ftw[0] = n^-1, ftw[1] = psi_br^-1[1] * n^-1
+// (ftw = tw, or a scaled pair: fold_tab) and fully reduces.
 template <int R, int U, int H>
 __device__ __forceinline__ void inv_stage_h(uint64_t* x, const tw_t* __restrict__ tw, int bidx, uint64_t q,
                                             uint64_t q4) {
@@ -173,12 +215,12 @@ __device__ __forceinline__ void inv_stage_h(uint64_t* x, const tw_t* __restrict_
 }
 template <int R, int U>
 __device__ __forceinline__ void inv_stages(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi, uint64_t q,
-                                           uint64_t q4, bool fold) {
+                                           uint64_t q4, bool fold, const tw_t* __restrict__ ftw) {
     if constexpr (U >= 0) {
         constexpr int half = 1 << (R - 1 - U);
         if (U == 0 && fold) {
-            const tw_t ni = tw[0];
-            const tw_t w1 = tw[1];
+            const tw_t ni = ftw[0];
+            const tw_t w1 = ftw[1];
 #pragma unroll
             for (int k = 0; k < half; k++) {
                 const uint64_t a = x[k], b = x[k + half];
@@ -188,13 +230,13 @@ __device__ __forceinline__ void inv_stages(uint64_t* x, const tw_t* __restrict__
         } else {
             inv_stage_h<R, U, 0>(x, tw, (1 << (s0 + U)) + (hi << U), q, q4);
         }
-        inv_stages<R, U - 1>(x, tw, s0, hi, q, q4, fold);
+        inv_stages<R, U - 1>(x, tw, s0, hi, q, q4, fold, ftw);
     }
 }
 template <int R>
 __device__ __forceinline__ void inv_group(uint64_t* x, const tw_t* __restrict__ tw, int s0, int hi,
-                                          uint64_t q, uint64_t q4, bool fold) {
-    inv_stages<R, R - 1>(x, tw, s0, hi, q, q4, fold);
+                                          uint64_t q, uint64_t q4, bool fold, const tw_t* __restrict__ ftw = nullptr) {
+    inv_stages<R, R - 1>(x, tw, s0, hi, q, q4, fold, ftw ? ftw : tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -341,7 +383,7 @@ __device__ __forceinline__ constexpr bool inv_direct_load() {
 template <int LOGB, class Src, class Dst, bool FULL = true>
 static __global__ void __launch_bounds__(1 << (LOGB - 4))
 ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
-                     int logn) {
+                     int logn, int ahead) {
     constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
     constexpr int R0 = RAD < LOGB ? RAD : LOGB, G0 = 1 << R0, lb0 = LOGB - R0;
     extern __shared__ uint64_t sm[];
@@ -353,6 +395,7 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const auto s = src.bind(row);
     const uint64_t q = rt.q, q4 = q << 2;
     PassCtx c{sm, rt.tw, t, logn - LOGB, blk << LOGB, logn, q, q4};
+    prefetch_next<LOGB>(src, ahead, nblk);
 
     // pass 0 straight from global memory: groups gi + k * 2^lb0 (consecutive lanes, coalesced);
     // groups one after another so fused loaders keep their temporaries in registers
@@ -385,7 +428,7 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
 template <int LOGB, class Src, class Dst, bool WHOLE = true>
 static __global__ void __launch_bounds__(1 << (LOGB - 4))
 ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
-                     int logn) {
+                     int logn, int ahead) {
     constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
     constexpr int R0 = RAD < LOGB ? RAD : LOGB, G0 = 1 << R0, lb0 = LOGB - R0;
     extern __shared__ uint64_t sm[];
@@ -397,6 +440,7 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const auto s = src.bind(row);
     const uint64_t q = rt.q, q4 = q << 2;
     PassCtx c{sm, rt.tw, t, logn - LOGB, blk << LOGB, logn, q, q4};
+    prefetch_next<LOGB>(src, ahead, nblk);
 
     if constexpr (inv_direct_load<LOGB, RAD>()) {
         inv_passes_load<LOGB, RAD, R0>(c, s);
@@ -411,6 +455,7 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     }
     // pass 0 (local stages 0..R0-1), coalesced stores
     const auto d = dst.bind(row);
+    const tw_t* ftw = fold_tab(dst, row, c.tw);
 #pragma unroll 1
     for (int g = 0; g < 16 / G0; g++) {
         const int gi = g * T + t;
@@ -418,7 +463,7 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
         const int pg = spad(gi);
 #pragma unroll
         for (int k = 0; k < G0; k++) x[k] = sm[spad_off<lb0>(pg, gi, k)];
-        inv_group<R0>(x, c.tw, c.sbase, c.goff >> LOGB, q, q4, WHOLE);
+        inv_group<R0>(x, c.tw, c.sbase, c.goff >> LOGB, q, q4, WHOLE, ftw);
 #pragma unroll
         for (int k = 0; k < G0; k++) d.store(c.goff + gi + (k << lb0), x[k]);
     }
@@ -460,7 +505,7 @@ __device__ __forceinline__ void ntt_inv_col(const Src& src, const Dst& dst, cons
     uint64_t x[1 << RC];
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) x[k] = s.load(c + k * cols);
-    inv_group<RC>(x, tw, 0, 0, q, q4, true);
+    inv_group<RC>(x, tw, 0, 0, q, q4, true, fold_tab(dst, row, tw));
 #pragma unroll
     for (int k = 0; k < (1 << RC); k++) d.store(c + k * cols, x[k]);
 }
@@ -487,6 +532,7 @@ static __global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restri
 // ---------------------------------------------------------------------------
 struct PtrRow {
     uint64_t* p;
+    __device__ __forceinline__ void prefetch(int off, int n) const { l2_prefetch(p + off, (uint32_t)n * 8); }
     __device__ __forceinline__ uint64_t load(int j) const { return p[j]; }
     __device__ __forceinline__ void store(int j, uint64_t v) const { p[j] = v; }
 };
@@ -499,6 +545,7 @@ struct RowsIO {
     int period;
     __device__ __forceinline__ int prime(int row) const { return p0 + row % period; }
     __device__ __forceinline__ PtrRow bind(int row) const { return PtrRow{base + ((size_t)row << logn)}; }
+    __device__ __forceinline__ void prefetch(int row, int off, int n) const { bind(row).prefetch(off, n); }
 };
 
 }  // namespace kbfv

@@ -16,6 +16,19 @@ struct PairQRowsP {
         const uint64_t* base = p < 2 ? pb.a[item] : pb.b[item];
         return PtrRow{const_cast<uint64_t*>(base) + (((size_t)(p & 1) * nq + l) << logn)};
     }
+    __device__ __forceinline__ void prefetch(int row, int off, int n) const { bind(row).prefetch(off, n); }
+};
+
+// K1 store target when the Q -> R base extension runs inside K3: rows over Q
+// (RowsIO layout) holding y_i = [x_i (Q/q_i)^-1]_{q_i}, the scale folded into
+// the inverse transform's last-stage constants
+struct QHatRowsIO {
+    uint64_t* base;
+    int logn, nq;
+    const tw_t* fold_base;  // DevConsts::q2r_fold
+    __device__ __forceinline__ int prime(int row) const { return row % nq; }
+    __device__ __forceinline__ PtrRow bind(int row) const { return PtrRow{base + ((size_t)row << logn)}; }
+    __device__ __forceinline__ const tw_t* fold(int row) const { return fold_base + 2 * (row % nq); }
 };
 
 // rows of consecutive Q|R polynomials; limb l of Q|R uses prime l (Q) or idx_r + l - nq (R)
@@ -340,6 +353,10 @@ void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, c
 // K5: scale-and-round, R -> Q and (mode 1) the key-switch digit lift
 template <int MAXQ>
 void k5_launch_m(const DevConsts& dc, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st);
+// K3 with the Q -> R base extension in its loader: `polys` polynomials of y
+// rows over Q (QHatRowsIO layout) -> NTT-form R limbs, fully reduced
+template <int MAXQ>
+void q2r_ntt_launch_m(const DevConsts& dc, const uint64_t* y, uint64_t* out, int polys, cudaStream_t st);
 void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st);
 // key-switch tail: key product, mod down and add, written to the outputs of pb
 void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* key, int ndig, uint64_t* se,

@@ -13,7 +13,10 @@ Knobs (include/kbfv.h, ``kbfv_tune_knob``):
   (CTA size of the Q -> R base conversion), ``k5_threads`` (CTA size of the
   scale-and-round / R -> Q / digit-lift kernels) and ``k5_fused_pairs``
   (batches of at most this many pairs run those as one kernel), ``bconv_cpt``
-  (coefficients per thread of the base conversion).
+  (coefficients per thread of the base conversion) and ``fuse_q2r_pairs``
+  (batches of at most this many pairs run the Q -> R base extension in the
+  loader of the forward NTT over R, no separate base-conversion launch),
+  ``l2_prefetch`` (NTT block kernels ask L2 for the block one wave ahead).
 
 Each candidate is timed on the device with CUDA events (two warm-up calls,
 then the median of three timed trials of ``reps`` calls). Knobs never change
@@ -44,9 +47,12 @@ PIPELINE_KNOBS = {
     "bconv_cpt": (2, 1),
     "k5_threads": (128, 64, 256),
     "split_rows": (48, 0, 256, 1 << 20),
+    "l2_prefetch": (1, 0),
 }
 # tuned on a two-pair multiply (the per-call size it governs)
 K5_FUSED_PAIRS = (2, 0, 4)
+# tuned on one-pair and two-pair multiplies together
+FUSE_Q2R_PAIRS = (1, 0, 2)
 
 
 def cache_key(device: str, log_n: int, q_count: int, p_count: int, dnum: int, pairs: int) -> str:
@@ -173,14 +179,16 @@ def tune_host_chunk(scheme, pairs: int = 64, reps: int = 3) -> Dict[str, object]
 
 def _sweep(ctx, knob, values, run, out, want, reps):
     """Time `run` for every value of `knob` (others as set); every output must
-    equal `want`. Leaves the fastest value applied; returns {value: ms}."""
+    equal `want` (a ciphertext and its expected tensor, or tuples of both).
+    Leaves the fastest value applied; returns {value: ms}."""
     import torch
+    outs, wants = (out, want) if isinstance(out, tuple) else ((out,), (want,))
     ms = {}
     for v in values:
         ctx.tune_set(knob, v)
         run()
         torch.cuda.synchronize()
-        if not torch.equal(out.cipher_device, want):
+        if not all(torch.equal(o.cipher_device, w) for o, w in zip(outs, wants)):
             raise RuntimeError(f"{knob}={v} changed the product")
         ms[v] = round(time_ms(run, reps), 4)
     ctx.tune_set(knob, min(ms, key=ms.get))
@@ -189,13 +197,14 @@ def _sweep(ctx, knob, values, run, out, want, reps):
 
 def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
     """The multiply pipeline's knobs (PIPELINE_KNOBS on a batch of `pairs`,
-    K5_FUSED_PAIRS on two pairs), one at a time from the defaults; every
-    candidate's product is compared with the default shapes' product."""
+    K5_FUSED_PAIRS on two pairs, FUSE_Q2R_PAIRS on one and two pairs), one at
+    a time from the defaults; every candidate's product is compared with the
+    default shapes' product."""
     import torch
 
     from .api import Ciphertext
     ctx = scheme.context
-    keep = {k: ctx.tune_get(k) for k in list(PIPELINE_KNOBS) + ["k5_fused_pairs"]}
+    keep = {k: ctx.tune_get(k) for k in list(PIPELINE_KNOBS) + ["k5_fused_pairs", "fuse_q2r_pairs"]}
     c1 = Ciphertext(ctx, _random_pairs(ctx, pairs, 2))
     c2 = Ciphertext(ctx, _random_pairs(ctx, pairs, 3))
     out = Ciphertext(ctx, count=pairs)
@@ -203,21 +212,33 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
     d1 = Ciphertext(ctx, c1.cipher_device[:two].clone())
     d2 = Ciphertext(ctx, c2.cipher_device[:two].clone())
     out2 = Ciphertext(ctx, count=two)
+    e1 = Ciphertext(ctx, c1.cipher_device[:1].clone())
+    e2 = Ciphertext(ctx, c2.cipher_device[:1].clone())
+    out1 = Ciphertext(ctx, count=1)
     result: Dict[str, object] = {}
     try:
         for k, vals in PIPELINE_KNOBS.items():  # defaults first: the reference products
             ctx.tune_set(k, vals[0])
         ctx.tune_set("k5_fused_pairs", K5_FUSED_PAIRS[0])
+        ctx.tune_set("fuse_q2r_pairs", FUSE_Q2R_PAIRS[0])
         scheme.mult_relin(c1, c2, out=out)
         scheme.mult_relin(d1, d2, out=out2)
+        scheme.mult_relin(e1, e2, out=out1)
         torch.cuda.synchronize()
-        want, want2 = out.cipher_device.clone(), out2.cipher_device.clone()
+        want, want2, want1 = out.cipher_device.clone(), out2.cipher_device.clone(), out1.cipher_device.clone()
         for k, vals in PIPELINE_KNOBS.items():
             ms = _sweep(ctx, k, vals, lambda: scheme.mult_relin(c1, c2, out=out), out, want, reps)
             result[k], result[k + "_ms"] = min(ms, key=ms.get), {str(v): t for v, t in ms.items()}
         ms = _sweep(ctx, "k5_fused_pairs", K5_FUSED_PAIRS, lambda: scheme.mult_relin(d1, d2, out=out2), out2,
                     want2, reps)
         result["k5_fused_pairs"], result["k5_fused_pairs_ms"] = min(ms, key=ms.get), {
+            str(v): t for v, t in ms.items()}
+
+        def per_call():
+            scheme.mult_relin(e1, e2, out=out1)
+            scheme.mult_relin(d1, d2, out=out2)
+        ms = _sweep(ctx, "fuse_q2r_pairs", FUSE_Q2R_PAIRS, per_call, (out1, out2), (want1, want2), reps)
+        result["fuse_q2r_pairs"], result["fuse_q2r_pairs_ms"] = min(ms, key=ms.get), {
             str(v): t for v, t in ms.items()}
     except Exception:
         for k, v in keep.items():
@@ -226,7 +247,8 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
     return result
 
 
-PIPELINE_CHOICES = ("branches", "bconv_threads", "bconv_cpt", "k5_threads", "split_rows", "k5_fused_pairs")
+PIPELINE_CHOICES = ("branches", "bconv_threads", "bconv_cpt", "k5_threads", "split_rows", "l2_prefetch",
+                    "k5_fused_pairs", "fuse_q2r_pairs")
 
 
 def apply_choice(ctx, choice: dict) -> None:

@@ -54,12 +54,14 @@ def test_autotune_applies_and_caches(tmp_path):
     assert ctx.tune_get("branches") == got["branches"]
     assert ctx.tune_get("host_chunk") == got["host_chunk"]
     assert set(got["branches_ms"]) == {str(b) for b in tune.BRANCHES}
-    for k in ("bconv_threads", "k5_threads", "split_rows", "k5_fused_pairs"):
+    for k in ("bconv_threads", "bconv_cpt", "k5_threads", "split_rows", "k5_fused_pairs", "fuse_q2r_pairs"):
         assert ctx.tune_get(k) == got[k], k
+    assert set(got["fuse_q2r_pairs_ms"]) == {str(v) for v in tune.FUSE_Q2R_PAIRS}
     # a fresh context of the same parameters takes the cached choice without timing
     ctx2 = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
     hit = tune.autotune(ctx2, None, pairs=32, cache_path=cache)
     assert hit["cached"] and ctx2.tune_get("branches") == got["branches"]
+    assert ctx2.tune_get("fuse_q2r_pairs") == got["fuse_q2r_pairs"]
     assert tune.apply_cached(ctx2, pairs=32, cache_path=cache)["host_chunk"] == got["host_chunk"]
 
 
@@ -100,7 +102,8 @@ def test_host_chunk_knob_drives_the_default_chunk():
 
 @pytest.mark.parametrize("knob,values", [("bconv_threads", (64, 128, 256, 512)), ("k5_threads", (64, 128, 256)),
                                          ("split_rows", (0, 48, 1 << 20)), ("k5_fused_pairs", (0, 2, 4)),
-                                         ("bconv_cpt", (1, 2))])
+                                         ("bconv_cpt", (1, 2)), ("fuse_q2r_pairs", (128, 0, 1)),
+                                         ("l2_prefetch", (0, 1))])
 def test_pipeline_shapes_keep_the_product(knob, values):
     """Every launch shape of the multiply pipeline gives the oracle's product
     (N=16384, 7 + 1 primes; 3 pairs: K5 fused or split by k5_fused_pairs,
@@ -139,12 +142,54 @@ def test_pipeline_knob_bounds_and_levels():
     import kunpbfv_b200 as kb
     ctx = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
     for knob, bad in (("bconv_threads", 100), ("bconv_threads", 1024), ("k5_threads", 512), ("k5_threads", 32),
-                      ("split_rows", -1), ("k5_fused_pairs", 129)):
+                      ("split_rows", -1), ("k5_fused_pairs", 129), ("fuse_q2r_pairs", 129), ("bconv_cpt", 3),
+                      ("l2_prefetch", 2)):
         with pytest.raises(kb.KbfvError):
             ctx.tune_set(knob, bad)
     assert (ctx.tune_get("split_rows"), ctx.tune_get("bconv_threads"), ctx.tune_get("k5_threads"),
-            ctx.tune_get("k5_fused_pairs"), ctx.tune_get("bconv_cpt")) == (48, 256, 128, 2, 2)
+            ctx.tune_get("k5_fused_pairs"), ctx.tune_get("bconv_cpt"), ctx.tune_get("fuse_q2r_pairs"),
+            ctx.tune_get("l2_prefetch")) == (48, 256, 128, 2, 2, 1, 1)
     lv = ctx.at_level(2)
     ctx.tune_set("k5_threads", 64)
     assert lv.tune_get("k5_threads") == 64  # levels follow the top level's knobs
     assert ctx.at_level(1).tune_get("k5_threads") == 64  # and so do levels made later
+
+
+@pytest.mark.parametrize("log_n,q_bits,p_bits,dnum,pairs,split_rows", [
+    (14, [60] * 7, [60], 1, 5, 48),        # whole-ring blocks (140- and 160-row transforms)
+    (14, [60] * 7, [60], 1, 1, 48),        # per-call size: column pass + 2^12 blocks, scale folded in the column pass
+    (14, [60] * 7, [60], 1, 3, 1 << 20),   # every transform split
+    (13, [50] * 3, [52], 3, 4, 48),        # 2^13 blocks, three digits
+    (15, [55] * 10, [58] * 2, 5, 2, 48),   # 2^15 column pass + blocks; 10 primes (the 16-prime bucket)
+    (16, [58] * 18, [60] * 2, 3, 1, 48),   # 2^16; 18 primes (the 24-prime bucket)
+])
+def test_fused_q2r_keeps_the_product(log_n, q_bits, p_bits, dnum, pairs, split_rows):
+    """The Q -> R base extension inside the NTT over R gives the products of
+    the separate base-conversion launch (itself pinned to the oracle by the
+    multiply tests), for mult_relin and for the tensor alone, on every
+    transform shape: whole-ring blocks, the split at N=2^14, the 2^15/2^16
+    column passes (the scaled last inverse stage then runs in the column
+    kernel) and the prime-count buckets."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200 import tune
+    ctx = kb.BFVContext.from_bits(log_n, q_bits, p_bits, 786433 if log_n == 16 else 65537, dnum=dnum)
+    sk = kb.SecretKey(ctx, b"\x51" * 32)
+    sch = kb.BFVScheme(ctx, b"\x52" * 32)
+    sch.addMultKey_23(sk)
+    c1 = kb.Ciphertext(ctx, tune._random_pairs(ctx, pairs, 21))
+    c2 = kb.Ciphertext(ctx, tune._random_pairs(ctx, pairs, 22))
+    keep = (ctx.tune_get("fuse_q2r_pairs"), ctx.tune_get("split_rows"))
+    try:
+        ctx.tune_set("split_rows", split_rows)
+        got = {}
+        for fuse in (0, 1):
+            ctx.tune_set("fuse_q2r_pairs", 128 * fuse)
+            got[fuse] = (sch.mult_relin(c1, c2).cipher_device.clone(), sch.mult(c1, c2).data.clone())
+        torch.cuda.synchronize()
+        assert torch.equal(got[0][0], got[1][0]), "mult_relin"
+        assert torch.equal(got[0][1], got[1][1]), "mult (tensor)"
+    finally:
+        ctx.tune_set("fuse_q2r_pairs", keep[0])
+        ctx.tune_set("split_rows", keep[1])
