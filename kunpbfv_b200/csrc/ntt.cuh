@@ -260,6 +260,53 @@ struct BlockShape {
     static constexpr int RAD = 4;
 };
 
+// Teams. After the forward transform's first radix-16 pass (before the
+// inverse's last) the block splits into independent sub-blocks of 2^(LOGB-4)
+// points, each held by 2^(LOGB-8) consecutive threads in every later pass. A
+// team of 128 threads owns 2048 contiguous points and synchronises those
+// passes with a named barrier of its own (ids 1..COUNT), so teams drift apart
+// and one team's shared-memory exchange overlaps the others' arithmetic. Blocks
+// of at most 2048 points are one team (the CTA barrier).
+template <int LOGB>
+struct Teams {
+    static constexpr int T = (1 << LOGB) / 16;
+    static constexpr int SIZE = T < 128 ? T : 128;
+    static constexpr int COUNT = T / SIZE;
+    static constexpr int TB = LOGB - 8;  // log2 of the threads of one sub-block
+};
+
+template <int LOGB>
+__device__ __forceinline__ void team_sync() {
+    if constexpr (Teams<LOGB>::COUNT == 1) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / Teams<LOGB>::SIZE), "n"(Teams<LOGB>::SIZE)
+                     : "memory");
+    }
+}
+
+// group index of register group g of thread t in a pass of R stages whose
+// groups are 2^R adjacent points (lb = 0, NG = 16 / 2^R groups per thread):
+// with teams, a thread's groups stay inside its own sub-block
+template <int LOGB, int R>
+__device__ __forceinline__ int adjacent_group(int g, int t) {
+    if constexpr (Teams<LOGB>::COUNT == 1) {
+        return g * Teams<LOGB>::T + t;
+    } else {
+        constexpr int TB = Teams<LOGB>::TB;
+        return ((t >> TB) << (LOGB - 4 - R)) | (g << TB) | (t & ((1 << TB) - 1));
+    }
+}
+
+// point k of thread t in a coalesced sweep of the block (k < 16): with teams,
+// the sweep covers the thread's own team's 2048 points
+template <int LOGB>
+__device__ __forceinline__ int sweep_index(int t, int k) {
+    constexpr int S = Teams<LOGB>::SIZE;
+    if constexpr (Teams<LOGB>::COUNT == 1) return t + k * Teams<LOGB>::T;
+    else return (t / S) * (S * 16) + (t % S) + k * S;
+}
+
 struct PassCtx {
     uint64_t* sm;
     const tw_t* tw;
@@ -280,13 +327,14 @@ __device__ __forceinline__ int group_base(int gi) {
     return ((gi >> lb) << (lb + R)) | (gi & ((1 << lb) - 1));
 }
 
-// one forward pass over shared memory
+// one forward pass over shared memory (a pass after the first: team-local)
 template <int LOGB, int S0, int R>
 __device__ __forceinline__ void fwd_pass_smem(const PassCtx& c) {
     constexpr int T = (1 << LOGB) / 16, G = 1 << R, NG = 16 / G, lb = LOGB - S0 - R;
+    static_assert(NG == 1 || lb == 0, "only the last pass holds several groups per thread");
 #pragma unroll
     for (int g = 0; g < NG; g++) {
-        const int lbase = group_base<LOGB, S0, R>(g * T + c.t);
+        const int lbase = group_base<LOGB, S0, R>(NG == 1 ? c.t : adjacent_group<LOGB, R>(g, c.t));
         const int pbase = spad(lbase);
         uint64_t x[G];
 #pragma unroll
@@ -296,7 +344,7 @@ __device__ __forceinline__ void fwd_pass_smem(const PassCtx& c) {
 #pragma unroll
         for (int k = 0; k < G; k++) c.sm[spad_off<lb>(pbase, lbase, k)] = x[k];
     }
-    __syncthreads();
+    team_sync<LOGB>();
 }
 
 template <int LOGB, int RAD, int S0>
@@ -308,13 +356,17 @@ __device__ __forceinline__ void fwd_passes(const PassCtx& c) {
     }
 }
 
-template <int LOGB, int S0, int R>
+// one inverse pass over shared memory; FULL: the last one before the first
+// pass (which spans the whole block) ends with the CTA barrier, the others
+// with their team's
+template <int LOGB, int S0, int R, bool FULL>
 __device__ __forceinline__ void inv_pass_smem(const PassCtx& c) {
     constexpr int T = (1 << LOGB) / 16, G = 1 << R, NG = 16 / G, lb = LOGB - S0 - R;
+    static_assert(NG == 1 || lb == 0, "only the last pass holds several groups per thread");
     // groups one after another: keeps the 1024-thread variant within 64 registers
 #pragma unroll 1
     for (int g = 0; g < NG; g++) {
-        const int lbase = group_base<LOGB, S0, R>(g * T + c.t);
+        const int lbase = group_base<LOGB, S0, R>(NG == 1 ? c.t : adjacent_group<LOGB, R>(g, c.t));
         const int pbase = spad(lbase);
         uint64_t x[G];
 #pragma unroll
@@ -324,16 +376,19 @@ __device__ __forceinline__ void inv_pass_smem(const PassCtx& c) {
 #pragma unroll
         for (int k = 0; k < G; k++) c.sm[spad_off<lb>(pbase, lbase, k)] = x[k];
     }
-    __syncthreads();
+    if constexpr (FULL) __syncthreads();
+    else team_sync<LOGB>();
 }
 
 // inverse passes with S0 >= first, run from the last stages back to `first`
+// (the pass at `first` = R0 precedes the whole-block first pass)
 template <int LOGB, int RAD, int S0>
 __device__ __forceinline__ void inv_passes(const PassCtx& c) {
     if constexpr (S0 < LOGB) {
         constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
+        constexpr int R0 = RAD < LOGB ? RAD : LOGB;
         inv_passes<LOGB, RAD, S0 + R>(c);
-        inv_pass_smem<LOGB, S0, R>(c);
+        inv_pass_smem<LOGB, S0, R, S0 == R0>(c);
     }
 }
 
@@ -342,13 +397,13 @@ __device__ __forceinline__ void inv_passes(const PassCtx& c) {
 // the row in shared memory and one barrier less (4.7% faster inverse NTT at
 // N=2^14 than a coalesced load-in; the loads of adjacent points hit the same
 // cache lines).
-template <int LOGB, int S0, int R, class SRow>
+template <int LOGB, int S0, int R, class SRow, bool FULL>
 __device__ __forceinline__ void inv_pass_load(const PassCtx& c, const SRow& s) {
-    constexpr int T = (1 << LOGB) / 16, G = 1 << R, NG = 16 / G;
+    constexpr int G = 1 << R, NG = 16 / G;
     static_assert(LOGB - S0 - R == 0, "the loading pass holds the last stages");
 #pragma unroll 1
     for (int g = 0; g < NG; g++) {
-        const int lbase = (g * T + c.t) << R;
+        const int lbase = adjacent_group<LOGB, R>(g, c.t) << R;
         uint64_t x[G];
 #pragma unroll
         for (int k = 0; k < G; k++) x[k] = s.load(c.goff + lbase + k);
@@ -357,16 +412,18 @@ __device__ __forceinline__ void inv_pass_load(const PassCtx& c, const SRow& s) {
 #pragma unroll
         for (int k = 0; k < G; k++) c.sm[spad(lbase + k)] = x[k];
     }
-    __syncthreads();
+    if constexpr (FULL) __syncthreads();
+    else team_sync<LOGB>();
 }
 template <int LOGB, int RAD, int S0, class SRow>
 __device__ __forceinline__ void inv_passes_load(const PassCtx& c, const SRow& s) {
     constexpr int R = (LOGB - S0) < RAD ? (LOGB - S0) : RAD;
+    constexpr int R0 = RAD < LOGB ? RAD : LOGB;
     if constexpr (S0 + R < LOGB) {
         inv_passes_load<LOGB, RAD, S0 + R>(c, s);
-        inv_pass_smem<LOGB, S0, R>(c);
+        inv_pass_smem<LOGB, S0, R, S0 == R0>(c);
     } else {
-        inv_pass_load<LOGB, S0, R>(c, s);
+        inv_pass_load<LOGB, S0, R, SRow, S0 == R0>(c, s);
     }
 }
 
@@ -418,7 +475,7 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     const auto d = dst.bind(row);
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        const int j = t + k * T;
+        const int j = sweep_index<LOGB>(t, k);
         const uint64_t v = sm[spad(j)];
         d.store(c.goff + j, FULL ? reduce_from(v, q, 3) : v);
     }
@@ -447,10 +504,10 @@ ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
     } else {
 #pragma unroll
         for (int k = 0; k < 16; k++) {
-            const int j = t + k * T;
+            const int j = sweep_index<LOGB>(t, k);
             sm[spad(j)] = s.load(c.goff + j);
         }
-        __syncthreads();
+        team_sync<LOGB>();
         inv_passes<LOGB, RAD, R0>(c);
     }
     // pass 0 (local stages 0..R0-1), coalesced stores
