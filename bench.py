@@ -471,8 +471,9 @@ def run_ours(args, world, rank, local):
 def per_op_native():
     """The per-call forms timed from native code over the C ABI
     (kunpbfv_b200/perop_bench: no interpreter between calls): the fused one-pair
-    call, the plain one-kernel-per-building-block form and the batched call, 64
-    pairs, same parameters as the headline."""
+    call, the same call replayed from a captured plan, the plain
+    one-kernel-per-building-block form and the batched call, 64 pairs, same
+    parameters as the headline."""
     from kunpbfv_b200 import build as kb_build
     exe = kb_build.PEROP_BIN
     if not os.path.exists(exe):
@@ -482,7 +483,8 @@ def per_op_native():
     if r.returncode != 0 or not lines:
         return {"error": (r.stderr or r.stdout)[-300:]}
     d = json.loads(lines[-1])
-    d["form"] = ("C++ loop over the C ABI: fused = kbfv_mul_relin with count 1 per pair; plain = one kernel per "
+    d["form"] = ("C++ loop over the C ABI: fused = kbfv_mul_relin with count 1 per pair; plan = kbfv_plan_launch "
+                 "of a one-pair plan (fixed buffers, one CUDA graph launch per call); plain = one kernel per "
                  "building block (about 25 launches and 10 device copies per pair) then kbfv_relinearize; "
                  "batched = one kbfv_mul_relin of all pairs (no CUDA graph)")
     return d

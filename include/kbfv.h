@@ -463,6 +463,28 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
 int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                            uint64_t* d_out, uint32_t count, kbfv_stream stream);
 
+/* ---- captured multiplies -------------------------------------------------
+ * No counterpart in the reference. A plan binds a multiply (the same operation
+ * and product as kbfv_mul_relin) to fixed device buffers: `count` consecutive
+ * pairs at d_ct_a / d_ct_b, products to d_out. kbfv_plan_launch multiplies
+ * whatever the buffers hold at launch time. Its first launch runs the multiply
+ * eagerly on `stream` and records the same launch sequence into a CUDA graph
+ * (recording executes nothing); later launches replay that graph with one
+ * cudaGraphLaunch (one pair per call at N=16384: about 135 instead of 160 us,
+ * the ~14 kernel launches of the eager path issued as one). A launch after
+ * the context's scratch arena moved or its tuning knobs changed records the
+ * graph again (eagerly, as the first). Creating a plan sizes the context's
+ * arena for `count` pairs (kbfv_reserve). Plans of one context share that
+ * arena with every other call on the context, so their launches must be
+ * ordered with those calls (one stream, or events), as for kbfv_mul_relin. */
+typedef struct kbfv_plan kbfv_plan;
+int kbfv_plan_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
+                        uint64_t* d_out, uint32_t count, kbfv_plan** plan);
+int kbfv_plan_launch(kbfv_plan* plan, kbfv_stream stream);
+/* launches so far and how many of them recorded the graph */
+int kbfv_plan_info(const kbfv_plan* plan, uint64_t* launches, uint64_t* captures);
+int kbfv_plan_destroy(kbfv_plan* plan);
+
 /* invariant noise budget in bits of one ciphertext (host-side diagnostic, synchronous) */
 int kbfv_noise_budget(kbfv_context* ctx, const uint64_t* d_sk, const uint64_t* d_ct, double* bits);
 

@@ -20,6 +20,7 @@ from .api import (  # noqa: F401
     BFVScheme,
     Ciphertext,
     KbfvError,
+    MulPlan,
     Plaintext,
     SecretKey,
     Tensor3,
@@ -33,6 +34,7 @@ __all__ = [
     "BFVScheme",
     "Ciphertext",
     "KbfvError",
+    "MulPlan",
     "Plaintext",
     "SecretKey",
     "Tensor3",

@@ -133,6 +133,10 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_tune_get": (I, [VP, I, C.POINTER(C.c_int64)]),
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
+        "kbfv_plan_mul_relin": (I, [VP, VP, VP, VP, VP, u32, C.POINTER(VP)]),
+        "kbfv_plan_launch": (I, [VP, VP]),
+        "kbfv_plan_info": (I, [VP, C.POINTER(u64), C.POINTER(u64)]),
+        "kbfv_plan_destroy": (I, [VP]),
         "kbfv_mul_relin_host": (I, [VP, VP, VP, VP, VP, u32, u32, VP]),
         "kbfv_context_klss": (I, [VP, C.POINTER(u32), C.POINTER(u32), U64P]),
         "kbfv_params_create": (I, [u32, C.POINTER(u32), u32, C.POINTER(u32), u32, u64, u32,
@@ -557,6 +561,41 @@ class Tensor3:
         self.data = data if data is not None else ctx.zeros(count, 3, ctx.q_count, ctx.N)
 
 
+class MulPlan:
+    """kbfv_plan_*: a hybrid mult+relin bound to fixed device buffers, replayed
+    as one CUDA graph after its first launch. Keeps its buffers and key alive."""
+
+    def __init__(self, scheme: "BFVScheme", c1: Ciphertext, c2: Ciphertext, out: Ciphertext):
+        self._keep = (scheme, c1, c2, out)
+        self._ctx = scheme.context
+        h = VP()
+        _check(lib().kbfv_plan_mul_relin(c1.ctx.handle, _ptr(scheme.rlk), _ptr(c1.cipher_device),
+                                         _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count, C.byref(h)))
+        self._h = h
+        self.out = out
+
+    def launch(self, stream=None) -> Ciphertext:
+        _check(lib().kbfv_plan_launch(self._h, _stream_ptr(stream)))
+        return self.out
+
+    def info(self):
+        """(launches, captures) so far."""
+        n, k = C.c_uint64(), C.c_uint64()
+        _check(lib().kbfv_plan_info(self._h, C.byref(n), C.byref(k)))
+        return n.value, k.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().kbfv_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BFVScheme:
     """BFVScheme (include/BFVScheme.h:12-178) over one context."""
 
@@ -764,6 +803,18 @@ class BFVScheme:
             else:
                 torch.cuda.synchronize()
         return out
+
+    def mult_relin_plan(self, c1: Ciphertext, c2: Ciphertext, out: Ciphertext) -> "MulPlan":
+        """A captured multiply bound to these three buffers (kbfv_plan_mul_relin):
+        each ``launch()`` multiplies whatever c1 and c2 hold at that time into
+        ``out``; launches after the first replay one CUDA graph."""
+        if self.rlk is None:
+            raise KbfvError(-5, "rotKey_23 not exists")
+        if self.relin != "hybrid":
+            raise KbfvInvalidArgument(-1, "captured multiplies run the hybrid key switch only")
+        if not (c1.count == c2.count == out.count):
+            raise KbfvInvalidArgument(-1, "c1, c2 and out must hold as many ciphertexts")
+        return MulPlan(self, c1, c2, out)
 
     def mult_relin_ptrs(self, a_ptrs, b_ptrs, out_ptrs, stream=None):
         n = len(a_ptrs)

@@ -17,7 +17,7 @@ PEROP_BIN = os.path.join(HERE, "perop_bench")
 OBJDIR = os.path.join(HERE, "_build")
 # translation units of libkbfv.so (compiled in parallel)
 SOURCES = [os.path.join(HERE, "csrc", f) for f in
-           ("k5_m8.cu", "k5_m16.cu", "k5_m24.cu", "k5_m33.cu", "mul.cu", "levels.cu", "scheme.cu", "ntt_ops.cu", "klss_api.cu", "context.cu", "serve.cpp")]
+           ("k5_m8.cu", "k5_m16.cu", "k5_m24.cu", "k5_m33.cu", "mul.cu", "levels.cu", "scheme.cu", "ntt_ops.cu", "klss_api.cu", "context.cu", "plan.cu", "serve.cpp")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))
            if f.endswith((".cuh", ".hpp", ".h"))] + [
     os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]

@@ -5,11 +5,13 @@
 //
 // N = 16384, 7 x 60-bit ciphertext primes + 1 special prime, t = 65537, dnum 1.
 // Prints one JSON line with, per pair: the fused one-pair call (kbfv_mul_relin,
-// count 1), the plain form (one kernel per building block: INTT, Q -> R, NTT,
-// copies into the Q|R layout, tensor, six INTTs, scale-and-round, R -> Q, NTT,
-// then kbfv_relinearize), and the batched call over all pairs. Each form runs
-// `reps` timed rounds after one warm-up round (CUDA events on one stream), and
-// the plain form's product of the first pair is compared with the fused one's.
+// count 1), the same call replayed from a captured plan (kbfv_plan_launch of a
+// one-pair plan bound to fixed buffers), the plain form (one kernel per
+// building block: INTT, Q -> R, NTT, copies into the Q|R layout, tensor, six
+// INTTs, scale-and-round, R -> Q, NTT, then kbfv_relinearize), and the batched
+// call over all pairs. Each form runs `reps` timed rounds after one warm-up
+// round (CUDA events on one stream); the plan's and the plain form's products
+// of the first pair are compared with the fused one's.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -109,6 +111,20 @@ int main(int argc, char** argv) {
     cu(cudaStreamSynchronize(st), "sync");
     cu(cudaMemcpy(want.data(), o, ctw * 8, cudaMemcpyDeviceToHost), "copy product");
 
+    // captured plan: one pair bound to fixed buffers (pair 0), replayed per call
+    uint64_t* po1 = dalloc(ctw);
+    kbfv_plan* plan = nullptr;
+    ok(kbfv_plan_mul_relin(ctx, rlk, a, b, po1, 1, &plan), "plan");
+    const double plan_ms = timed([&] {
+        for (int i = 0; i < pairs; i++) ok(kbfv_plan_launch(plan, S), "plan launch");
+    });
+    cu(cudaStreamSynchronize(st), "sync");
+    cu(cudaMemcpy(got.data(), po1, ctw * 8, cudaMemcpyDeviceToHost), "copy product");
+    const bool plan_matches = std::memcmp(got.data(), want.data(), ctw * 8) == 0;
+    uint64_t plan_launches = 0, plan_captures = 0;
+    ok(kbfv_plan_info(plan, &plan_launches, &plan_captures), "plan info");
+    ok(kbfv_plan_destroy(plan), "plan destroy");
+
     // plain: one kernel per building block
     uint64_t* x4 = dalloc(4 * nq * N);
     uint64_t* r4 = dalloc(4 * nr * N);
@@ -156,12 +172,16 @@ int main(int argc, char** argv) {
     const double batch_ms = timed([&] { ok(kbfv_mul_relin(ctx, rlk, a, b, o, pairs, S), "mul_relin batch"); });
 
     std::printf("{\"pairs\": %d, \"reps\": %d, \"fused_per_call_ms_per_pair\": %.5f, "
+                "\"plan_per_call_ms_per_pair\": %.5f, "
                 "\"plain_per_op_ms_per_pair\": %.5f, \"batched_ms_per_call\": %.5f, "
-                "\"fused_per_call_ct_per_s\": %.1f, \"plain_per_op_ct_per_s\": %.1f, \"batched_ct_per_s\": %.1f, "
-                "\"plain_matches_fused\": %s}\n",
-                pairs, reps, fused_ms / pairs, plain_ms / pairs, batch_ms, pairs / fused_ms * 1e3,
-                pairs / plain_ms * 1e3, pairs / batch_ms * 1e3, plain_matches ? "true" : "false");
-    for (uint64_t* p : {sk, pk, rlk, d_slots, d_m, a, b, o, x4, r4, qr, tz, sr, d3, po}) cudaFree(p);
+                "\"fused_per_call_ct_per_s\": %.1f, \"plan_per_call_ct_per_s\": %.1f, "
+                "\"plain_per_op_ct_per_s\": %.1f, \"batched_ct_per_s\": %.1f, "
+                "\"plain_matches_fused\": %s, \"plan_matches_fused\": %s, \"plan_captures\": %llu}\n",
+                pairs, reps, fused_ms / pairs, plan_ms / pairs, plain_ms / pairs, batch_ms, pairs / fused_ms * 1e3,
+                pairs / plan_ms * 1e3, pairs / plain_ms * 1e3, pairs / batch_ms * 1e3,
+                plain_matches ? "true" : "false", plan_matches ? "true" : "false",
+                (unsigned long long)plan_captures);
+    for (uint64_t* p : {sk, pk, rlk, d_slots, d_m, a, b, o, x4, r4, qr, tz, sr, d3, po, po1}) cudaFree(p);
     kbfv_context_destroy(ctx);
-    return plain_matches ? 0 : 1;
+    return plain_matches && plan_matches ? 0 : 1;
 }

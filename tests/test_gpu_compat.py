@@ -81,13 +81,15 @@ def test_reference_demo_unmodified():
 
 def test_native_per_call_forms():
     """kunpbfv_b200/perop_bench (C++ over the C ABI): the plain one-kernel-per-
-    building-block multiply gives the fused pipeline's product, and every form
-    reports a positive rate."""
+    building-block multiply and the replayed one-pair plan give the fused
+    pipeline's product, and every form reports a positive rate."""
     import json
     from kunpbfv_b200 import build as kb_build
     exe = kb_build.build_perop()
     r = subprocess.run([exe, "4", "1"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
-    assert d["plain_matches_fused"] is True
+    assert d["plain_matches_fused"] is True and d["plan_matches_fused"] is True
+    assert d["plan_captures"] == 1
     assert d["fused_per_call_ct_per_s"] > 0 and d["plain_per_op_ct_per_s"] > 0 and d["batched_ct_per_s"] > 0
+    assert d["plan_per_call_ct_per_s"] > 0
