@@ -87,6 +87,13 @@ static inline int resident_ctas(const void* kernel, int threads, int smem) {
     return sms * std::max(per, 1);
 }
 
+// the same for launch shapes chosen at run time: cached per CTA size (64..512)
+static inline int resident_ctas_at(const void* kernel, int threads, int smem, int (&cache)[4]) {
+    const int i = std::min(3, std::max(0, __builtin_ctz((unsigned)threads) - 6));
+    if (!cache[i]) cache[i] = resident_ctas(kernel, threads, smem);
+    return cache[i];
+}
+
 template <int LOGB, class Src, class Dst, bool FULL = true>
 static void launch_fwd_block(const DevConsts& dc, Src s, Dst d, int rows, int logn, cudaStream_t st) {
     constexpr int SMEM = BlockShape<LOGB>::SMEM_BYTES;

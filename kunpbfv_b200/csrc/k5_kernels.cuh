@@ -60,7 +60,9 @@ static __global__ void k5_round_kernel(DevConsts c, const uint64_t* __restrict__
 // K5, in two kernels so that each holds fewer registers (more warps per SM):
 // K5a: t/Q scale-and-round Q|R -> R of each tensor polynomial into rr ([poly][nr]).
 template <int MAXQ>
-static __global__ void k5_scale_kernel(DevConsts c, const uint64_t* __restrict__ sc, uint64_t* __restrict__ rr_out) {
+static __global__ void k5_scale_kernel(DevConsts c, const uint64_t* __restrict__ sc, uint64_t* __restrict__ rr_out,
+                                       int ahead) {
+    prefetch_chunk_ahead(sc, (size_t)c.nqr << c.logn, c.nqr, c.logn, blockDim.x, ahead);
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int poly = blockIdx.y;
     const uint64_t* src = sc + ((size_t)poly * c.nqr << c.logn);
@@ -84,7 +86,8 @@ static __global__ void k5_scale_kernel(DevConsts c, const uint64_t* __restrict__
 // mode 2: a1*a2 over Q into sd2 ([item][nq]); cross, b1*b2 to sd (T-base key switch).
 template <int MAXQ>
 static __global__ void k5_lift_kernel(DevConsts c, const uint64_t* __restrict__ rr_in, uint64_t* __restrict__ out0,
-                               uint64_t* __restrict__ sd, uint64_t* __restrict__ sd2, int mode) {
+                               uint64_t* __restrict__ sd, uint64_t* __restrict__ sd2, int mode, int ahead) {
+    prefetch_chunk_ahead(rr_in, (size_t)c.nr << c.logn, c.nr, c.logn, blockDim.x, ahead);
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int poly = blockIdx.y, item = poly / 3, which = poly % 3;
     const uint64_t* src = rr_in + ((size_t)poly * c.nr << c.logn);
@@ -130,8 +133,11 @@ void k5_launch_m(const DevConsts& dc, int count, const MulScratch& m, uint64_t* 
     if (count <= dc.shape.k5_fused_pairs) {
         k5_round_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sc, out0, m.sd, m.sd2, mode);
     } else {
-        k5_scale_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sc, m.sb);
-        k5_lift_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sb, out0, m.sd, m.sd2, mode);
+        static int res_scale[4] = {0, 0, 0, 0}, res_lift[4] = {0, 0, 0, 0};
+        const int a = dc.shape.l2_prefetch ? resident_ctas_at((const void*)k5_scale_kernel<MAXQ>, threads, 0, res_scale) : 0;
+        const int b = dc.shape.l2_prefetch ? resident_ctas_at((const void*)k5_lift_kernel<MAXQ>, threads, 0, res_lift) : 0;
+        k5_scale_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sc, m.sb, a);
+        k5_lift_kernel<MAXQ><<<grid, threads, 0, st>>>(dc, m.sb, out0, m.sd, m.sd2, mode, b);
     }
     check_launch("k5_round");
 }

@@ -14,6 +14,20 @@ namespace kbfv {
 // HPS base extension (BaseConverter::bConv_HPS, include/BasisConv_QR.cuh:191-207;
 // include/poly_arithmetic.cuh:1078-1178): centred lift of x mod B into O.
 // ===========================================================================
+// Per-coefficient kernels over a 2-D grid (x: chunks of `chunk` coefficients,
+// y: polynomials of `nrows` limbs, `poly_stride` words apart): threads
+// 0 .. nrows-1 ask L2 for their limb's chunk of the CTA `ahead` places later in
+// launch order (ahead = CTAs resident at once; 0: none), so that CTA's loads
+// hit L2 instead of waiting on HBM.
+__device__ __forceinline__ void prefetch_chunk_ahead(const uint64_t* in, size_t poly_stride, int nrows, int logn,
+                                                     int chunk, int ahead) {
+    if (ahead <= 0 || (int)threadIdx.x >= nrows) return;
+    const unsigned lin = blockIdx.y * gridDim.x + blockIdx.x + (unsigned)ahead;
+    if (lin >= gridDim.x * gridDim.y) return;
+    const unsigned bx = lin % gridDim.x, by = lin / gridDim.x;
+    l2_prefetch(in + by * poly_stride + ((size_t)threadIdx.x << logn) + (size_t)bx * chunk, (uint32_t)chunk * 8);
+}
+
 template <int MAXIN>
 __device__ __forceinline__ long long bconv_prep(uint64_t* y, const uint64_t* x, int nin,
                                                 const uint64_t* __restrict__ in_mods,
@@ -66,8 +80,9 @@ __host__ __device__ inline BconvTables r2q_tables(const DevConsts& c) {
 // one thread per coefficient; grid.y = polynomial
 template <int MAXIN>
 static __global__ void bconv_kernel(BconvTables tb, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
-                             int logn, size_t in_stride, size_t out_stride) {
+                             int logn, size_t in_stride, size_t out_stride, int ahead) {
     extern __shared__ uint64_t sh_hat[];
+    prefetch_chunk_ahead(in, in_stride, tb.nin, logn, blockDim.x, ahead);
     for (int i = threadIdx.x; i < tb.nin * tb.nout; i += blockDim.x) sh_hat[i] = tb.hat[i];
     __syncthreads();
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,8 +105,9 @@ static __global__ void bconv_kernel(BconvTables tb, const uint64_t* __restrict__
 // independent. Per coefficient the arithmetic is bconv_kernel's.
 template <int MAXIN>
 static __global__ void bconv2_kernel(BconvTables tb, const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
-                                     int logn, size_t in_stride, size_t out_stride) {
+                                     int logn, size_t in_stride, size_t out_stride, int ahead) {
     extern __shared__ uint64_t sh_hat[];
+    prefetch_chunk_ahead(in, in_stride, tb.nin, logn, 2 * blockDim.x, ahead);
     for (int i = threadIdx.x; i < tb.nin * tb.nout; i += blockDim.x) sh_hat[i] = tb.hat[i];
     __syncthreads();
     const size_t k = 2 * ((size_t)blockIdx.x * blockDim.x + threadIdx.x);

@@ -48,10 +48,16 @@ void launch_bconv(const DevConsts& dc, const BconvTables& tb, const uint64_t* in
     const int threads = dc.shape.bconv_threads, cpt = dc.shape.bconv_cpt;
     dim3 grid((unsigned)((1u << dc.logn) / (threads * cpt)), (unsigned)polys);
     const size_t sh = (size_t)tb.nin * tb.nout * 8;
-#define L_BC(M)                                                                                        \
-    do {                                                                                               \
-        if (cpt == 2) bconv2_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride); \
-        else bconv_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride);  \
+#define L_BC(M)                                                                                            \
+    do {                                                                                                   \
+        static int res1[4] = {0, 0, 0, 0}, res2[4] = {0, 0, 0, 0};                                         \
+        if (cpt == 2) {                                                                                    \
+            const int a = dc.shape.l2_prefetch ? resident_ctas_at((const void*)bconv2_kernel<M>, threads, (int)sh, res2) : 0; \
+            bconv2_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride, a);   \
+        } else {                                                                                           \
+            const int a = dc.shape.l2_prefetch ? resident_ctas_at((const void*)bconv_kernel<M>, threads, (int)sh, res1) : 0; \
+            bconv_kernel<M><<<grid, threads, sh, st>>>(tb, in, out, dc.logn, in_stride, out_stride, a);    \
+        }                                                                                                  \
     } while (0)
     DISPATCH_MAXQ(tb.nin, L_BC);
 #undef L_BC
