@@ -295,7 +295,7 @@ def run_reference(args, world, rank):
                    "batch_pairs_per_step": cpu.pairs_per_step, "parallelism": f"{cpu.cores} host threads"},
         "steps_requested": args.steps,
         "cpu_baseline": {"value": round(v, 3), "unit": "ct/s", "cores": cpu.cores, "kind": "port",
-                         "sample": cpu.describe(per_step, steps)},
+                         "sample": cpu.describe(per_step, steps), "seal": seal_on_host()},
         "e2e": {"value": round(v, 3), "unit": "ct/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if steps < args.steps:
@@ -343,6 +343,19 @@ def reference_gpu_timing(reps: int = 20):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+SEAL_GLOBS = ("/usr/local/include/SEAL-4.*", "/usr/include/SEAL-4.*", "/usr/local/lib/libseal*",
+              "/usr/local/lib64/libseal*", "/usr/lib/libseal*", "/usr/lib/x86_64-linux-gnu/libseal*")
+
+
+def seal_on_host():
+    """Microsoft SEAL 4.x, the CPU BFV library the baseline would use if this
+    host had it: the paths found (none on these hosts, so the C oracle on all
+    host cores is the CPU baseline)."""
+    import glob
+    found = sorted(p for g in SEAL_GLOBS for p in glob.glob(g))
+    return {"installed": bool(found), "checked": list(SEAL_GLOBS), "found": found[:4]}
+
+
 def cpu_baseline_sample(seconds=12.0):
     """The CPU oracle on the host cores, by the reference arm's method, over a
     bounded sample (about `seconds` of timed steps)."""
@@ -351,7 +364,7 @@ def cpu_baseline_sample(seconds=12.0):
     per_step, steps = cpu.run(max(3, int(seconds / max(est, 1e-3))), 0, budget_s=seconds)
     cpu.close()
     return {"value": round(cpu.pairs_per_step / per_step, 3), "unit": "ct/s", "cores": cpu.cores, "kind": "port",
-            "sample": cpu.describe(per_step, steps)}
+            "sample": cpu.describe(per_step, steps), "seal": seal_on_host()}
 
 
 def run_ours(args, world, rank, local):
