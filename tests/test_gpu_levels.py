@@ -243,3 +243,33 @@ def test_mixed_levels_span_several_launch_sequences():
         assert o.ctx.q_count == levels[j]
         alone = sch.mult_relin(a, b)
         assert np.array_equal(host(alone.cipher_device), host(o.cipher_device)), (j, levels[j])
+
+
+@pytest.mark.parametrize("log_n,q_bits,p_bits,dnum,t,levels", [
+    (14, [60] * 7, [60], 1, 65537, [7, 6, 5, 4, 7, 6, 5, 4]),   # 2^14 whole-row block kernels (rows > 48)
+    (14, [60] * 7, [60], 1, 65537, [7, 4]),                     # 2^14 column pass + 2^12-point blocks
+    (13, [50] * 5, [52], 5, 65537, [5, 3, 4, 2, 1, 5]),         # 2^13 blocks, one-prime digits
+    (16, [60] * 6, [60], 2, 786433, [6, 4, 5, 3]),              # 2^16 column pass + 2^12-point blocks
+])
+def test_mixed_levels_on_other_rings(log_n, q_bits, p_bits, dnum, t, levels):
+    """One launch sequence over pairs at mixed levels on the block shapes the
+    other level tests do not reach: every product equals the pair multiplied
+    alone at its level (itself pinned to the oracle per level)."""
+    import kunpbfv_b200 as kb
+    ctx = kb.BFVContext.from_bits(log_n, q_bits, p_bits, t, dnum=dnum)
+    sk = kb.SecretKey(ctx, SEED)
+    sch = kb.BFVScheme(ctx, SEED)
+    sch.addEncKey(sk)
+    sch.addMultKey_23(sk)
+    rng = np.random.default_rng(log_n + len(levels))
+    pairs = []
+    for j, live in enumerate(levels):
+        v = rng.integers(0, t, size=(2, ctx.N), dtype=np.uint64)
+        a = sch.mod_switch_to(sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v[0]))), enc_id=700 + 2 * j), live)
+        b = sch.mod_switch_to(sch.encryptMsg(kb.Plaintext(ctx, ctx.encode(dev(v[1]))), enc_id=701 + 2 * j), live)
+        pairs.append((a, b))
+    outs = sch.mult_relin_levels(pairs)
+    for j, ((a, b), o) in enumerate(zip(pairs, outs)):
+        assert o.ctx.q_count == levels[j]
+        alone = sch.mult_relin(a, b)
+        assert np.array_equal(host(alone.cipher_device), host(o.cipher_device)), (j, levels[j])
