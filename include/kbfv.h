@@ -378,8 +378,10 @@ int kbfv_mod_switch(kbfv_context* ctx_level, const uint64_t* d_ct, uint64_t* d_o
                     kbfv_stream stream);
 /* Multiply + relinearise a batch whose pairs sit at different levels: pair i has
  * live_q[i] live primes (both inputs and the output at that level). One call on
- * one stream: pairs are grouped by level and each group runs as one batched
- * launch sequence of that level's context. d_rlk is the top-level key. */
+ * one stream: up to 128 pairs in up to 8 levels run as ONE launch sequence of
+ * the multiply pipeline (every kernel takes its items' level constants from a
+ * per-level table; the top-level key is read through a limb map), larger
+ * batches as several. d_rlk is the top-level key. */
 int kbfv_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32_t* live_q,
                           const uint64_t* const* ct_a, const uint64_t* const* ct_b, uint64_t* const* out,
                           uint32_t count, kbfv_stream stream);
@@ -481,6 +483,12 @@ typedef struct kbfv_plan kbfv_plan;
 int kbfv_plan_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                         uint64_t* d_out, uint32_t count, kbfv_plan** plan);
 int kbfv_plan_launch(kbfv_plan* plan, kbfv_stream stream);
+/* The same for a batch at mixed levels (kbfv_mul_relin_levels' arguments; the
+ * arrays are copied, the buffers they point to are bound): each launch replays
+ * the whole uneven batch as one CUDA graph launch. */
+int kbfv_plan_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32_t* live_q,
+                               const uint64_t* const* ct_a, const uint64_t* const* ct_b, uint64_t* const* out,
+                               uint32_t count, kbfv_plan** plan);
 /* launches so far and how many of them recorded the graph */
 int kbfv_plan_info(const kbfv_plan* plan, uint64_t* launches, uint64_t* captures);
 int kbfv_plan_destroy(kbfv_plan* plan);

@@ -134,6 +134,8 @@ def _declare(L: C.CDLL) -> None:
         "kbfv_mul_relin": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_mul_relin_noalloc": (I, [VP, VP, VP, VP, VP, u32, VP]),
         "kbfv_plan_mul_relin": (I, [VP, VP, VP, VP, VP, u32, C.POINTER(VP)]),
+        "kbfv_plan_mul_relin_levels": (I, [VP, VP, C.POINTER(u32), C.POINTER(VP), C.POINTER(VP), C.POINTER(VP), u32,
+                                           C.POINTER(VP)]),
         "kbfv_plan_launch": (I, [VP, VP]),
         "kbfv_plan_info": (I, [VP, C.POINTER(u64), C.POINTER(u64)]),
         "kbfv_plan_destroy": (I, [VP]),
@@ -563,14 +565,25 @@ class Tensor3:
 
 class MulPlan:
     """kbfv_plan_*: a hybrid mult+relin bound to fixed device buffers, replayed
-    as one CUDA graph after its first launch. Keeps its buffers and key alive."""
+    as one CUDA graph after its first launch. Keeps its buffers and key alive.
+    With `pairs` (a list of (ct_a, ct_b) at possibly different levels) and
+    `outs`, the plan is the mixed-level multiply (kbfv_plan_mul_relin_levels)."""
 
-    def __init__(self, scheme: "BFVScheme", c1: Ciphertext, c2: Ciphertext, out: Ciphertext):
-        self._keep = (scheme, c1, c2, out)
+    def __init__(self, scheme: "BFVScheme", c1: Ciphertext = None, c2: Ciphertext = None, out=None, pairs=None):
+        self._keep = (scheme, c1, c2, out, pairs)
         self._ctx = scheme.context
         h = VP()
-        _check(lib().kbfv_plan_mul_relin(c1.ctx.handle, _ptr(scheme.rlk), _ptr(c1.cipher_device),
-                                         _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count, C.byref(h)))
+        if pairs is None:
+            _check(lib().kbfv_plan_mul_relin(c1.ctx.handle, _ptr(scheme.rlk), _ptr(c1.cipher_device),
+                                             _ptr(c2.cipher_device), _ptr(out.cipher_device), c1.count, C.byref(h)))
+        else:
+            n = len(pairs)
+            lv = (C.c_uint32 * n)(*[a.ctx.q_count for a, _ in pairs])
+            A = (VP * n)(*[_ptr(a.cipher_device) for a, _ in pairs])
+            B = (VP * n)(*[_ptr(b.cipher_device) for _, b in pairs])
+            O = (VP * n)(*[_ptr(o.cipher_device) for o in out])
+            _check(lib().kbfv_plan_mul_relin_levels(scheme.context.handle, _ptr(scheme.rlk), lv, A, B, O, n,
+                                                    C.byref(h)))
         self._h = h
         self.out = out
 
@@ -815,6 +828,16 @@ class BFVScheme:
         if not (c1.count == c2.count == out.count):
             raise KbfvInvalidArgument(-1, "c1, c2 and out must hold as many ciphertexts")
         return MulPlan(self, c1, c2, out)
+
+    def mult_relin_levels_plan(self, pairs, outs) -> "MulPlan":
+        """A captured mixed-level multiply (kbfv_plan_mul_relin_levels): each
+        ``launch()`` multiplies the pairs' current contents into ``outs`` (each
+        at its pair's level) with one CUDA graph launch after the first."""
+        if self.rlk is None:
+            raise KbfvError(-5, "rotKey_23 not exists")
+        if len(outs) != len(pairs):
+            raise KbfvInvalidArgument(-1, "one output per pair")
+        return MulPlan(self, out=outs, pairs=pairs)
 
     def mult_relin_ptrs(self, a_ptrs, b_ptrs, out_ptrs, stream=None):
         n = len(a_ptrs)

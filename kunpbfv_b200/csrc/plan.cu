@@ -1,7 +1,11 @@
 // Captured multiplies (kbfv_plan_*): a caller that multiplies the same device
 // buffers again and again (a request loop with fixed staging buffers) replays
 // the whole multiply as one CUDA graph launch instead of issuing its ~14
-// kernel launches one by one. No counterpart in the reference.
+// kernel launches one by one; a batch of pairs at mixed levels
+// (kbfv_mul_relin_levels) likewise becomes one graph launch. No counterpart in
+// the reference.
+#include <vector>
+
 #include "pipeline.cuh"
 
 struct kbfv_plan {
@@ -11,6 +15,11 @@ struct kbfv_plan {
     const uint64_t* b = nullptr;
     uint64_t* out = nullptr;
     uint32_t count = 0;
+    // mixed levels: pair i at live_q[i] live primes, its own pointers
+    bool levels = false;
+    std::vector<uint32_t> live_q;
+    std::vector<const uint64_t*> va, vb;
+    std::vector<uint64_t*> vo;
     cudaStream_t cs = nullptr;  // the stream the graph is captured on
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -40,13 +49,20 @@ bool graph_current(const kbfv_plan& p) {
 // kernel attributes and scratch growth happens here, outside any capture),
 // then records the same launch sequence on the plan's own stream into a graph.
 // Capturing executes nothing.
+int run_once(kbfv_plan& p, cudaStream_t st) {
+    if (p.levels)
+        return kbfv_mul_relin_levels(p.ctx, p.rlk, p.live_q.data(), p.va.data(), p.vb.data(), p.vo.data(), p.count,
+                                     (kbfv_stream)st);
+    return kbfv_mul_relin(p.ctx, p.rlk, p.a, p.b, p.out, p.count, (kbfv_stream)st);
+}
+
 void run_and_capture(kbfv_plan& p, cudaStream_t st) {
-    int rc = kbfv_mul_relin(p.ctx, p.rlk, p.a, p.b, p.out, p.count, (kbfv_stream)st);
+    int rc = run_once(p, st);
     if (rc != KBFV_OK) throw KbfvError(rc, g_last_error);
     drop_graph(p);
     if (!p.cs) KB_CHECK_CUDA(cudaStreamCreateWithFlags(&p.cs, cudaStreamNonBlocking));
     KB_CHECK_CUDA(cudaStreamBeginCapture(p.cs, cudaStreamCaptureModeThreadLocal));
-    rc = kbfv_mul_relin(p.ctx, p.rlk, p.a, p.b, p.out, p.count, (kbfv_stream)p.cs);
+    rc = run_once(p, p.cs);
     const std::string err = rc == KBFV_OK ? std::string() : g_last_error;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(p.cs, &g);  // ends the capture on every path
@@ -88,6 +104,36 @@ int kbfv_plan_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t
         p->out = d_out;
         p->count = count;
         *out = p;
+    });
+}
+
+int kbfv_plan_mul_relin_levels(kbfv_context* ctx, const uint64_t* d_rlk, const uint32_t* live_q,
+                               const uint64_t* const* ct_a, const uint64_t* const* ct_b, uint64_t* const* out,
+                               uint32_t count, kbfv_plan** plan) {
+    return guarded([&] {
+        Context& c = CX(ctx);
+        require_batchable(c);
+        KB_REQUIRE(!c.parent, KBFV_ERR_INVALID, "call on the top-level context");
+        KB_REQUIRE(plan, KBFV_ERR_INVALID, "null argument");
+        KB_REQUIRE(d_rlk, KBFV_ERR_NO_KEY, "relinearisation key missing");
+        KB_REQUIRE(live_q && ct_a && ct_b && out, KBFV_ERR_INVALID, "null pointer array");
+        KB_REQUIRE(count >= 1, KBFV_ERR_INVALID, "a plan multiplies at least one pair");
+        for (uint32_t i = 0; i < count; i++) {
+            KB_REQUIRE(live_q[i] >= 1 && live_q[i] <= (uint32_t)c.nq, KBFV_ERR_LEVEL, "live prime count out of range");
+            KB_REQUIRE(ct_a[i] && ct_b[i] && out[i], KBFV_ERR_INVALID, "null ciphertext pointer");
+        }
+        // the mixed batch uses the top level's per-pair scratch layout
+        ensure_scratch(c, mul_scratch_need(c, (int)std::min<uint32_t>(count, kMaxBatch)));
+        auto* p = new kbfv_plan();
+        p->ctx = ctx;
+        p->rlk = d_rlk;
+        p->count = count;
+        p->levels = true;
+        p->live_q.assign(live_q, live_q + count);
+        p->va.assign(ct_a, ct_a + count);
+        p->vb.assign(ct_b, ct_b + count);
+        p->vo.assign(out, out + count);
+        *plan = p;
     });
 }
 

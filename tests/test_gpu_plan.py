@@ -93,3 +93,38 @@ def test_plan_rejects_bad_arguments():
                                     _ptr(a.cipher_device), 1, C.byref(h)) != 0
     assert lib().kbfv_plan_launch(None, None) != 0
     assert lib().kbfv_plan_destroy(None) == 0
+
+
+def test_levels_plan_replays_the_mixed_batch():
+    """A plan over pairs at four levels (kbfv_plan_mul_relin_levels): every
+    launch equals kbfv_mul_relin_levels on the buffers' current contents."""
+    import torch
+
+    import kunpbfv_b200 as kb
+    from kunpbfv_b200 import tune
+    ctx = kb.BFVContext.from_bits(14, [60] * 7, [60], 65537, dnum=1)
+    sk = kb.SecretKey(ctx, b"\x63" * 32)
+    sch = kb.BFVScheme(ctx, b"\x64" * 32)
+    sch.addMultKey_23(sk)
+    pairs, outs = [], []
+    for j in range(10):
+        lv = ctx.at_level(7 - j % 4)
+        pairs.append((kb.Ciphertext(lv, tune._random_pairs(lv, 1, 30 + j)),
+                      kb.Ciphertext(lv, tune._random_pairs(lv, 1, 60 + j))))
+        outs.append(kb.Ciphertext(lv, count=1))
+    plan = sch.mult_relin_levels_plan(pairs, outs)
+    try:
+        for rnd in range(3):
+            if rnd:
+                for j, (a, b) in enumerate(pairs):
+                    a.cipher_device.copy_(tune._random_pairs(a.ctx, 1, 100 * rnd + j).view_as(a.cipher_device))
+            plan.launch()
+            torch.cuda.synchronize()
+            got = [o.cipher_device.clone() for o in outs]
+            want = sch.mult_relin_levels(pairs)
+            torch.cuda.synchronize()
+            for j, (g, w) in enumerate(zip(got, want)):
+                assert torch.equal(g, w.cipher_device), (rnd, j)
+        assert plan.info() == (3, 1)
+    finally:
+        plan.close()
