@@ -287,10 +287,13 @@ typedef enum {
                                     scaled by (Q/q_i)^-1, and there is no base-conversion launch
                                     and no HBM round trip of the R limbs; each R row then reads
                                     all q_count Q limbs, which larger batches pay for in L2 traffic */
-    KBFV_TUNE_L2_PREFETCH = 9    /* 0 or 1 (default): NTT block kernels whose input is plain rows
+    KBFV_TUNE_L2_PREFETCH = 9,   /* 0 or 1 (default): NTT block kernels whose input is plain rows
                                     (standalone transforms, the multiply's INTT of its inputs and
                                     its NTTs over R and Q|P) ask L2 for the block one wave of CTAs
                                     ahead of their own */
+    KBFV_TUNE_SPLIT_ROWS_ALONE = 10 /* 0..2^20 (default 148): KBFV_TUNE_SPLIT_ROWS for a multiply
+                                    that runs as one stream (batches too small for sub-batches,
+                                    kbfv_mul), where no sibling sub-batch fills idle SMs */
 } kbfv_tune_knob;
 int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value);
 int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value);

@@ -39,7 +39,8 @@ _ERR_NAMES = {
 # kbfv_tune_knob (include/kbfv.h)
 TUNE_KNOBS = {"ntt_block_log": 0, "branches": 1, "host_chunk": 2, "split_rows": 3, "bconv_threads": 4,
               "k5_threads": 5, "k5_fused_pairs": 6, "bconv_cpt": 7,
-              "fuse_q2r_pairs": 8, "l2_prefetch": 9}
+              "fuse_q2r_pairs": 8, "l2_prefetch": 9,
+              "split_rows_alone": 10}
 
 
 class KbfvError(RuntimeError):

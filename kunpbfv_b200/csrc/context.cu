@@ -141,7 +141,7 @@ void build_context(Context& c, const kbfv_params& prm) {
     DevConsts& dc = c.dc;
     // two coefficients per base-conversion thread: 16% fewer IMAD instructions,
     // 8% faster than one at N=16384, 7 + 1 primes, 32-pair sub-batches (B200)
-    dc.shape = LaunchShape{kSplitRows14Default, 256, 2, 128, 2, 1, 1};
+    dc.shape = LaunchShape{kSplitRows14Default, 256, 2, 128, 2, 1, 1, kSplitRowsAloneDefault};
     dc.logn = c.logn; dc.nq = c.nq; dc.np = c.np; dc.nr = c.nr; dc.nt = c.nt;
     dc.dnum = c.dnum; dc.alpha = c.alpha; dc.npq = c.nq + c.np; dc.nqr = c.nq + c.nr;
     dc.idx_p = c.nq; dc.idx_r = c.nq + c.np; dc.idx_t = c.nq + c.np + c.nr; dc.idx_pt = nall - 1;
@@ -714,6 +714,10 @@ int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
                 KB_REQUIRE(value == 0 || value == 1, KBFV_ERR_INVALID, "L2 prefetch: 0 or 1");
                 c.dc.shape.l2_prefetch = (int)value;
                 break;
+            case KBFV_TUNE_SPLIT_ROWS_ALONE:
+                KB_REQUIRE(value >= 0 && value <= (1 << 20), KBFV_ERR_INVALID, "split rows (one stream) must be 0..2^20");
+                c.dc.shape.split_rows_alone = (int)value;
+                break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
         // the levels of a top context run with the top level's knobs
@@ -741,6 +745,7 @@ int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value) {
             case KBFV_TUNE_BCONV_CPT: *value = c.dc.shape.bconv_cpt; break;
             case KBFV_TUNE_FUSE_Q2R_PAIRS: *value = c.dc.shape.fuse_q2r_pairs; break;
             case KBFV_TUNE_L2_PREFETCH: *value = c.dc.shape.l2_prefetch; break;
+            case KBFV_TUNE_SPLIT_ROWS_ALONE: *value = c.dc.shape.split_rows_alone; break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
     });

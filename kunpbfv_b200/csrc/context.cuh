@@ -26,6 +26,7 @@ struct LaunchShape {
     int fuse_q2r_pairs;  // batches of at most this many pairs run the Q -> R base extension in the
                          // loader of the NTT over R (no K2 launch)
     int l2_prefetch;     // 1: block kernels ask L2 for the block one wave of CTAs ahead
+    int split_rows_alone;  // split_rows14 for a multiply that runs as one stream
 };
 
 // Everything a kernel needs, passed by value (all pointers into one device pool).

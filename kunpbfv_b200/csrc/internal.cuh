@@ -142,6 +142,12 @@ static inline Dst plain_of(const Dst& d) { return d; }
 // batched multiply ~1%, so 64-row launches keep the whole-ring blocks. The
 // default of LaunchShape::split_rows14 (KBFV_TUNE_SPLIT_ROWS).
 constexpr int kSplitRows14Default = 48;
+// The same threshold for a multiply that runs as one stream (batches below two
+// sub-batches, the tensor-only multiply): launches of up to 148 rows would
+// leave SMs idle with one 1024-thread CTA per row, and no sibling sub-batch
+// fills them, so they split (2 pairs: 0.211 -> 0.192 ms on the B200). The
+// default of LaunchShape::split_rows_alone (KBFV_TUNE_SPLIT_ROWS_ALONE).
+constexpr int kSplitRowsAloneDefault = 148;
 
 // Forward NTT of `rows` rows read through `s` and written through `d`.
 // For logn <= 14 one block kernel (N = 2^14 with at most shape.split_rows14 rows:

@@ -27,8 +27,8 @@ static void klss_keyswitch(Context& c, const uint64_t* rlk_t, int count, const M
 static void mul_relin_klss_chunk(Context& c, const uint64_t* rlk_t, const PtrBatch& pb, int count,
                                  const MulScratch& m, cudaStream_t st) {
     const DevConsts& dc = c.dc;
-    mul_front(c, pb, count, m, st);
-    k5_launch(c, count, m, nullptr, 2, st);
+    mul_front(c.dc, pb, count, m, st);
+    k5_launch(c.dc, count, m, nullptr, 2, st);
     klss_keyswitch(c, rlk_t, count, m, st);
     ntt_fwd(dc, ModDownAddSrc{m.se, m.sd, dc}, OutCtDst{pb, dc.logn, dc.nq}, count * 2 * dc.nq, st);
 }

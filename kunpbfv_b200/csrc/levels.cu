@@ -410,8 +410,8 @@ int kbfv_mul_relin_gadget(kbfv_context* ctx, const uint64_t* d_gk, uint32_t log_
             uint8_t* base = ensure_scratch(c, mb + gadget_sg_bytes(c, cnt, w));
             MulScratch m = mul_scratch_layout(c, cnt, base);
             uint64_t* sg = (uint64_t*)(base + mb);
-            mul_front(c, pb, cnt, m, st);
-            k5_launch(c, cnt, m, nullptr, 2, st);
+            mul_front(c.dc, pb, cnt, m, st);
+            k5_launch(c.dc, cnt, m, nullptr, 2, st);
             gadget_keyswitch(c, d_gk, w, cnt, m, sg, m.sd, pb, st);
         }
     });

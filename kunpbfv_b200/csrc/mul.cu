@@ -23,8 +23,7 @@ void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* key, int 
         ntt_fwd(dc, ModDownAddSrc{se, add, dc, true}, dst, count * 2 * dc.nq, st);
 }
 
-void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st) {
-    const DevConsts& dc = c.dc;
+void mul_front(const DevConsts& dc, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st) {
     if (count <= dc.shape.fuse_q2r_pairs) {
         // K1 stores y_i = [x_i (Q/q_i)^-1]_{q_i}; K3's loader extends them to R
         ntt_inv(dc, PairQRowsP{pb, dc.logn, dc.nq}, QHatRowsIO{m.sa, dc.logn, dc.nq, dc.q2r_fold},
@@ -46,17 +45,16 @@ void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, c
     ntt_inv(dc, ts, QRRowsIO{m.sc, dc.logn, dc.nq, dc.nqr, dc.idx_r}, count * 3 * dc.nqr, st);
 }
 
-void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st) {
-#define L_K5(M) k5_launch_m<M>(c.dc, count, m, out0, mode, st)
-    DISPATCH_MAXQ(c.dc.nq + 1, L_K5);
+void k5_launch(const DevConsts& dc, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st) {
+#define L_K5(M) k5_launch_m<M>(dc, count, m, out0, mode, st)
+    DISPATCH_MAXQ(dc.nq + 1, L_K5);
 #undef L_K5
 }
 
-void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb, int count, const MulScratch& m,
-                            cudaStream_t st) {
-    const DevConsts& dc = c.dc;
-    mul_front(c, pb, count, m, st);
-    k5_launch(c, count, m, nullptr, 1, st);
+void mul_relin_chunk(const DevConsts& dc, const uint64_t* rlk, const PtrBatch& pb, int count, const MulScratch& m,
+                     cudaStream_t st) {
+    mul_front(dc, pb, count, m, st);
+    k5_launch(dc, count, m, nullptr, 1, st);
     // K6a: NTT over Q|P of the lifted digits, in place, fully reduced (key product uses barrett_prod)
     ntt_fwd<RowsIO, RowsIO, true>(dc, rows_io(dc, m.sd2, 0, dc.npq), rows_io(dc, m.sd2, 0, dc.npq),
                                    count * dc.dnum * dc.npq, st);
@@ -94,10 +92,11 @@ int kbfv_mul(kbfv_context* ctx, const uint64_t* d_ct1, const uint64_t* d_ct2, ui
             uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
             MulScratch m = mul_scratch_layout(c, cnt, base);
             uint64_t* out = d_tensor + (size_t)off * 3 * lq;
-            mul_front(c, pb, cnt, m, st);
-            k5_launch(c, cnt, m, out, 0, st);
-            RowsIO io = rows_io(c.dc, out, 0, c.nq);
-            ntt_fwd(c.dc, io, io, cnt * 3 * c.nq, st);
+            const DevConsts dc = alone_consts(c);  // one stream: no sibling sub-batch fills the SMs
+            mul_front(dc, pb, cnt, m, st);
+            k5_launch(dc, cnt, m, out, 0, st);
+            RowsIO io = rows_io(dc, out, 0, c.nq);
+            ntt_fwd(dc, io, io, cnt * 3 * c.nq, st);
         }
     });
 }
@@ -159,7 +158,7 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
                 PtrBatch pb = make_batch(ct_a + off, ct_b + off, out + off, cnt);
                 uint8_t* base = ensure_scratch(c, mul_scratch_layout(c, cnt, nullptr).bytes);
                 MulScratch m = mul_scratch_layout(c, cnt, base);
-                mul_relin_chunk(c, d_rlk, pb, cnt, m, st);
+                mul_relin_chunk(alone_consts(c), d_rlk, pb, cnt, m, st);
                 continue;
             }
             // sub-batches on the caller's stream and auxiliary streams, each with its
@@ -175,7 +174,7 @@ int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_
                 if (n <= 0) break;
                 PtrBatch pb = make_batch(ct_a + off + lo, ct_b + off + lo, out + off + lo, n);
                 MulScratch m = mul_scratch_layout(c, n, base + b * each);
-                mul_relin_chunk(c, d_rlk, pb, n, m, b == 0 ? st : c.aux[b - 1]);
+                mul_relin_chunk(c.dc, d_rlk, pb, n, m, b == 0 ? st : c.aux[b - 1]);
             }
             for (int b = 1; b < nb; b++) {
                 KB_CHECK_CUDA(cudaEventRecord(c.join_ev[b - 1], c.aux[b - 1]));
@@ -307,7 +306,7 @@ int kbfv_mul_relin_host(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t
             }
             PtrBatch pb = make_batch(A.data(), B.data(), O.data(), n);
             MulScratch m = mul_scratch_layout(c, n, base + k * region);
-            mul_relin_chunk(c, d_rlk, pb, n, m, comp);
+            mul_relin_chunk(c.dc, d_rlk, pb, n, m, comp);
             KB_CHECK_CUDA(cudaEventRecord(c.hcomp[s], comp));
             if (j >= 1) copy_out(j - 1);
         }
@@ -413,7 +412,7 @@ int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint6
             pb.b[i] = d_ct_b + i * stride;
             pb.o[i] = d_out + i * stride;
         }
-        mul_relin_chunk(c, d_rlk, pb, (int)count, m, S(stream));
+        mul_relin_chunk(c.dc, d_rlk, pb, (int)count, m, S(stream));
     });
 }
 

@@ -349,7 +349,7 @@ struct DecSrc {
 
 // INTT over Q of the four input polynomials, Q -> R, NTT over R, fused tensor +
 // INTT over Q|R: steps shared by kbfv_mul and the fused multiply-relinearise.
-void mul_front(Context& c, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st);
+void mul_front(const DevConsts& dc, const PtrBatch& pb, int count, const MulScratch& m, cudaStream_t st);
 // K5: scale-and-round, R -> Q and (mode 1) the key-switch digit lift
 template <int MAXQ>
 void k5_launch_m(const DevConsts& dc, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st);
@@ -357,12 +357,20 @@ void k5_launch_m(const DevConsts& dc, int count, const MulScratch& m, uint64_t* 
 // rows over Q (QHatRowsIO layout) -> NTT-form R limbs, fully reduced
 template <int MAXQ>
 void q2r_ntt_launch_m(const DevConsts& dc, const uint64_t* y, uint64_t* out, int polys, cudaStream_t st);
-void k5_launch(Context& c, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st);
+void k5_launch(const DevConsts& dc, int count, const MulScratch& m, uint64_t* out0, int mode, cudaStream_t st);
 // key-switch tail: key product, mod down and add, written to the outputs of pb
 void ks_tail(const DevConsts& dc, const uint64_t* sd2, const uint64_t* key, int ndig, uint64_t* se,
              const uint64_t* add, const PtrBatch& pb, int count, cudaStream_t st);
 // the auxiliary streams and fork / join events of the sub-batches (created once)
 void ensure_branch_streams(Context& c);
 // the whole multiply + relinearise of one sub-batch (9 launches)
-void mul_relin_chunk(Context& c, const uint64_t* rlk, const PtrBatch& pb, int count, const MulScratch& m,
+void mul_relin_chunk(const DevConsts& dc, const uint64_t* rlk, const PtrBatch& pb, int count, const MulScratch& m,
                      cudaStream_t st);
+// The constants with the launch shapes of a multiply that runs as one stream
+// (no sibling sub-batch on another stream to fill the SMs): 2^14-point
+// transforms of up to shape.split_rows_alone rows run split.
+static inline DevConsts alone_consts(const Context& c) {
+    DevConsts d = c.dc;
+    d.shape.split_rows14 = d.shape.split_rows_alone;
+    return d;
+}
