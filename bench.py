@@ -459,9 +459,10 @@ def run_ours(args, world, rank, local):
                    "l2": "inputs 235 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}",
                    "tuned": tuned},
         "decrypt_exact": ok, "noise_budget_bits": round(budget, 2),
-        # 9 kernels per sub-batch; batches of 16+ pairs run as `branches` sub-batches
-        # (at least 8 pairs each) on forked streams
-        "gpu_launches": 9 * max(1, min(ctx.tune_get("branches"), BATCH // 8)) * args.steps,
+        # 9 kernels per sub-batch; batches of 2 x min_branch_pairs pairs and more run as `branches` sub-batches
+        # (at least min_branch_pairs pairs each) on forked streams
+        "gpu_launches": 9 * max(1, min(ctx.tune_get("branches"), BATCH // ctx.tune_get("min_branch_pairs")))
+        * args.steps,
         "clocks": clk.summary(),
     }
     line["e2e"] = e2e_all_ranks(world, sch, c1, c2, out, stream)

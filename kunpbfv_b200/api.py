@@ -40,7 +40,7 @@ _ERR_NAMES = {
 TUNE_KNOBS = {"ntt_block_log": 0, "branches": 1, "host_chunk": 2, "split_rows": 3, "bconv_threads": 4,
               "k5_threads": 5, "k5_fused_pairs": 6, "bconv_cpt": 7,
               "fuse_q2r_pairs": 8, "l2_prefetch": 9,
-              "split_rows_alone": 10}
+              "split_rows_alone": 10, "min_branch_pairs": 11}
 
 
 class KbfvError(RuntimeError):

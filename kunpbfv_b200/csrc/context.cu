@@ -718,6 +718,10 @@ int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
                 KB_REQUIRE(value >= 0 && value <= (1 << 20), KBFV_ERR_INVALID, "split rows (one stream) must be 0..2^20");
                 c.dc.shape.split_rows_alone = (int)value;
                 break;
+            case KBFV_TUNE_MIN_BRANCH_PAIRS:
+                KB_REQUIRE(value >= 1 && value <= 64, KBFV_ERR_INVALID, "pairs per sub-batch must be 1..64");
+                c.min_branch_pairs = (int)value;
+                break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
         // the levels of a top context run with the top level's knobs
@@ -726,6 +730,7 @@ int kbfv_tune_set(kbfv_context* ctx, int knob, int64_t value) {
             Context& l = reinterpret_cast<kbfv_context*>(lv)->c;
             l.dc.shape = c.dc.shape;
             l.branches = c.branches;
+            l.min_branch_pairs = c.min_branch_pairs;
         }
     });
 }
@@ -746,6 +751,7 @@ int kbfv_tune_get(const kbfv_context* ctx, int knob, int64_t* value) {
             case KBFV_TUNE_FUSE_Q2R_PAIRS: *value = c.dc.shape.fuse_q2r_pairs; break;
             case KBFV_TUNE_L2_PREFETCH: *value = c.dc.shape.l2_prefetch; break;
             case KBFV_TUNE_SPLIT_ROWS_ALONE: *value = c.dc.shape.split_rows_alone; break;
+            case KBFV_TUNE_MIN_BRANCH_PAIRS: *value = c.min_branch_pairs; break;
             default: throw KbfvError(KBFV_ERR_INVALID, "unknown tuning knob");
         }
     });

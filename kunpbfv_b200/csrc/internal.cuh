@@ -295,10 +295,13 @@ static inline MulScratch mul_scratch_layout(const Context& c, int count, uint8_t
     m.bytes = off;
     return m;
 }
-// sub-batches of a batched multiply: one per `branches`, at least 8 pairs each
-constexpr int kMinBranchPairs = 8;
+// Sub-batches of a batched multiply hold at least Context::min_branch_pairs
+// pairs (default 2; KBFV_TUNE_MIN_BRANCH_PAIRS): from 4 pairs on, two
+// sub-batches on two streams fill the SMs that one batch's launches of fewer
+// rows than SMs leave idle (4 pairs 0.314 -> 0.270 ms, 8 pairs 0.481 -> 0.410 ms,
+// 12 pairs 0.679 -> 0.598 ms on the B200 against a minimum of 8).
 static inline int branch_count(const Context& c, int cnt) {
-    return std::max(1, std::min(c.branches, cnt / kMinBranchPairs));
+    return std::max(1, std::min(c.branches, cnt / std::max(1, c.min_branch_pairs)));
 }
 static inline size_t branch_region_bytes(const Context& c, int per) {
     return (mul_scratch_layout(c, per, nullptr).bytes + 255) & ~(size_t)255;

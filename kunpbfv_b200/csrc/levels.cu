@@ -217,6 +217,7 @@ int kbfv_context_at_level(kbfv_context* ctx, uint32_t live_q, kbfv_context** out
             h->c.parent = &c;
             h->c.dc.shape = c.dc.shape;
             h->c.branches = c.branches;
+            h->c.min_branch_pairs = c.min_branch_pairs;
             h->c.dc.key_nq = c.nq;
             h->c.dc.key_npq = c.nq + c.np;
             std::memcpy(h->c.seed, c.seed, 32);

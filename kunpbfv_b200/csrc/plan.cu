@@ -26,7 +26,7 @@ struct kbfv_plan {
     // what the captured kernels address and how they were shaped
     void* scratch = nullptr;
     LaunchShape shape{};
-    int branches = 0;
+    int branches = 0, min_branch_pairs = 0;
     uint64_t launches = 0, captures = 0;
 };
 
@@ -41,7 +41,7 @@ void drop_graph(kbfv_plan& p) {
 
 bool graph_current(const kbfv_plan& p) {
     const Context& c = p.ctx->c;
-    return p.exec && c.scratch == p.scratch && c.branches == p.branches &&
+    return p.exec && c.scratch == p.scratch && c.branches == p.branches && c.min_branch_pairs == p.min_branch_pairs &&
            std::memcmp(&c.dc.shape, &p.shape, sizeof(LaunchShape)) == 0;
 }
 
@@ -77,6 +77,7 @@ void run_and_capture(kbfv_plan& p, cudaStream_t st) {
     p.scratch = c.scratch;
     p.shape = c.dc.shape;
     p.branches = c.branches;
+    p.min_branch_pairs = c.min_branch_pairs;
     p.captures++;
 }
 

@@ -17,8 +17,9 @@ Knobs (include/kbfv.h, ``kbfv_tune_knob``):
   (batches of at most this many pairs run the Q -> R base extension in the
   loader of the forward NTT over R, no separate base-conversion launch),
   ``l2_prefetch`` (NTT block kernels ask L2 for the block one wave ahead)
-  and ``split_rows_alone`` (``split_rows`` for multiplies that run as one
-  stream, where no sibling sub-batch fills idle SMs).
+  ``split_rows_alone`` (``split_rows`` for multiplies that run as one
+  stream, where no sibling sub-batch fills idle SMs) and ``min_branch_pairs``
+  (pairs per sub-batch at least).
 
 Each candidate is timed on the device with CUDA events (two warm-up calls,
 then the median of three timed trials of ``reps`` calls). Knobs never change
@@ -55,7 +56,9 @@ PIPELINE_KNOBS = {
 K5_FUSED_PAIRS = (2, 0, 4)
 # tuned on one-pair and two-pair multiplies together
 FUSE_Q2R_PAIRS = (1, 0, 2)
-# tuned on two-pair and eight-pair multiplies (one stream each)
+# tuned on four-pair and eight-pair multiplies
+MIN_BRANCH_PAIRS = (2, 1, 4, 8)
+# tuned on two-pair and eight-pair multiplies
 SPLIT_ROWS_ALONE = (148, 48, 96, 256, 512)
 
 
@@ -209,7 +212,7 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
     from .api import Ciphertext
     ctx = scheme.context
     keep = {k: ctx.tune_get(k) for k in list(PIPELINE_KNOBS) + ["k5_fused_pairs", "fuse_q2r_pairs",
-                                                                  "split_rows_alone"]}
+                                                                  "split_rows_alone", "min_branch_pairs"]}
     c1 = Ciphertext(ctx, _random_pairs(ctx, pairs, 2))
     c2 = Ciphertext(ctx, _random_pairs(ctx, pairs, 3))
     out = Ciphertext(ctx, count=pairs)
@@ -224,6 +227,10 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
     f1 = Ciphertext(ctx, c1.cipher_device[:eight].clone())
     f2 = Ciphertext(ctx, c2.cipher_device[:eight].clone())
     out8 = Ciphertext(ctx, count=eight)
+    four = min(4, pairs)
+    g1 = Ciphertext(ctx, c1.cipher_device[:four].clone())
+    g2 = Ciphertext(ctx, c2.cipher_device[:four].clone())
+    out4 = Ciphertext(ctx, count=four)
     result: Dict[str, object] = {}
     try:
         for k, vals in PIPELINE_KNOBS.items():  # defaults first: the reference products
@@ -231,13 +238,16 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
         ctx.tune_set("k5_fused_pairs", K5_FUSED_PAIRS[0])
         ctx.tune_set("fuse_q2r_pairs", FUSE_Q2R_PAIRS[0])
         ctx.tune_set("split_rows_alone", SPLIT_ROWS_ALONE[0])
+        ctx.tune_set("min_branch_pairs", MIN_BRANCH_PAIRS[0])
         scheme.mult_relin(c1, c2, out=out)
         scheme.mult_relin(d1, d2, out=out2)
         scheme.mult_relin(e1, e2, out=out1)
         scheme.mult_relin(f1, f2, out=out8)
+        scheme.mult_relin(g1, g2, out=out4)
         torch.cuda.synchronize()
         want, want2, want1 = out.cipher_device.clone(), out2.cipher_device.clone(), out1.cipher_device.clone()
         want8 = out8.cipher_device.clone()
+        want4 = out4.cipher_device.clone()
         for k, vals in PIPELINE_KNOBS.items():
             ms = _sweep(ctx, k, vals, lambda: scheme.mult_relin(c1, c2, out=out), out, want, reps)
             result[k], result[k + "_ms"] = min(ms, key=ms.get), {str(v): t for v, t in ms.items()}
@@ -251,6 +261,13 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
             scheme.mult_relin(d1, d2, out=out2)
         ms = _sweep(ctx, "fuse_q2r_pairs", FUSE_Q2R_PAIRS, per_call, (out1, out2), (want1, want2), reps)
         result["fuse_q2r_pairs"], result["fuse_q2r_pairs_ms"] = min(ms, key=ms.get), {
+            str(v): t for v, t in ms.items()}
+
+        def small():
+            scheme.mult_relin(g1, g2, out=out4)
+            scheme.mult_relin(f1, f2, out=out8)
+        ms = _sweep(ctx, "min_branch_pairs", MIN_BRANCH_PAIRS, small, (out4, out8), (want4, want8), reps)
+        result["min_branch_pairs"], result["min_branch_pairs_ms"] = min(ms, key=ms.get), {
             str(v): t for v, t in ms.items()}
 
         def one_stream():
@@ -267,7 +284,7 @@ def tune_pipeline(scheme, pairs: int = 64, reps: int = 5) -> Dict[str, object]:
 
 
 PIPELINE_CHOICES = ("branches", "bconv_threads", "bconv_cpt", "k5_threads", "split_rows", "l2_prefetch",
-                    "k5_fused_pairs", "fuse_q2r_pairs", "split_rows_alone")
+                    "k5_fused_pairs", "fuse_q2r_pairs", "min_branch_pairs", "split_rows_alone")
 
 
 def apply_choice(ctx, choice: dict) -> None:

@@ -55,7 +55,7 @@ def test_autotune_applies_and_caches(tmp_path):
     assert ctx.tune_get("host_chunk") == got["host_chunk"]
     assert set(got["branches_ms"]) == {str(b) for b in tune.BRANCHES}
     for k in ("bconv_threads", "bconv_cpt", "k5_threads", "split_rows", "k5_fused_pairs", "fuse_q2r_pairs",
-              "split_rows_alone"):
+              "split_rows_alone", "min_branch_pairs"):
         assert ctx.tune_get(k) == got[k], k
     assert set(got["fuse_q2r_pairs_ms"]) == {str(v) for v in tune.FUSE_Q2R_PAIRS}
     # a fresh context of the same parameters takes the cached choice without timing
@@ -104,7 +104,8 @@ def test_host_chunk_knob_drives_the_default_chunk():
 @pytest.mark.parametrize("knob,values", [("bconv_threads", (64, 128, 256, 512)), ("k5_threads", (64, 128, 256)),
                                          ("split_rows", (0, 48, 1 << 20)), ("k5_fused_pairs", (0, 2, 4)),
                                          ("bconv_cpt", (1, 2)), ("fuse_q2r_pairs", (128, 0, 1)),
-                                         ("l2_prefetch", (0, 1)), ("split_rows_alone", (0, 48, 148, 1 << 20))])
+                                         ("l2_prefetch", (0, 1)), ("split_rows_alone", (0, 48, 148, 1 << 20)),
+                                         ("min_branch_pairs", (1, 2, 8))])
 def test_pipeline_shapes_keep_the_product(knob, values):
     """Every launch shape of the multiply pipeline gives the oracle's product
     (N=16384, 7 + 1 primes; 3 pairs: K5 fused or split by k5_fused_pairs,
@@ -144,12 +145,14 @@ def test_pipeline_knob_bounds_and_levels():
     ctx = kb.BFVContext.from_bits(13, [50, 50, 50], [52], 65537, dnum=3)
     for knob, bad in (("bconv_threads", 100), ("bconv_threads", 1024), ("k5_threads", 512), ("k5_threads", 32),
                       ("split_rows", -1), ("k5_fused_pairs", 129), ("fuse_q2r_pairs", 129), ("bconv_cpt", 3),
-                      ("l2_prefetch", 2), ("split_rows_alone", -1)):
+                      ("l2_prefetch", 2), ("split_rows_alone", -1), ("min_branch_pairs", 0),
+                      ("min_branch_pairs", 65)):
         with pytest.raises(kb.KbfvError):
             ctx.tune_set(knob, bad)
     assert (ctx.tune_get("split_rows"), ctx.tune_get("bconv_threads"), ctx.tune_get("k5_threads"),
             ctx.tune_get("k5_fused_pairs"), ctx.tune_get("bconv_cpt"), ctx.tune_get("fuse_q2r_pairs"),
-            ctx.tune_get("l2_prefetch"), ctx.tune_get("split_rows_alone")) == (48, 256, 128, 2, 2, 1, 1, 148)
+            ctx.tune_get("l2_prefetch"), ctx.tune_get("split_rows_alone"),
+            ctx.tune_get("min_branch_pairs")) == (48, 256, 128, 2, 2, 1, 1, 148, 2)
     lv = ctx.at_level(2)
     ctx.tune_set("k5_threads", 64)
     assert lv.tune_get("k5_threads") == 64  # levels follow the top level's knobs
