@@ -251,7 +251,7 @@ int kbfv_relinearize(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d
 int kbfv_mul_relin_batch(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* const* ct_a,
                          const uint64_t* const* ct_b, uint64_t* const* out, uint32_t count,
                          kbfv_stream stream);
-/* Batches of 4 or more pairs (2 x KBFV_TUNE_MIN_BRANCH_PAIRS) run as sub-batches on the caller's stream and on
+/* Batches of 2 or more pairs (2 x KBFV_TUNE_MIN_BRANCH_PAIRS) run as sub-batches on the caller's stream and on
  * auxiliary streams of the context, forked from and joined back into the
  * caller's stream with events (the call stays ordered on `stream`); the partial
  * last wave of one sub-batch's kernels then overlaps the others'. branches: 1..4
@@ -294,7 +294,7 @@ typedef enum {
     KBFV_TUNE_SPLIT_ROWS_ALONE = 10, /* 0..2^20 (default 148): KBFV_TUNE_SPLIT_ROWS for a multiply
                                     that runs as one stream (batches too small for sub-batches,
                                     kbfv_mul), where no sibling sub-batch fills idle SMs */
-    KBFV_TUNE_MIN_BRANCH_PAIRS = 11 /* 1..64 (default 2): a batched multiply splits into
+    KBFV_TUNE_MIN_BRANCH_PAIRS = 11 /* 1..64 (default 1): a batched multiply splits into
                                     KBFV_TUNE_BRANCHES sub-batches only with at least this many
                                     pairs in each */
 } kbfv_tune_knob;
@@ -445,7 +445,7 @@ int kbfv_mul_relin_klss(kbfv_context* ctx, const uint64_t* d_rlk_t, const uint64
  * contexts built with T-base primes): 143 limbs of 128 KiB = 17.9 MiB per pair
  * at N=16384 with 7 + 1 primes and dnum 1, so 2 pairs; with dnum 7 one pair.
  * For a single pair kbfv_mul_relin_scratch_bytes(ctx, count) returns the same
- * figure (from 2 x KBFV_TUNE_MIN_BRANCH_PAIRS pairs on, 4 by default, it counts
+ * figure (from 2 x KBFV_TUNE_MIN_BRANCH_PAIRS pairs on, 2 by default, it counts
  * the batched multiply's sub-batches).
  * Larger requests return KBFV_ERR_INVALID and launch nothing; nothing on this
  * path calls cudaMalloc, cudaFree or any allocating routine, and the

@@ -131,7 +131,7 @@ struct Context {
     // auxiliary streams (forked and joined with events), so one sub-batch's
     // partial last wave overlaps the others' kernels
     int branches = 2;
-    int min_branch_pairs = 2;  // pairs per sub-batch at least (smaller batches run as one stream)
+    int min_branch_pairs = 1;  // pairs per sub-batch at least (smaller batches run as one stream)
     // tuning knobs (kbfv_tune_set): block size 2^ntt_block_log of the standalone
     // NTT on rings above it (the rest runs as a column pass of logn - ntt_block_log
     // stages); pairs per chunk of the host-memory multiply (0: by bytes)

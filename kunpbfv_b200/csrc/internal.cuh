@@ -296,10 +296,11 @@ static inline MulScratch mul_scratch_layout(const Context& c, int count, uint8_t
     return m;
 }
 // Sub-batches of a batched multiply hold at least Context::min_branch_pairs
-// pairs (default 2; KBFV_TUNE_MIN_BRANCH_PAIRS): from 4 pairs on, two
+// pairs (default 1; KBFV_TUNE_MIN_BRANCH_PAIRS): from 2 pairs on, two
 // sub-batches on two streams fill the SMs that one batch's launches of fewer
-// rows than SMs leave idle (4 pairs 0.314 -> 0.270 ms, 8 pairs 0.481 -> 0.410 ms,
-// 12 pairs 0.679 -> 0.598 ms on the B200 against a minimum of 8).
+// rows than SMs leave idle (3 pairs 0.252 -> 0.243 ms against a minimum of 2;
+// 4 pairs 0.314 -> 0.265 ms, 8 pairs 0.481 -> 0.408 ms, 12 pairs 0.679 ->
+// 0.597 ms on the B200 against a minimum of 8).
 static inline int branch_count(const Context& c, int cnt) {
     return std::max(1, std::min(c.branches, cnt / std::max(1, c.min_branch_pairs)));
 }

@@ -56,8 +56,9 @@ PIPELINE_KNOBS = {
 K5_FUSED_PAIRS = (2, 0, 4)
 # tuned on one-pair and two-pair multiplies together
 FUSE_Q2R_PAIRS = (1, 0, 2)
-# tuned on four-pair and eight-pair multiplies
-MIN_BRANCH_PAIRS = (2, 1, 4, 8)
+# tuned on four-pair and eight-pair multiplies (1 and 2 tie there; 1 is 3.5%
+# faster at three pairs)
+MIN_BRANCH_PAIRS = (1, 2, 4, 8)
 # tuned on two-pair and eight-pair multiplies
 SPLIT_ROWS_ALONE = (148, 48, 96, 256, 512)
 

@@ -152,7 +152,7 @@ def test_pipeline_knob_bounds_and_levels():
     assert (ctx.tune_get("split_rows"), ctx.tune_get("bconv_threads"), ctx.tune_get("k5_threads"),
             ctx.tune_get("k5_fused_pairs"), ctx.tune_get("bconv_cpt"), ctx.tune_get("fuse_q2r_pairs"),
             ctx.tune_get("l2_prefetch"), ctx.tune_get("split_rows_alone"),
-            ctx.tune_get("min_branch_pairs")) == (48, 256, 128, 2, 2, 1, 1, 148, 2)
+            ctx.tune_get("min_branch_pairs")) == (48, 256, 128, 2, 2, 1, 1, 148, 1)
     lv = ctx.at_level(2)
     ctx.tune_set("k5_threads", 64)
     assert lv.tune_get("k5_threads") == 64  # levels follow the top level's knobs
