@@ -485,7 +485,8 @@ int kbfv_mul_relin_noalloc(kbfv_context* ctx, const uint64_t* d_rlk, const uint6
  * graph again (eagerly, as the first). Creating a plan sizes the context's
  * arena for `count` pairs (kbfv_reserve). Plans of one context share that
  * arena with every other call on the context, so their launches must be
- * ordered with those calls (one stream, or events), as for kbfv_mul_relin. */
+ * ordered with those calls (one stream, or events), as for kbfv_mul_relin.
+ * A plan refers to its context and buffers: destroy it before them. */
 typedef struct kbfv_plan kbfv_plan;
 int kbfv_plan_mul_relin(kbfv_context* ctx, const uint64_t* d_rlk, const uint64_t* d_ct_a, const uint64_t* d_ct_b,
                         uint64_t* d_out, uint32_t count, kbfv_plan** plan);
