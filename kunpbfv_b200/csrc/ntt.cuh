@@ -307,6 +307,18 @@ __device__ __forceinline__ int sweep_index(int t, int k) {
     else return (t / S) * (S * 16) + (t % S) + k * S;
 }
 
+// Resident CTAs per SM a block kernel is compiled for (0: left to ptxas). The
+// 2^13-point blocks (512 threads, 68 KiB of shared memory) get two, i.e. 64
+// registers a thread: left to itself ptxas gives them 88 and one CTA per SM
+// (N = 8192 multiply, 64 pairs: 0.825 -> 0.760 ms). Capping the 2^12-point
+// blocks at 64 registers as well (four CTAs) measured mixed (-1% for the
+// N = 32768 multiply, +3.5% for a two-pair multiply at N = 16384), so they,
+// and the 1024-thread 2^14 blocks (64 registers either way), keep ptxas's choice.
+template <int LOGB>
+constexpr int block_min_ctas() {
+    return LOGB == 13 ? 2 : 0;
+}
+
 struct PassCtx {
     uint64_t* sm;
     const tw_t* tw;
@@ -438,7 +450,7 @@ __device__ __forceinline__ constexpr bool inv_direct_load() {
 
 // FULL: fully reduce the output to [0, q); otherwise outputs are in [0, 8q).
 template <int LOGB, class Src, class Dst, bool FULL = true>
-static __global__ void __launch_bounds__(1 << (LOGB - 4))
+static __global__ void __launch_bounds__(1 << (LOGB - 4), block_min_ctas<LOGB>())
 ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
                      int logn, int ahead) {
     constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
@@ -483,7 +495,7 @@ ntt_fwd_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const ui
 
 // WHOLE: the block is the whole ring (logn == LOGB), so n^-1 is applied here.
 template <int LOGB, class Src, class Dst, bool WHOLE = true>
-static __global__ void __launch_bounds__(1 << (LOGB - 4))
+static __global__ void __launch_bounds__(1 << (LOGB - 4), block_min_ctas<LOGB>())
 ntt_inv_block_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods,
                      int logn, int ahead) {
     constexpr int NB = 1 << LOGB, T = NB / 16, RAD = BlockShape<LOGB>::RAD;
