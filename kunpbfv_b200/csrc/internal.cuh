@@ -188,7 +188,7 @@ static void ntt_fwd(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
             const size_t total = (size_t)rows << 12;
             using DP = decltype(plain_of(d));
             const DP dp = plain_of(d);
-            ntt_fwd_col_kernel<4, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
+            ntt_fwd_col16_kernel<4, Src, DP><<<stride_blocks(total, 256), 256, 0, st>>>(s, dp, dc.tw_fwd, dc.mods, 16, total);
             launch_fwd_block<12, DP, Dst, FULL>(dc, dp, d, rows, 16, st);
             break;
         }
@@ -224,7 +224,7 @@ static void ntt_inv(const DevConsts& dc, Src s, Dst d, int rows, cudaStream_t st
         case 16: {
             launch_inv_block<12, Src, Dst, false>(dc, s, d, rows, 16, st);
             const size_t total = (size_t)rows << 12;
-            ntt_inv_col_kernel<4, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
+            ntt_inv_col16_kernel<4, Dst, Dst><<<stride_blocks(total, 256), 256, 0, st>>>(d, d, dc.tw_inv, dc.mods, 16, total);
             break;
         }
         default: throw KbfvError(KBFV_ERR_INVALID, "unsupported ring degree");

@@ -596,6 +596,29 @@ static __global__ void ntt_inv_col_kernel(Src src, Dst dst, const tw_t* __restri
         ntt_inv_col<RC>(src, dst, tw_all, mods, logn, gid);
 }
 
+// The radix-16 column pass (N = 2^16 ahead of / behind 2^12-point blocks)
+// holds 16 points a thread: compiled for three 256-thread CTAs per SM (80
+// registers) instead of ptxas's own 104 registers and two CTAs (forward
+// 0.881 -> 0.838 ms, inverse 0.894 -> 0.846 ms per 1024 rows at N = 65536).
+// Launched with 256 threads.
+template <int RC, class Src, class Dst>
+static __global__ void __launch_bounds__(256, 3)
+ntt_fwd_col16_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods, int logn,
+                     size_t ncol_total) {
+    for (size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gid < ncol_total;
+         gid += (size_t)gridDim.x * blockDim.x)
+        ntt_fwd_col<RC>(src, dst, tw_all, mods, logn, gid);
+}
+
+template <int RC, class Src, class Dst>
+static __global__ void __launch_bounds__(256, 3)
+ntt_inv_col16_kernel(Src src, Dst dst, const tw_t* __restrict__ tw_all, const uint64_t* __restrict__ mods, int logn,
+                     size_t ncol_total) {
+    for (size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x; gid < ncol_total;
+         gid += (size_t)gridDim.x * blockDim.x)
+        ntt_inv_col<RC>(src, dst, tw_all, mods, logn, gid);
+}
+
 // ---------------------------------------------------------------------------
 // Row functors: prime(row), bind(row) -> {load(j), store(j, v)}
 // ---------------------------------------------------------------------------

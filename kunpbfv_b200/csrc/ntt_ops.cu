@@ -9,13 +9,21 @@ template <int RC, int LB>
 static void ntt_rows_split(const DevConsts& dc, RowsIO io, int rows, bool fwd, cudaStream_t st) {
     const size_t total = (size_t)rows << LB;
     if (fwd) {
-        ntt_fwd_col_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_fwd, dc.mods,
-                                                                                      dc.logn, total);
+        if constexpr (RC == 4)
+            ntt_fwd_col16_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_fwd,
+                                                                                            dc.mods, dc.logn, total);
+        else
+            ntt_fwd_col_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_fwd,
+                                                                                          dc.mods, dc.logn, total);
         launch_fwd_block<LB, RowsIO, RowsIO, true>(dc, io, io, rows, dc.logn, st);
     } else {
         launch_inv_block<LB, RowsIO, RowsIO, false>(dc, io, io, rows, dc.logn, st);
-        ntt_inv_col_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_inv, dc.mods,
-                                                                                      dc.logn, total);
+        if constexpr (RC == 4)
+            ntt_inv_col16_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_inv,
+                                                                                            dc.mods, dc.logn, total);
+        else
+            ntt_inv_col_kernel<RC, RowsIO, RowsIO><<<stride_blocks(total, 256), 256, 0, st>>>(io, io, dc.tw_inv,
+                                                                                          dc.mods, dc.logn, total);
     }
     check_launch(fwd ? "ntt_fwd" : "ntt_inv");
 }
