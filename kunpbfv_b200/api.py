@@ -344,7 +344,7 @@ class BFVContext:
         return self._h
 
     def set_branches(self, branches: int):
-        """sub-batches (and streams) a batched multiply of 16+ pairs uses, 1..4"""
+        """sub-batches (and streams) a batched multiply of two or more pairs uses, 1..4"""
         _check(lib().kbfv_set_branches(self._h, branches))
 
     def tune_set(self, knob: str, value: int):
